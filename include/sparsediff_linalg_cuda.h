@@ -1,0 +1,141 @@
+/* sparsediff_linalg B200 extension API.
+ *
+ * The drop-in headers under sparsediff_linalg/ keep the upstream host-pointer API.
+ * This header adds what a GPU-resident caller needs and upstream has no
+ * counterpart for:
+ *   - status codes and error text instead of exit(1);
+ *   - device-resident products, transposes and duplicate coalescing whose
+ *     operands and results stay in HBM (all pointers below are DEVICE pointers
+ *     unless a comment says otherwise);
+ *   - the batched refill engine and the learned row scheduler.
+ * Every function is extern "C" with plain pointers and sizes. Streams are passed
+ * as void* (a cudaStream_t); NULL means the library's own stream. */
+#ifndef SPARSEDIFF_LINALG_CUDA_H
+#define SPARSEDIFF_LINALG_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "sparsediff_linalg/COO_matrix.h"
+#include "sparsediff_linalg/CSC_matrix.h"
+#include "sparsediff_linalg/CSR_matrix.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum sdl_status
+{
+    SDL_OK = 0,
+    SDL_ERR_NO_DEVICE = 1,   /* no usable CUDA device */
+    SDL_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    SDL_ERR_INVALID = 3,     /* malformed input (bad pointers, sizes, indices) */
+    SDL_ERR_OVERFLOW = 4,    /* a result does not fit int32 indexing */
+    SDL_ERR_OOM = 5,         /* device allocation failed */
+    SDL_ERR_UNSUPPORTED = 6, /* operand combination not provided by this build */
+    SDL_ERR_TIMEOUT = 7,     /* a bounded device wait gave up */
+    SDL_ERR_INTERNAL = 8     /* a device-side consistency check failed */
+} sdl_status;
+
+/* Status and message of the last failing call on this thread (SDL_OK / "" when
+   none). */
+sdl_status sdl_last_status(void);
+const char *sdl_last_error(void);
+void sdl_clear_error(void);
+
+/* The upstream API has no error returns: by default a device failure inside one
+   of its entry points prints the message to stderr and exits(1), as upstream does
+   on its own fatal conditions. With fatal = 0 those entry points instead record
+   the status (sdl_last_status) and return NULL / leave outputs unchanged. */
+void sdl_set_fatal_errors(int fatal);
+
+/* 1 if a CUDA device is usable (initialises the library runtime on it). */
+int sdl_device_available(void);
+/* Number of device allocations / kernel launches the library has made so far. */
+unsigned long long sdl_device_alloc_count(void);
+unsigned long long sdl_kernel_launch_count(void);
+/* The library's stream (a cudaStream_t) and a full synchronisation of it. */
+void *sdl_stream(void);
+sdl_status sdl_synchronize(void);
+/* Frees a buffer the library allocated and handed out (device pointer). */
+void sdl_free(void *device_ptr);
+
+/* ------------------------------------------------------------------------
+   Device-resident sparse product  C = kron(I_blocks, L) diag(d) A.
+   L is given by rows (Lp, Li): for B^T D A, L is the CSC of B (its columns);
+   for C = B A, L is B's CSR. A is CSR with A_m = blocks * (rows of A per block).
+   L_map (optional) makes the value of L entry ii equal Lx[L_map[ii]], which lets
+   the fill read B's values straight from its CSR (L_map = the CSR position of
+   each CSC entry) with no separate CSC refresh.
+   ------------------------------------------------------------------------ */
+typedef struct sdl_product sdl_product;
+
+typedef struct sdl_product_desc
+{
+    const int *Lp;
+    const int *Li;
+    const int *L_map; /* may be NULL */
+    int L_m, L_nnz;
+    int blocks; /* >= 1 */
+    const int *Ap;
+    const int *Ai;
+    int A_m, A_n, A_nnz;
+} sdl_product_desc;
+
+/* Symbolic phase (exact structure, rows sorted ascending, unique) and the
+   numeric schedule. The operand structure arrays must stay alive and unchanged
+   while the product is used. Synchronises the stream. */
+sdl_status sdl_product_create(const sdl_product_desc *desc, void *stream,
+                              sdl_product **out);
+/* Shape, nnz and device pointers to C's row offsets / column indices (owned by
+   the product). */
+sdl_status sdl_product_info(const sdl_product *P, int *m, int *n, int *nnz,
+                            long long *terms, const int **Cp, const int **Ci);
+/* Numeric phase: Cx[0 .. nnz) = values of C. Lx (NULL = every L value is 1.0),
+   d (A_m values, NULL = identity), Ax. Asynchronous on the stream; never
+   allocates; each entry is summed in the upstream order with the upstream
+   roundings (no FMA). */
+sdl_status sdl_product_fill(const sdl_product *P, const double *Lx, const double *d,
+                            const double *Ax, double *Cx, void *stream);
+void sdl_product_destroy(sdl_product *P);
+
+/* ------------------------------------------------------------------------
+   Device-resident stable transpose of a compressed structure (CSR -> CSC,
+   CSC -> CSR, A -> A^T). The source is rows x cols with nnz entries; the result
+   has cols + 1 offsets, the source row of each entry (ascending within each
+   output row) and the source position of each entry (src).
+   ------------------------------------------------------------------------ */
+typedef struct sdl_transpose sdl_transpose;
+sdl_status sdl_transpose_create(const int *p, const int *idx, int rows, int cols,
+                                int nnz, void *stream, sdl_transpose **out);
+sdl_status sdl_transpose_info(const sdl_transpose *T, const int **Tp,
+                              const int **Ti, const int **src);
+/* Tx[q] = x[src[q]]. */
+sdl_status sdl_transpose_fill(const sdl_transpose *T, const double *x, double *Tx,
+                              void *stream);
+void sdl_transpose_destroy(sdl_transpose *T);
+
+/* ------------------------------------------------------------------------
+   Duplicate coalescing: COO triplets -> CSR with sorted unique columns per row,
+   duplicates summed in ascending triplet order (the order upstream's row_reduce
+   sums sources in). Two phases: the plan (structure) and the fill (values).
+   ------------------------------------------------------------------------ */
+typedef struct sdl_coalesce sdl_coalesce;
+sdl_status sdl_coalesce_create(const int *rows, const int *cols, int nnz_in, int m,
+                               int n, void *stream, sdl_coalesce **out);
+sdl_status sdl_coalesce_info(const sdl_coalesce *C, int *nnz_out, const int **Cp,
+                             const int **Ci);
+sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, double *Cx,
+                             void *stream);
+void sdl_coalesce_destroy(sdl_coalesce *C);
+
+/* Host-pointer form for COO_matrix users (no upstream counterpart): the
+   coalesced CSR of A (m x n), and a refill of its values from A->x. */
+CSR_matrix *COO_coalesce_alloc(const COO_matrix *A);
+void COO_coalesce_fill_values(const COO_matrix *A, CSR_matrix *C);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARSEDIFF_LINALG_CUDA_H */

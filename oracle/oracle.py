@@ -1,0 +1,213 @@
+"""Checker side of the tests and of bench.py's CPU baseline (test infrastructure).
+
+Two CPU implementations live here, both built by ``oracle/Makefile`` into
+``oracle/_ref/``:
+
+* ``port``: ``libsdl_oracle.so``, this repository's plain-C restatement of the
+  upstream algorithms (``sdl_oracle.c``; every function cites the upstream lines
+  it follows);
+* ``reference``: ``libsdl_ref.so``, the upstream library itself compiled from its
+  own C sources, called through its public API.
+
+Nothing in the product package imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+PORT_LIB = REF_DIR / "libsdl_oracle.so"
+REF_LIB = REF_DIR / "libsdl_ref.so"
+
+ip = C.POINTER(C.c_int)
+dp = C.POINTER(C.c_double)
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the port (always) and the upstream library (when its sources exist)."""
+    r = subprocess.run(["make", "-s", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+    if not quiet:
+        print(r.stdout)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(C.POINTER(t)) if a is not None else None
+
+
+_PORT = None
+_REF = None
+
+
+def port():
+    global _PORT
+    if _PORT is None:
+        if not PORT_LIB.exists():
+            build()
+        L = C.CDLL(str(PORT_LIB))
+        L.orc_gustavson_count.restype = C.c_longlong
+        L.orc_gustavson_count.argtypes = [ip, ip, C.c_int, C.c_int, ip, ip, C.c_int, C.c_int, ip, ip]
+        L.orc_gustavson_structure.restype = None
+        L.orc_gustavson_structure.argtypes = [ip, ip, C.c_int, C.c_int, ip, ip, C.c_int, C.c_int, ip, ip, ip]
+        L.orc_gustavson_values.restype = None
+        L.orc_gustavson_values.argtypes = [ip, ip, dp, C.c_int, C.c_int, dp, ip, ip, dp, C.c_int,
+                                           C.c_int, ip, ip, dp, dp]
+        L.orc_transpose.restype = None
+        L.orc_transpose.argtypes = [ip, ip, dp, C.c_int, C.c_int, ip, ip, dp, ip]
+        L.orc_coalesce_count.restype = C.c_longlong
+        L.orc_coalesce_count.argtypes = [ip, ip, C.c_int, C.c_int, C.c_int, ip]
+        L.orc_coalesce_fill.restype = None
+        L.orc_coalesce_fill.argtypes = [ip, ip, dp, C.c_int, C.c_int, C.c_int, ip, ip, dp]
+        L.orc_row_gather_count.restype = C.c_longlong
+        L.orc_row_gather_count.argtypes = [ip, ip, C.c_int, ip]
+        L.orc_row_gather_fill.restype = None
+        L.orc_row_gather_fill.argtypes = [ip, ip, dp, ip, C.c_int, ip, ip, dp]
+        L.orc_row_reduce_count.restype = C.c_longlong
+        L.orc_row_reduce_count.argtypes = [ip, ip, C.c_int, C.c_int, ip, C.c_int, ip]
+        L.orc_row_reduce_fill.restype = None
+        L.orc_row_reduce_fill.argtypes = [ip, ip, dp, C.c_int, C.c_int, ip, C.c_int, ip, ip, dp]
+        L.orc_dense_btdb.restype = None
+        L.orc_dense_btdb.argtypes = [dp, dp, dp, C.c_int, C.c_int, C.c_int, dp]
+        _PORT = L
+    return _PORT
+
+
+def reference_available() -> bool:
+    return REF_LIB.exists()
+
+
+def reference():
+    """The upstream library (compiled from its sources), with the upstream
+    signatures bound. Raises if it was not built."""
+    global _REF
+    if _REF is None:
+        if not REF_LIB.exists():
+            raise RuntimeError("upstream library not built (oracle/_ref/libsdl_ref.so)")
+        from sparsediff_linalg_b200._lib import UPSTREAM_SIGNATURES, bind, CSR_p, CSC_p, matrix_p
+        L = C.CDLL(str(REF_LIB))
+        bind(L, UPSTREAM_SIGNATURES)
+        vp = C.c_void_p
+        extra = {
+            "new_sparse_matrix": (matrix_p, [CSR_p]),
+            "free_matrix": (None, [matrix_p]),
+            "BTA_matrices_alloc": (matrix_p, [matrix_p, matrix_p]),
+            "BTDA_matrices_fill_values": (None, [matrix_p, vp, matrix_p, matrix_p]),
+            "BA_matrices_alloc": (matrix_p, [matrix_p, matrix_p]),
+            "BA_matrices_fill_values": (None, [matrix_p, matrix_p, matrix_p]),
+            "ATA_matrices_alloc": (matrix_p, [matrix_p]),
+            "ATDA_matrices_fill_values": (None, [matrix_p, vp, matrix_p]),
+        }
+        bind(L, extra)
+        _REF = L
+    return _REF
+
+
+# ----------------------------------------------------------------- numpy helpers
+def gustavson(Lp, Li, Lx, L_m, blocks, d, Ap, Ai, Ax, A_m, A_n):
+    """(Cp, Ci, Cx) of C = kron(I_blocks, L) diag(d) A by the port."""
+    L = port()
+    Lp = np.ascontiguousarray(Lp, np.int32); Li = np.ascontiguousarray(Li, np.int32)
+    Ap = np.ascontiguousarray(Ap, np.int32); Ai = np.ascontiguousarray(Ai, np.int32)
+    Cp = np.zeros(L_m * blocks + 1, np.int32)
+    work = np.zeros(max(1, A_n), np.int32)
+    nnz = L.orc_gustavson_count(_ptr(Lp, C.c_int), _ptr(Li, C.c_int), L_m, blocks,
+                                _ptr(Ap, C.c_int), _ptr(Ai, C.c_int), A_m, A_n,
+                                _ptr(Cp, C.c_int), _ptr(work, C.c_int))
+    if nnz < 0:
+        raise OverflowError("nnz(C) exceeds INT_MAX")
+    Ci = np.zeros(max(1, nnz), np.int32)
+    L.orc_gustavson_structure(_ptr(Lp, C.c_int), _ptr(Li, C.c_int), L_m, blocks,
+                              _ptr(Ap, C.c_int), _ptr(Ai, C.c_int), A_m, A_n,
+                              _ptr(Cp, C.c_int), _ptr(Ci, C.c_int), _ptr(work, C.c_int))
+    Cx = np.zeros(max(1, nnz), np.float64)
+    if Ax is not None:
+        Lx = None if Lx is None else np.ascontiguousarray(Lx, np.float64)
+        d = None if d is None else np.ascontiguousarray(d, np.float64)
+        Ax = np.ascontiguousarray(Ax, np.float64)
+        dwork = np.zeros(max(1, A_n), np.float64)
+        L.orc_gustavson_values(_ptr(Lp, C.c_int), _ptr(Li, C.c_int), _ptr(Lx, C.c_double), L_m,
+                               blocks, _ptr(d, C.c_double), _ptr(Ap, C.c_int), _ptr(Ai, C.c_int),
+                               _ptr(Ax, C.c_double), A_m, A_n, _ptr(Cp, C.c_int),
+                               _ptr(Ci, C.c_int), _ptr(Cx, C.c_double), _ptr(dwork, C.c_double))
+    return Cp, Ci[:nnz], Cx[:nnz]
+
+
+def transpose(p, idx, x, rows, cols):
+    """(Tp, Ti, Tx) of the stable transpose by the port."""
+    L = port()
+    p = np.ascontiguousarray(p, np.int32); idx = np.ascontiguousarray(idx, np.int32)
+    nnz = int(p[rows])
+    Tp = np.zeros(cols + 1, np.int32)
+    Ti = np.zeros(max(1, nnz), np.int32)
+    Tx = np.zeros(max(1, nnz), np.float64)
+    xx = None if x is None else np.ascontiguousarray(x, np.float64)
+    work = np.zeros(max(1, cols), np.int32)
+    L.orc_transpose(_ptr(p, C.c_int), _ptr(idx, C.c_int), _ptr(xx, C.c_double), rows, cols,
+                    _ptr(Tp, C.c_int), _ptr(Ti, C.c_int), _ptr(Tx, C.c_double), _ptr(work, C.c_int))
+    return Tp, Ti[:nnz], Tx[:nnz]
+
+
+def coalesce(rows, cols, x, m, n):
+    L = port()
+    rows = np.ascontiguousarray(rows, np.int32); cols = np.ascontiguousarray(cols, np.int32)
+    x = np.ascontiguousarray(x, np.float64)
+    nnz = len(rows)
+    Cp = np.zeros(m + 1, np.int32)
+    out = L.orc_coalesce_count(_ptr(rows, C.c_int), _ptr(cols, C.c_int), nnz, m, n, _ptr(Cp, C.c_int))
+    Ci = np.zeros(max(1, out), np.int32)
+    Cx = np.zeros(max(1, out), np.float64)
+    L.orc_coalesce_fill(_ptr(rows, C.c_int), _ptr(cols, C.c_int), _ptr(x, C.c_double), nnz, m, n,
+                        _ptr(Cp, C.c_int), _ptr(Ci, C.c_int), _ptr(Cx, C.c_double))
+    return Cp, Ci[:out], Cx[:out]
+
+
+def row_gather(Ap, Ai, Ax, mp):
+    L = port()
+    Ap = np.ascontiguousarray(Ap, np.int32); Ai = np.ascontiguousarray(Ai, np.int32)
+    Ax = np.ascontiguousarray(Ax, np.float64); mp = np.ascontiguousarray(mp, np.int32)
+    m_out = len(mp)
+    Cp = np.zeros(m_out + 1, np.int32)
+    nnz = L.orc_row_gather_count(_ptr(Ap, C.c_int), _ptr(mp, C.c_int), m_out, _ptr(Cp, C.c_int))
+    Ci = np.zeros(max(1, nnz), np.int32)
+    Cx = np.zeros(max(1, nnz), np.float64)
+    L.orc_row_gather_fill(_ptr(Ap, C.c_int), _ptr(Ai, C.c_int), _ptr(Ax, C.c_double),
+                          _ptr(mp, C.c_int), m_out, _ptr(Cp, C.c_int), _ptr(Ci, C.c_int),
+                          _ptr(Cx, C.c_double))
+    return Cp, Ci[:nnz], Cx[:nnz]
+
+
+def row_reduce(Ap, Ai, Ax, m, n, group, m_out):
+    L = port()
+    Ap = np.ascontiguousarray(Ap, np.int32); Ai = np.ascontiguousarray(Ai, np.int32)
+    Ax = np.ascontiguousarray(Ax, np.float64); group = np.ascontiguousarray(group, np.int32)
+    Cp = np.zeros(m_out + 1, np.int32)
+    nnz = L.orc_row_reduce_count(_ptr(Ap, C.c_int), _ptr(Ai, C.c_int), m, n, _ptr(group, C.c_int),
+                                 m_out, _ptr(Cp, C.c_int))
+    Ci = np.zeros(max(1, nnz), np.int32)
+    Cx = np.zeros(max(1, nnz), np.float64)
+    L.orc_row_reduce_fill(_ptr(Ap, C.c_int), _ptr(Ai, C.c_int), _ptr(Ax, C.c_double), m, n,
+                          _ptr(group, C.c_int), m_out, _ptr(Cp, C.c_int), _ptr(Ci, C.c_int),
+                          _ptr(Cx, C.c_double))
+    return Cp, Ci[:nnz], Cx[:nnz]
+
+
+def btda(A, B_csr, d):
+    """C = B^T diag(d) A with A, B given as CSR tuples (p, i, x, m, n): the port."""
+    Ap, Ai, Ax, m, nA = A
+    Bp, Bi, Bx, mB, nB = B_csr
+    Tp, Ti, Tx = transpose(Bp, Bi, Bx, mB, nB)
+    return gustavson(Tp, Ti, Tx, nB, 1, d, Ap, Ai, Ax, m, nA)
+
+
+def spgemm(A, B):
+    """C = A B (A, B CSR tuples) by the port (L = A's rows)."""
+    Ap, Ai, Ax, mA, nA = A
+    Bp, Bi, Bx, mB, nB = B
+    return gustavson(Ap, Ai, Ax, mA, 1, None, Bp, Bi, Bx, mB, nB)

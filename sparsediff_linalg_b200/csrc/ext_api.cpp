@@ -1,0 +1,213 @@
+// Device-resident extension API (sparsediff_linalg_cuda.h): products, transposes
+// and duplicate coalescing whose operands and results stay in HBM.
+#include <memory>
+
+#include "capi_common.h"
+
+using namespace sdl;
+
+struct sdl_product
+{
+    Product P;
+};
+
+struct sdl_transpose
+{
+    TransposePlan T;
+};
+
+// Coalescing = group triplets by row (stable transpose of the one-entry-per-row
+// structure rows[]), then a unit-valued row-wise product with the triplet matrix
+// (row t = {(cols[t], x[t])}): each output entry sums its duplicates in ascending
+// triplet order, starting from +0.0, as upstream's row_reduce does.
+struct sdl_coalesce
+{
+    int m = 0, n = 0, nnz_in = 0;
+    TransposePlan G;
+    DevBuf<int> Ap, Ai;
+    Product P;
+};
+
+extern "C" int sdl_device_available(void)
+{
+    try
+    {
+        runtime();
+        return 1;
+    }
+    catch (...)
+    {
+        return 0;
+    }
+}
+
+extern "C" unsigned long long sdl_device_alloc_count(void) { return g_dev_allocs.load(); }
+extern "C" unsigned long long sdl_kernel_launch_count(void) { return g_launches.load(); }
+
+extern "C" void *sdl_stream(void)
+{
+    try
+    {
+        return runtime().stream;
+    }
+    catch (...)
+    {
+        return nullptr;
+    }
+}
+
+extern "C" sdl_status sdl_synchronize(void)
+{
+    return guard_status("sdl_synchronize", [&]() { SDL_CUDA(cudaStreamSynchronize(runtime().stream)); });
+}
+
+extern "C" void sdl_free(void *device_ptr) { dev_free(device_ptr); }
+
+// ------------------------------------------------------------------ product
+extern "C" sdl_status sdl_product_create(const sdl_product_desc *desc, void *stream,
+                                         sdl_product **out)
+{
+    return guard_status("sdl_product_create", [&]() {
+        if (!desc || !out) fail(SDL_ERR_INVALID, "NULL argument");
+        *out = nullptr;
+        ProductDesc d;
+        d.Lp = desc->Lp;
+        d.Li = desc->Li;
+        d.L_map = desc->L_map;
+        d.L_m = desc->L_m;
+        d.L_nnz = desc->L_nnz;
+        d.blocks = desc->blocks;
+        d.Ap = desc->Ap;
+        d.Ai = desc->Ai;
+        d.A_m = desc->A_m;
+        d.A_n = desc->A_n;
+        d.A_nnz = desc->A_nnz;
+        if (!d.Lp || !d.Ap) fail(SDL_ERR_INVALID, "NULL structure pointer");
+        auto p = std::make_unique<sdl_product>();
+        product_symbolic(d, TuneConfig{}, p->P, pick_stream(stream));
+        *out = p.release();
+    });
+}
+
+extern "C" sdl_status sdl_product_info(const sdl_product *P, int *m, int *n, int *nnz,
+                                       long long *terms, const int **Cp, const int **Ci)
+{
+    return guard_status("sdl_product_info", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        if (m) *m = P->P.m_out;
+        if (n) *n = P->P.n;
+        if (nnz) *nnz = P->P.nnz;
+        if (terms) *terms = P->P.terms;
+        if (Cp) *Cp = P->P.Cp.get();
+        if (Ci) *Ci = P->P.Ci.get();
+    });
+}
+
+extern "C" sdl_status sdl_product_fill(const sdl_product *P, const double *Lx, const double *d,
+                                       const double *Ax, double *Cx, void *stream)
+{
+    return guard_status("sdl_product_fill", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        if (P->P.nnz > 0 && (!Ax || !Cx)) fail(SDL_ERR_INVALID, "NULL value pointer");
+        product_numeric(P->P, Lx, d, Ax, Cx, pick_stream(stream));
+    });
+}
+
+extern "C" void sdl_product_destroy(sdl_product *P) { delete P; }
+
+// ------------------------------------------------------------------ transpose
+extern "C" sdl_status sdl_transpose_create(const int *p, const int *idx, int rows, int cols, int nnz,
+                                           void *stream, sdl_transpose **out)
+{
+    return guard_status("sdl_transpose_create", [&]() {
+        if (!out) fail(SDL_ERR_INVALID, "NULL argument");
+        *out = nullptr;
+        cudaStream_t s = pick_stream(stream);
+        validate_compressed(p, idx, rows, cols, nnz, "transpose operand", s);
+        auto t = std::make_unique<sdl_transpose>();
+        transpose_build(p, idx, rows, cols, nnz, t->T, s);
+        *out = t.release();
+    });
+}
+
+extern "C" sdl_status sdl_transpose_info(const sdl_transpose *T, const int **Tp, const int **Ti,
+                                         const int **src)
+{
+    return guard_status("sdl_transpose_info", [&]() {
+        if (!T) fail(SDL_ERR_INVALID, "NULL transpose");
+        if (Tp) *Tp = T->T.Tp.get();
+        if (Ti) *Ti = T->T.Ti.get();
+        if (src) *src = T->T.src.get();
+    });
+}
+
+extern "C" sdl_status sdl_transpose_fill(const sdl_transpose *T, const double *x, double *Tx,
+                                         void *stream)
+{
+    return guard_status("sdl_transpose_fill", [&]() {
+        if (!T) fail(SDL_ERR_INVALID, "NULL transpose");
+        gather_values(T->T.src.get(), x, Tx, T->T.nnz, pick_stream(stream));
+    });
+}
+
+extern "C" void sdl_transpose_destroy(sdl_transpose *T) { delete T; }
+
+// ------------------------------------------------------------------ coalesce
+extern "C" sdl_status sdl_coalesce_create(const int *rows, const int *cols, int nnz_in, int m, int n,
+                                          void *stream, sdl_coalesce **out)
+{
+    return guard_status("sdl_coalesce_create", [&]() {
+        if (!out) fail(SDL_ERR_INVALID, "NULL argument");
+        *out = nullptr;
+        if (nnz_in < 0 || m < 0 || n < 0) fail(SDL_ERR_INVALID, "negative size");
+        cudaStream_t s = pick_stream(stream);
+        validate_compressed(nullptr, rows, 0, m, nnz_in, "coalesce rows", s);
+        validate_compressed(nullptr, cols, 0, n, nnz_in, "coalesce cols", s);
+        auto c = std::make_unique<sdl_coalesce>();
+        c->m = m;
+        c->n = n;
+        c->nnz_in = nnz_in;
+        transpose_build(nullptr, rows, nnz_in, m, nnz_in, c->G, s);
+        c->Ap.reset((size_t)nnz_in + 1);
+        fill_iota(c->Ap.get(), nnz_in + 1, s);
+        c->Ai.reset(std::max(1, nnz_in));
+        if (nnz_in)
+            SDL_CUDA(cudaMemcpyAsync(c->Ai.get(), cols, (size_t)nnz_in * sizeof(int),
+                                     cudaMemcpyDeviceToDevice, s));
+        ProductDesc d;
+        d.Lp = c->G.Tp.get();
+        d.Li = c->G.Ti.get();
+        d.L_m = m;
+        d.L_nnz = nnz_in;
+        d.blocks = 1;
+        d.Ap = c->Ap.get();
+        d.Ai = c->Ai.get();
+        d.A_m = nnz_in;
+        d.A_n = n;
+        d.A_nnz = nnz_in;
+        product_symbolic(d, TuneConfig{}, c->P, s);
+        *out = c.release();
+    });
+}
+
+extern "C" sdl_status sdl_coalesce_info(const sdl_coalesce *C, int *nnz_out, const int **Cp,
+                                        const int **Ci)
+{
+    return guard_status("sdl_coalesce_info", [&]() {
+        if (!C) fail(SDL_ERR_INVALID, "NULL plan");
+        if (nnz_out) *nnz_out = C->P.nnz;
+        if (Cp) *Cp = C->P.Cp.get();
+        if (Ci) *Ci = C->P.Ci.get();
+    });
+}
+
+extern "C" sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, double *Cx,
+                                        void *stream)
+{
+    return guard_status("sdl_coalesce_fill", [&]() {
+        if (!C) fail(SDL_ERR_INVALID, "NULL plan");
+        product_numeric(C->P, nullptr, nullptr, x, Cx, pick_stream(stream));
+    });
+}
+
+extern "C" void sdl_coalesce_destroy(sdl_coalesce *C) { delete C; }

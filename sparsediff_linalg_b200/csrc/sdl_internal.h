@@ -1,0 +1,223 @@
+// Internal C++ interface of the B200 sparse-product library.
+//
+// Everything here is device-resident: pointers named d_* or held in DevBuf are
+// device memory on the library's device, and every launch goes to the stream the
+// caller passes (the library stream by default). The C ABI layers (capi_*.cpp,
+// ext_api.cpp) translate host structs and status codes onto these types.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+
+#include "sparsediff_linalg_cuda.h"
+
+namespace sdl {
+
+// ---------------------------------------------------------------- errors
+struct Error : std::runtime_error
+{
+    sdl_status code;
+    Error(sdl_status c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(sdl_status code, const std::string &msg);
+[[noreturn]] void cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define SDL_CUDA(call)                                                                 \
+    do                                                                                 \
+    {                                                                                  \
+        cudaError_t sdl_e_ = (call);                                                   \
+        if (sdl_e_ != cudaSuccess) ::sdl::cuda_fail(sdl_e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+// Every kernel launch of the library goes through this so launches are counted
+// and launch errors surface at the call site.
+extern std::atomic<unsigned long long> g_launches;
+#define SDL_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
+    do                                                                             \
+    {                                                                              \
+        kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                \
+        ::sdl::g_launches.fetch_add(1, std::memory_order_relaxed);                 \
+        SDL_CUDA(cudaGetLastError());                                              \
+    } while (0)
+
+// ---------------------------------------------------------------- runtime
+struct Runtime
+{
+    int device = -1;
+    cudaStream_t stream = nullptr; // library default stream (non-blocking)
+    int num_sms = 0;
+    int smem_optin = 0; // max dynamic shared memory per block (opt-in)
+    int l2_bytes = 0;
+    int *d_error = nullptr; // device error word (kernel-side checks), 0 = ok
+};
+
+// Initialises on first use (device = current device at that moment). Throws
+// Error(SDL_ERR_NO_DEVICE) when no CUDA device is usable.
+Runtime &runtime();
+inline cudaStream_t pick_stream(void *s)
+{
+    return s ? static_cast<cudaStream_t>(s) : runtime().stream;
+}
+
+// Reads and clears the device error word (synchronises the stream).
+int take_device_error(cudaStream_t s);
+
+// ---------------------------------------------------------------- memory
+void *dev_alloc(size_t bytes); // cudaMalloc, counted; throws on failure
+void dev_free(void *p);
+extern std::atomic<unsigned long long> g_dev_allocs;
+
+template <class T>
+struct DevBuf
+{
+    T *ptr = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { reset(count); }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : ptr(o.ptr), n(o.n)
+    {
+        o.ptr = nullptr;
+        o.n = 0;
+    }
+    DevBuf &operator=(DevBuf &&o) noexcept
+    {
+        if (this != &o)
+        {
+            release();
+            ptr = o.ptr;
+            n = o.n;
+            o.ptr = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void reset(size_t count)
+    {
+        release();
+        n = count;
+        if (count) ptr = static_cast<T *>(dev_alloc(count * sizeof(T)));
+    }
+    void release()
+    {
+        if (ptr) dev_free(ptr);
+        ptr = nullptr;
+        n = 0;
+    }
+    T *get() const { return ptr; }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------- primitives
+// out[0] = 0, out[k + 1] = in[0] + ... + in[k]; out has n + 1 entries. Returns the
+// total (synchronises). For the int variant the caller checks the total fits.
+long long exclusive_scan_i64(const long long *d_in, long long *d_out, long long n,
+                             cudaStream_t s);
+// Exclusive scan of int counts into int offsets; fails with SDL_ERR_OVERFLOW if
+// the total exceeds INT_MAX. Returns the total.
+int exclusive_scan_i32_checked(const int *d_in, int *d_out, int n, cudaStream_t s);
+void fill_iota(int *d, int n, cudaStream_t s);
+
+// Validates a compressed structure (p has rows + 1 entries, indices in [0, cols)):
+// p[0] == 0, p non-decreasing, p[rows] == nnz, 0 <= idx < cols. Throws
+// SDL_ERR_INVALID otherwise.
+void validate_compressed(const int *d_p, const int *d_idx, int rows, int cols, int nnz,
+                         const char *what, cudaStream_t s);
+
+// ---------------------------------------------------------------- transpose
+// Stable transpose of a compressed structure (rows x cols, nnz entries): Tp has
+// cols + 1 offsets, Ti the source row of each transposed entry (ascending inside
+// every output row), src the source position of each transposed entry. With
+// d_p == nullptr the source is the "one entry per row" structure p = 0..rows.
+struct TransposePlan
+{
+    int rows = 0, cols = 0, nnz = 0;
+    DevBuf<int> Tp, Ti, src;
+};
+void transpose_build(const int *d_p, const int *d_idx, int rows, int cols, int nnz,
+                     TransposePlan &out, cudaStream_t s);
+// Tx[q] = x[src[q]].
+void gather_values(const int *d_src, const double *d_x, double *d_out, int n,
+                   cudaStream_t s);
+
+// ---------------------------------------------------------------- Gustavson
+// Row classes of the row-wise product. Thresholds are tunable (autotuner).
+enum
+{
+    SYM_W32 = 0,
+    SYM_W128,
+    SYM_W512,
+    SYM_C2K,
+    SYM_C8K,
+    SYM_BITMAP,
+    SYM_NBINS
+};
+enum
+{
+    NUM_W32 = 0,
+    NUM_W128,
+    NUM_W512,
+    NUM_C2K,
+    NUM_C8K,
+    NUM_GMEM,
+    NUM_NBINS
+};
+
+struct TuneConfig
+{
+    // rows whose term count (upper bound of their nnz) is <= warp_cap[k] go to the
+    // warp kernel of capacity class k (32, 128, 512); larger rows go to the CTA
+    // kernels; rows above cta_cap[1] terms are built with the bitmap kernel.
+    int warp_max_terms = 512; // rows above this go to CTA kernels
+    int rows_per_cta_warp = 8; // warps per CTA for the warp kernels
+    int cta_threads_2k = 256;
+    int cta_threads_8k = 512;
+    int gmem_threads = 512;
+};
+
+// Operand description of C = kron(I_blocks, L) diag(d) A.
+struct ProductDesc
+{
+    const int *Lp = nullptr; // L_m + 1
+    const int *Li = nullptr; // column index of each L entry (row of A within a block)
+    const int *L_map = nullptr; // optional: value of L entry ii is Lx[L_map[ii]]
+    int L_m = 0, L_nnz = 0;
+    int blocks = 1;
+    const int *Ap = nullptr, *Ai = nullptr;
+    int A_m = 0, A_n = 0, A_nnz = 0;
+};
+
+struct Product
+{
+    ProductDesc desc;
+    int m_out = 0, n = 0, nnz = 0, n_L = 0;
+    long long terms = 0;
+    DevBuf<int> Cp, Ci;
+    DevBuf<int> num_rows; // row ids grouped by numeric class
+    int num_count[NUM_NBINS] = {0};
+    int num_offset[NUM_NBINS + 1] = {0};
+    DevBuf<int> gmem_scratch; // posmap scratch for NUM_GMEM rows (slots x n ints)
+    int gmem_slots = 0;
+    TuneConfig cfg;
+    // per-row statistics kept for the learned scheduler (optional)
+    DevBuf<long long> row_terms; // ub per row
+};
+
+// Symbolic phase: fills P.Cp, P.Ci, P.nnz and the numeric schedule.
+void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P,
+                      cudaStream_t s, bool keep_row_terms = false);
+// Numeric phase. Lx: values of L (indexed through L_map when set), or nullptr for
+// a unit L (every L value 1.0). d: A_m values or nullptr. Never allocates.
+void product_numeric(const Product &P, const double *Lx, const double *d,
+                     const double *Ax, double *Cx, cudaStream_t s);
+
+} // namespace sdl

@@ -1,0 +1,144 @@
+"""Device-resident wrappers (torch tensors in HBM) over the extension C API.
+
+Torch provides device memory and streams only; every computation is a kernel of
+``libsparsediff_linalg_b200.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from ._lib import check, lib, sdl_product_desc
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class _DevView:
+    """__cuda_array_interface__ over a library-owned device array."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {
+            "shape": (int(n),), "typestr": typestr, "data": (int(ptr or 0), False), "version": 3,
+            "strides": None,
+        }
+
+
+def _as_tensor(ptr, n, typestr="<i4"):
+    if n == 0:
+        return torch.zeros(0, dtype=torch.int32, device="cuda")
+    return torch.as_tensor(_DevView(ptr, n, typestr), device="cuda")
+
+
+class Product:
+    """C = kron(I_blocks, L) diag(d) A with device-resident operands.
+
+    L is given by rows (Lp, Li) over the rows of A (within a block); L_map (optional)
+    makes L's value of entry ii equal Lx[L_map[ii]]. The structure tensors must stay
+    alive (they are referenced, not copied)."""
+
+    def __init__(self, Lp, Li, Ap, Ai, A_n, L_map=None, blocks=1, stream=None):
+        L = lib()
+        self._keep = (Lp, Li, Ap, Ai, L_map)
+        desc = sdl_product_desc(
+            _ptr(Lp).value, _ptr(Li).value, _ptr(L_map).value if L_map is not None else None,
+            Lp.numel() - 1, Li.numel(), blocks, _ptr(Ap).value, _ptr(Ai).value,
+            Ap.numel() - 1, A_n, Ai.numel())
+        h = C.c_void_p()
+        check(L.sdl_product_create(C.byref(desc), _stream(stream), C.byref(h)))
+        self.handle = h
+        m, n, nnz = C.c_int(), C.c_int(), C.c_int()
+        terms = C.c_longlong()
+        cp, ci = C.c_void_p(), C.c_void_p()
+        check(L.sdl_product_info(h, C.byref(m), C.byref(n), C.byref(nnz), C.byref(terms),
+                                 C.byref(cp), C.byref(ci)))
+        self.m, self.n, self.nnz, self.terms = m.value, n.value, nnz.value, terms.value
+        self.Cp = _as_tensor(cp.value, self.m + 1)
+        self.Ci = _as_tensor(ci.value, self.nnz)
+
+    def fill(self, Lx, d, Ax, Cx, stream=None):
+        check(lib().sdl_product_fill(self.handle, _ptr(Lx), _ptr(d), _ptr(Ax), _ptr(Cx),
+                                     _stream(stream)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().sdl_product_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class Transpose:
+    """Stable transpose plan of a device compressed structure (rows x cols)."""
+
+    def __init__(self, p, idx, rows, cols, stream=None):
+        L = lib()
+        self._keep = (p, idx)
+        h = C.c_void_p()
+        nnz = idx.numel()
+        check(L.sdl_transpose_create(_ptr(p), _ptr(idx), rows, cols, nnz, _stream(stream), C.byref(h)))
+        self.handle = h
+        tp, ti, src = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(L.sdl_transpose_info(h, C.byref(tp), C.byref(ti), C.byref(src)))
+        self.nnz = nnz
+        self.Tp = _as_tensor(tp.value, cols + 1)
+        self.Ti = _as_tensor(ti.value, nnz)
+        self.src = _as_tensor(src.value, nnz)
+
+    def fill(self, x, Tx, stream=None):
+        check(lib().sdl_transpose_fill(self.handle, _ptr(x), _ptr(Tx), _stream(stream)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().sdl_transpose_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+class Coalesce:
+    """Duplicate-coalescing plan of device COO triplets (rows, cols) into an m x n CSR."""
+
+    def __init__(self, rows, cols, m, n, stream=None):
+        L = lib()
+        h = C.c_void_p()
+        check(L.sdl_coalesce_create(_ptr(rows), _ptr(cols), rows.numel(), m, n, _stream(stream),
+                                    C.byref(h)))
+        self.handle = h
+        nnz = C.c_int()
+        cp, ci = C.c_void_p(), C.c_void_p()
+        check(L.sdl_coalesce_info(h, C.byref(nnz), C.byref(cp), C.byref(ci)))
+        self.m, self.n, self.nnz = m, n, nnz.value
+        self.Cp = _as_tensor(cp.value, m + 1)
+        self.Ci = _as_tensor(ci.value, self.nnz)
+
+    def fill(self, x, Cx, stream=None):
+        check(lib().sdl_coalesce_fill(self.handle, _ptr(x), _ptr(Cx), _stream(stream)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().sdl_coalesce_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def btda_product(A_p, A_i, A_n, B_p, B_i, B_n, stream=None):
+    """Device plan of C = B^T D A with A, B given as device CSR structures: B's CSC is
+    built by a transpose plan and its values are read through the CSR positions
+    (no CSC value refresh). Returns (product, transpose)."""
+    m = A_p.numel() - 1
+    T = Transpose(B_p, B_i, m, B_n, stream=stream)
+    P = Product(T.Tp, T.Ti, A_p, A_i, A_n, L_map=T.src, stream=stream)
+    return P, T

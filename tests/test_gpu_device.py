@@ -1,0 +1,85 @@
+"""GPU parity of the device-resident extension API (operands in HBM, torch tensors
+for memory only) against the CPU oracle, bit for bit."""
+import numpy as np
+import pytest
+
+from sparsediff_linalg_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.int64)
+
+
+def T(a, dtype=None):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda", dtype=dtype)
+
+
+def test_btda_device_fused_csc(sdl, orc):
+    """B's values are read through the CSC->CSR position map (no CSC refresh)."""
+    import torch
+    from sparsediff_linalg_b200.device import btda_product
+    rng = np.random.default_rng(21)
+    A = wl.fixed_rowlen_csr(5000, 3000, 8, rng)
+    B = wl.fixed_rowlen_csr(5000, 2500, 8, rng)
+    d = rng.uniform(0.1, 10, 5000)
+    P, Tr = btda_product(T(A[0]), T(A[1]), A[4], T(B[0]), T(B[1]), B[4])
+    Cx = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    P.fill(T(B[2]), T(d), T(A[2]), Cx)
+    torch.cuda.synchronize()
+    wp, wi, wx = orc.btda(A, B, d)
+    assert np.array_equal(P.Cp.cpu().numpy(), wp) and np.array_equal(P.Ci.cpu().numpy(), wi)
+    assert np.array_equal(bits(Cx.cpu().numpy()), bits(wx))
+
+
+def test_kron_blocks(sdl, orc):
+    import torch
+    from sparsediff_linalg_b200.device import Product
+    rng = np.random.default_rng(5)
+    blocks, nL, mL, n = 4, 50, 40, 60
+    Lp, Li, Lx, _, _ = wl.small_random_csr(mL, nL, 0.1, rng)
+    A = wl.small_random_csr(blocks * nL, n, 0.1, rng)
+    d = rng.uniform(0.5, 2, blocks * nL)
+    P = Product(T(Lp), T(Li), T(A[0]), T(A[1]), n, blocks=blocks)
+    Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda")
+    P.fill(T(Lx), T(d), T(A[2]), Cx)
+    torch.cuda.synchronize()
+    wp, wi, wx = orc.gustavson(Lp, Li, Lx, mL, blocks, d, A[0], A[1], A[2], A[3], A[4])
+    assert np.array_equal(P.Cp.cpu().numpy(), wp) and np.array_equal(P.Ci.cpu().numpy(), wi)
+    assert np.array_equal(bits(Cx[:P.nnz].cpu().numpy()), bits(wx))
+
+
+def test_unit_L_product_is_row_reduce(sdl, orc):
+    """A unit-valued L (no Lx) is upstream's row_reduce: C[g] = sum of rows with group g."""
+    import torch
+    from sparsediff_linalg_b200.device import Product, Transpose
+    rng = np.random.default_rng(8)
+    m, n, m_out = 3000, 700, 300
+    A = wl.small_random_csr(m, n, 0.01, rng)
+    group = rng.integers(0, m_out, m).astype(np.int32)
+    G = Transpose(T(np.arange(m + 1, dtype=np.int32)), T(group), m, m_out)
+    P = Product(G.Tp, G.Ti, T(A[0]), T(A[1]), n)
+    Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda")
+    P.fill(None, None, T(A[2]), Cx)
+    torch.cuda.synchronize()
+    wp, wi, wx = orc.row_reduce(A[0], A[1], A[2], m, n, group, m_out)
+    assert np.array_equal(P.Cp.cpu().numpy(), wp) and np.array_equal(P.Ci.cpu().numpy(), wi)
+    assert np.array_equal(bits(Cx[:P.nnz].cpu().numpy()), bits(wx))
+
+
+@pytest.mark.slow
+def test_btda_full_size_config(sdl, orc):
+    """The 100000 x 50000 / 100000 x 40000, 8-per-row configuration at full size."""
+    import torch
+    from sparsediff_linalg_b200.device import btda_product
+    A, B, d = wl.btda(seed=1)
+    P, Tr = btda_product(T(A[0]), T(A[1]), A[4], T(B[0]), T(B[1]), B[4])
+    Cx = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    P.fill(T(B[2]), T(d), T(A[2]), Cx)
+    torch.cuda.synchronize()
+    wp, wi, wx = orc.btda(A, B, d)
+    assert P.nnz == len(wi)
+    assert np.array_equal(P.Cp.cpu().numpy(), wp) and np.array_equal(P.Ci.cpu().numpy(), wi)
+    assert np.array_equal(bits(Cx.cpu().numpy()), bits(wx))
