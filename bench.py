@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark of the B^T D A / SpGEMM hot path on B200.
+
+Workload (one "step"): a value refill of C = B^T diag(d) A with a cached pattern,
+A 100000 x 50000 and B 100000 x 40000 CSR FP64 with 8 distinct uniform columns per
+row (N(0,1) values), d ~ U[0.1, 10]; C is 40000 x 50000 with ~6.39M entries. This is
+the configuration the headline metric is quoted on; SparseDiffEngine re-evaluates
+the same pattern with new values, so every step brings new A, B and d values.
+
+  value   algorithmic HBM GB/s of the device-resident refill (inputs in HBM),
+          L2 flushed between timed steps, CUDA events on the launching stream,
+          max over ranks (N > 1 runs one independent product per rank: weak scaling)
+  e2e     the same metric through the upstream C ABI with host buffers
+          (BTDA_matrices_fill_values on sparse matrix handles: the host->device
+          copies of A.x, B.x and d and the device->host copy of C.x are inside the
+          timed region)
+  roofline / cpu_baseline / clocks / gpu_launches: see the JSON keys.
+
+``--impl reference`` times the upstream CPU implementation (compiled from its own
+sources by oracle/Makefile) on the same workload on the host cores (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="budget of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def algorithmic_bytes_refill(nnzA, mA, nnzL, nL, len_d, nnzC, mC):
+    """Bytes a refill must move at least once (int32 = 4 B, FP64 = 8 B):
+    A (x, i, p), L = CSC of B (row indices, CSR positions of the entries and B's
+    values read through them, column offsets), d, C (read C.i, write C.x) and C.p."""
+    return (12 * nnzA + 4 * (mA + 1) + 16 * nnzL + 4 * (nL + 1) + 8 * len_d
+            + 12 * nnzC + 4 * (mC + 1))
+
+
+class Clocks:
+    """nvidia-smi sampler running while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_barrier(world):
+    import torch
+    import torch.distributed as dist
+    if world <= 1:
+        return (lambda: None), (lambda v: v)
+    import datetime
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        dist.barrier()
+
+    def allmax(v):
+        t = torch.tensor([float(v)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return barrier, allmax
+
+
+# ---------------------------------------------------------------- reference arm
+def reference_btda_times(A, B, d, A2x, B2x, d2, reps):
+    from oracle import oracle
+    lib_path = oracle.REF_DIR / "libsdl_reftime.so"
+    if not lib_path.exists():
+        raise RuntimeError("upstream timing library not built")
+    L = C.CDLL(str(lib_path))
+    ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+    L.ref_time_btda.argtypes = [ip, ip, dp, dp, C.c_int, C.c_int, ip, ip, dp, dp, C.c_int, dp, dp,
+                                C.c_int, dp]
+    L.ref_time_btda.restype = None
+    c = lambda a, t: np.ascontiguousarray(a).ctypes.data_as(C.POINTER(t))  # noqa: E731
+    keep = [np.ascontiguousarray(a) for a in (A[0], A[1], A[2], A2x, B[0], B[1], B[2], B2x, d, d2)]
+    out = np.zeros(3)
+    L.ref_time_btda(c(keep[0], C.c_int), c(keep[1], C.c_int), c(keep[2], C.c_double),
+                    c(keep[3], C.c_double), A[3], A[4], c(keep[4], C.c_int), c(keep[5], C.c_int),
+                    c(keep[6], C.c_double), c(keep[7], C.c_double), B[4], c(keep[8], C.c_double),
+                    c(keep[9], C.c_double), reps, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out  # alloc s, refill s, nnz
+
+
+def reference_spgemm_times(A, B, reps):
+    from oracle import oracle
+    L = C.CDLL(str(oracle.REF_DIR / "libsdl_reftime.so"))
+    ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+    L.ref_time_spgemm.argtypes = [ip, ip, dp, C.c_int, C.c_int, ip, ip, dp, C.c_int, C.c_int, dp]
+    L.ref_time_spgemm.restype = None
+    keep = [np.ascontiguousarray(a) for a in (A[0], A[1], A[2], B[0], B[1], B[2])]
+    c = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    out = np.zeros(3)
+    L.ref_time_spgemm(c(keep[0], C.c_int), c(keep[1], C.c_int), c(keep[2], C.c_double), A[3], A[4],
+                      c(keep[3], C.c_int), c(keep[4], C.c_int), c(keep[5], C.c_double), B[4], reps,
+                      out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def workload():
+    from sparsediff_linalg_b200 import workloads as wl
+    A, B, d = wl.btda(seed=1)
+    rng = np.random.default_rng(2)
+    A2x = rng.standard_normal(len(A[1]))
+    B2x = rng.standard_normal(len(B[1]))
+    d2 = rng.uniform(0.1, 10.0, A[3])
+    return A, B, d, A2x, B2x, d2
+
+
+WORKLOAD_NAME = ("btda_refill: C = B^T diag(d) A, A 100000x50000, B 100000x40000 CSR FP64, "
+                 "8 nnz/row uniform, values N(0,1), d U[0.1,10], new A/B/d values every step")
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    A, B, d, A2x, B2x, d2 = workload()
+    nnzC_est = None
+    # one step = one upstream refill (CSC mirror refresh + planned fill); warmup first
+    t_alloc = None
+    times = []
+    for phase, reps in (("warmup", max(1, args.warmup)), ("timed", args.steps)):
+        out = reference_btda_times(A, B, d, A2x, B2x, d2, reps)
+        t_alloc, t_step, nnzC_est = out
+        if phase == "timed":
+            times.append(t_step)
+    t_step = times[0]
+    nnzC = int(nnzC_est)
+    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], nnzC, B[4])
+    gbs = B_alg / t_step / 1e9
+    line = {
+        "impl": "reference", "metric": "btda_refill_hbm_gbs", "value": round(gbs, 3), "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t_step * 1e3, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD_NAME, "nnz_C": nnzC},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} upstream BTDA_matrices_fill_values refills "
+                                   f"(A, B, d changed each time) on one host core"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "reference_alloc_ms": round(t_alloc * 1e3, 3),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- b200 arm
+def run_b200(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    barrier, allmax = make_barrier(world)
+    from sparsediff_linalg_b200 import lib
+    from sparsediff_linalg_b200.device import btda_product, Product
+    L = lib()
+    assert L.sdl_device_available() == 1, "CUDA library cannot use the device"
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    A, B, d, A2x, B2x, d2 = workload()
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
+    Ap, Ai, Bp, Bi = T(A[0]), T(A[1]), T(B[0]), T(B[1])
+    sets = [(T(A[2]), T(B[2]), T(d)), (T(A2x), T(B2x), T(d2))]
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    P, Tr = btda_product(Ap, Ai, A[4], Bp, Bi, B[4])
+    torch.cuda.synchronize()
+    symbolic_ms = (time.perf_counter() - t0) * 1e3
+    Cx = torch.empty(P.nnz, dtype=torch.float64, device=dev)
+    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], P.nnz, B[4])
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    for w in range(args.warmup):
+        ax, bx, dd = sets[w % 2]
+        P.fill(bx, dd, ax, Cx, stream=stream)
+    torch.cuda.synchronize()
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    clk = Clocks(local)
+    clk.start()
+    launches0 = L.sdl_kernel_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        ax, bx, dd = sets[k % 2]
+        flush.zero_()
+        evs[k][0].record(stream)
+        P.fill(bx, dd, ax, Cx, stream=stream)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = L.sdl_kernel_launch_count() - launches0
+    clocks = clk.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    mean_ms = sum(step_ms) / len(step_ms)
+    mean_ms_max = allmax(mean_ms)
+    value = world * B_alg / (mean_ms_max * 1e-3) / 1e9
+
+    peak, peak_kind = peaks()
+    achieved = B_alg / (mean_ms * 1e-3) / 1e9
+    traffic = None
+    tj = ROOT / "profiles" / "btda_refill_traffic.json"
+    if tj.exists():
+        traffic = json.loads(tj.read_text()).get("dram_bytes_per_launch")
+
+    # ---- SpGEMM 2000x2000, 5 per row (launch-bound case): symbolic + numeric times
+    from sparsediff_linalg_b200 import workloads as wl
+    SA, SB = wl.spgemm_small(seed=0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    SP = Product(T(SA[0]), T(SA[1]), T(SB[0]), T(SB[1]), SB[4])
+    torch.cuda.synchronize()
+    sp_sym_ms = (time.perf_counter() - t0) * 1e3
+    SCx = torch.empty(max(1, SP.nnz), dtype=torch.float64, device=dev)
+    sax, sbx = T(SA[2]), T(SB[2])
+    for _ in range(3):
+        SP.fill(sax, None, sbx, SCx, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(50):
+        SP.fill(sax, None, sbx, SCx, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sp_num_us = e0.elapsed_time(e1) / 50 * 1e3
+
+    # ---- e2e through the upstream C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world)
+
+    line = {
+        "metric": "btda_refill_hbm_gbs", "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(mean_ms_max, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD_NAME, "nnz_C": P.nnz, "terms": P.terms,
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"{world} independent products (one per GPU)" if world > 1 else "1 GPU"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_kind": f"{peak_kind} (copy bandwidth)",
+                     "algorithmic_bytes": B_alg,
+                     "kernel": "numeric refill (all row-class launches of one step)"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "symbolic_ms": round(symbolic_ms, 3),
+        "spgemm_2000": {"symbolic_ms": round(sp_sym_ms, 3), "numeric_us": round(sp_num_us, 2),
+                        "nnz_C": SP.nnz},
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world):
+    """The metric through BTDA_matrices_fill_values on sparse matrix handles with
+    host value buffers (upstream API, what SparseDiffEngine calls)."""
+    import torch
+    from sparsediff_linalg_b200 import lib
+    from sparsediff_linalg_b200.matrices import SparseMatrix
+    L = lib()
+    Am = SparseMatrix.from_csr(*A)
+    Bm = SparseMatrix.from_csr(*B)
+    Cm = Am.BTA_alloc_with(Bm)
+    vals = [(A[2], B[2], np.ascontiguousarray(d)), (A2x, B2x, np.ascontiguousarray(d2))]
+    for w in range(args.warmup):
+        ax, bx, dd = vals[w % 2]
+        Am.set_values(ax)
+        Bm.set_values(bx)
+        Cm.BTDA_fill(Am, dd, Bm)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        ax, bx, dd = vals[k % 2]
+        Am.set_values(ax)       # host write + matrix_values_changed, as a caller does
+        Bm.set_values(bx)
+        Cm.BTDA_fill(Am, dd, Bm)  # returns with C.x current on the host
+    t = (time.perf_counter() - t0) / args.steps
+    t = allmax(t)
+    h2d = 8 * (len(A[1]) + len(B[1]) + A[3])
+    d2h = 8 * Cm.nnz
+    return {"value": round(world * B_alg / t / 1e9, 3), "unit": "GB/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": round(t * 1e3, 4),
+            "api": "BTDA_matrices_fill_values (host buffers, pageable)"}
+
+
+def cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg):
+    try:
+        # estimate the refill time with a couple of reps, then size the sample
+        est = reference_btda_times(A, B, d, A2x, B2x, d2, 2)[1]
+        reps = int(max(3, min(500, args.cpu_seconds / max(est, 1e-4))))
+        out = reference_btda_times(A, B, d, A2x, B2x, d2, reps)
+        return {"value": round(B_alg / out[1] / 1e9, 4), "unit": "GB/s", "cores": 1,
+                "kind": "reference", "ms_per_step": round(out[1] * 1e3, 3),
+                "alloc_ms": round(out[0] * 1e3, 2), "host_cores": os.cpu_count(),
+                "sample": f"{reps} refills of the same workload by the upstream library "
+                          f"(BTDA_matrices_fill_values), single-threaded"}
+    except Exception as e:  # the port is the fallback checker
+        return {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_b200(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

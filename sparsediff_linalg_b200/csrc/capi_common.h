@@ -90,15 +90,27 @@ sdl_status guard_status(const char *fn, F &&f)
     }
 }
 
+// Host arrays allocated by this library's constructors (new_CSR_matrix, ...) are
+// page-locked in place (cudaHostRegister) the first time a large transfer touches
+// them, so copies run at full link speed; they are unregistered before the library
+// frees or reallocates them. Arrays the caller allocated are never registered.
+void host_track(void *p, size_t bytes);
+void host_untrack(void *p);
+void host_pin_if_owned(const void *p, size_t bytes);
+
 template <class T>
 void h2d(T *dst, const T *src, size_t count, cudaStream_t s)
 {
-    if (count) SDL_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    if (!count) return;
+    host_pin_if_owned(src, count * sizeof(T));
+    SDL_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 template <class T>
 void d2h(T *dst, const T *src, size_t count, cudaStream_t s)
 {
-    if (count) SDL_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+    if (!count) return;
+    host_pin_if_owned(dst, count * sizeof(T));
+    SDL_CUDA(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s));
 }
 template <class T>
 DevBuf<T> upload(const T *src, size_t count, cudaStream_t s)

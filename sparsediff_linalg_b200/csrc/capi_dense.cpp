@@ -1,0 +1,282 @@
+// permuted_dense and stacked_pd kinds (upstream src/permuted_dense/permuted_dense.c,
+// src/stacked_pd/stacked_pd.c): constructors, destructors, CSR views and the
+// product dispatch for operand pairs that involve a dense-block kind.
+#include <climits>
+#include <cstring>
+
+#include "capi_common.h"
+#include "matrix_kinds.h"
+#include "sparsediff_linalg/matrix.h"
+#include "sparsediff_linalg/tracked_alloc.h"
+
+namespace sdl {
+
+struct PdImpl
+{
+};
+struct SpdImpl
+{
+};
+
+namespace {
+
+// CSR pattern of row-disjoint dense blocks (upstream permuted_dense.c:344-385):
+// each dense row contributes a copy of its block's col_perm.
+void blocks_csr_pattern(permuted_dense *const *blocks, int n_blocks, int m, int *Cp, int *Ci)
+{
+    std::memset(Cp, 0, ((size_t)m + 1) * sizeof(int));
+    for (int k = 0; k < n_blocks; ++k)
+        for (int ii = 0; ii < blocks[k]->m0; ++ii) Cp[blocks[k]->row_perm[ii] + 1] = blocks[k]->n0;
+    for (int r = 0; r < m; ++r) Cp[r + 1] += Cp[r];
+    for (int k = 0; k < n_blocks; ++k)
+        for (int ii = 0; ii < blocks[k]->m0; ++ii)
+            if (blocks[k]->n0)
+                std::memcpy(Ci + Cp[blocks[k]->row_perm[ii]], blocks[k]->col_perm,
+                            (size_t)blocks[k]->n0 * sizeof(int));
+}
+
+CSR_matrix *pd_to_csr(matrix *self)
+{
+    permuted_dense *pd = as_pd(self);
+    if (!pd->csr_cache)
+    {
+        CSR_matrix *C = new_CSR_matrix(pd->base.m, pd->base.n, pd->m0 * pd->n0);
+        sp_free(C->x);
+        C->x = pd->X; // values alias the block (upstream permuted_dense.c:314-330)
+        permuted_dense *one = pd;
+        blocks_csr_pattern(&one, 1, pd->base.m, C->p, C->i);
+        pd->csr_cache = C;
+    }
+    return pd->csr_cache;
+}
+
+matrix *unsupported_gather(const matrix *, const int *, int)
+{
+    return guard_upstream<matrix *>("row_gather_alloc", nullptr, []() -> matrix * {
+        fail(SDL_ERR_UNSUPPORTED, "row_gather of dense-block kinds is not provided by this build");
+    });
+}
+void unsupported_fill(const matrix *, matrix *)
+{
+    guard_upstream_void("fill", []() {
+        fail(SDL_ERR_UNSUPPORTED, "operation not provided by this build for dense-block kinds");
+    });
+}
+matrix *unsupported_reduce(const matrix *, const int *, int)
+{
+    return guard_upstream<matrix *>("row_reduce_alloc", nullptr, []() -> matrix * {
+        fail(SDL_ERR_UNSUPPORTED, "row_reduce of dense-block kinds is not provided by this build");
+    });
+}
+
+void wire_pd(permuted_dense *pd)
+{
+    pd->base.kind = MATRIX_PERMUTED_DENSE;
+    pd->base.to_csr = pd_to_csr;
+    pd->base.row_gather_alloc = unsupported_gather;
+    pd->base.row_gather_fill_values = unsupported_fill;
+    pd->base.row_reduce_alloc = unsupported_reduce;
+    pd->base.row_reduce_fill_values = unsupported_fill;
+}
+
+CSR_matrix *spd_to_csr(matrix *self)
+{
+    sdl_stacked *spd = as_spd(self);
+    if (!spd->csr_cache)
+    {
+        CSR_matrix *C = new_CSR_matrix(spd->base.m, spd->base.n, spd->base.nnz);
+        blocks_csr_pattern(spd->blocks, spd->n_blocks, spd->base.m, C->p, C->i);
+        spd->csr_cache = C;
+    }
+    // values: scatter the blocks' rows (upstream stacked_pd.c:65-86 refreshes iff
+    // the version moved; the copy is cheap and always current here)
+    CSR_matrix *C = spd->csr_cache;
+    for (int k = 0; k < spd->n_blocks; ++k)
+    {
+        permuted_dense *b = spd->blocks[k];
+        for (int ii = 0; ii < b->m0; ++ii)
+            if (b->n0)
+                std::memcpy(C->x + C->p[b->row_perm[ii]], b->X + (size_t)ii * b->n0,
+                            (size_t)b->n0 * sizeof(double));
+    }
+    return C;
+}
+
+void wire_spd(sdl_stacked *spd)
+{
+    spd->base.kind = MATRIX_STACKED_PD;
+    spd->base.to_csr = spd_to_csr;
+    spd->base.row_gather_alloc = unsupported_gather;
+    spd->base.row_gather_fill_values = unsupported_fill;
+    spd->base.row_reduce_alloc = unsupported_reduce;
+    spd->base.row_reduce_fill_values = unsupported_fill;
+}
+
+[[noreturn]] void unsupported(const char *what)
+{
+    fail(SDL_ERR_UNSUPPORTED, std::string(what) +
+                                  ": this operand-kind combination is not provided by the B200 build");
+}
+
+} // namespace
+
+void pd_free(permuted_dense *pd)
+{
+    sp_free(pd->row_perm);
+    sp_free(pd->col_perm);
+    sp_free(pd->row_inv);
+    sp_free(pd->col_inv);
+    if (pd->csr_cache)
+    {
+        pd->csr_cache->x = nullptr;
+        free_CSR_matrix(pd->csr_cache);
+    }
+    if (pd->owns_X) sp_free(pd->X);
+    delete pd->impl;
+    sp_free(pd);
+}
+
+void spd_free(sdl_stacked *spd)
+{
+    for (int k = 0; k < spd->n_blocks; ++k) free_matrix(&spd->blocks[k]->base);
+    sp_free(spd->blocks);
+    sp_free(spd->src_block_idx_p);
+    sp_free(spd->src_block_idx);
+    free_CSR_matrix(spd->csr_cache);
+    sp_free(spd->values);
+    delete spd->impl;
+    sp_free(spd);
+}
+
+matrix *pd_copy_sparsity(const permuted_dense *A)
+{
+    return new_permuted_dense(A->base.m, A->base.n, A->m0, A->n0, A->row_perm, A->col_perm, nullptr);
+}
+
+matrix *spd_copy_sparsity(const sdl_stacked *A)
+{
+    permuted_dense **blocks = (permuted_dense **)sp_malloc(sizeof(permuted_dense *) * std::max(1, A->n_blocks));
+    for (int k = 0; k < A->n_blocks; ++k) blocks[k] = as_pd(pd_copy_sparsity(A->blocks[k]));
+    matrix *C = new_stacked_pd(A->base.m, A->base.n, A->n_blocks, blocks, A->src_block_idx_p,
+                               A->src_block_idx);
+    sp_free(blocks);
+    return C;
+}
+
+matrix *dense_BTA_alloc(matrix *, matrix *) { unsupported("BTA_matrices_alloc"); }
+void dense_BTDA_fill(matrix *, const double *, matrix *, matrix *) { unsupported("BTDA_matrices_fill_values"); }
+matrix *dense_BA_alloc(const matrix *, matrix *) { unsupported("BA_matrices_alloc"); }
+void dense_BA_fill(const matrix *, const matrix *, matrix *) { unsupported("BA_matrices_fill_values"); }
+matrix *dense_ATA_alloc(matrix *) { unsupported("ATA_matrices_alloc"); }
+void dense_ATDA_fill(const matrix *, const double *, matrix *) { unsupported("ATDA_matrices_fill_values"); }
+void dense_DA_fill(const double *, const matrix *, matrix *) { unsupported("DA_matrices_fill_values"); }
+matrix *dense_transpose_alloc(const matrix *) { unsupported("transpose_matrices_alloc"); }
+void dense_transpose_fill(const matrix *, matrix *) { unsupported("transpose_matrices_fill_values"); }
+
+} // namespace sdl
+
+using namespace sdl;
+
+extern "C" matrix *new_permuted_dense(int m, int n, int m0, int n0, const int *row_perm,
+                                      const int *col_perm, const double *X_data)
+{
+    return guard_upstream<matrix *>("new_permuted_dense", nullptr, [&]() -> matrix * {
+        if (m < 0 || n < 0 || m0 < 0 || n0 < 0 || m0 > m || n0 > n)
+            fail(SDL_ERR_INVALID, "bad block shape");
+        for (int ii = 1; ii < m0; ++ii)
+            if (row_perm[ii] <= row_perm[ii - 1]) fail(SDL_ERR_INVALID, "row_perm must be strictly increasing");
+        for (int jj = 1; jj < n0; ++jj)
+            if (col_perm[jj] <= col_perm[jj - 1]) fail(SDL_ERR_INVALID, "col_perm must be strictly increasing");
+        if (m0 > 0 && (row_perm[0] < 0 || row_perm[m0 - 1] >= m)) fail(SDL_ERR_INVALID, "row_perm out of range");
+        if (n0 > 0 && (col_perm[0] < 0 || col_perm[n0 - 1] >= n)) fail(SDL_ERR_INVALID, "col_perm out of range");
+        if (m0 > 0 && n0 > INT_MAX / m0)
+            fail(SDL_ERR_OVERFLOW, "dense block m0 * n0 exceeds INT_MAX"); // upstream permuted_dense.c:258-262
+        permuted_dense *pd = (permuted_dense *)sp_calloc(1, sizeof(permuted_dense));
+        pd->base.m = m;
+        pd->base.n = n;
+        pd->base.nnz = m0 * n0;
+        pd->m0 = m0;
+        pd->n0 = n0;
+        pd->row_perm = (int *)sp_malloc(sizeof(int) * std::max(1, m0));
+        pd->col_perm = (int *)sp_malloc(sizeof(int) * std::max(1, n0));
+        pd->row_inv = (int *)sp_malloc(sizeof(int) * std::max(1, m));
+        pd->col_inv = (int *)sp_malloc(sizeof(int) * std::max(1, n));
+        pd->X = (double *)sp_malloc(sizeof(double) * std::max(1, m0 * n0));
+        pd->owns_X = true;
+        pd->base.x = pd->X;
+        if (m0) std::memcpy(pd->row_perm, row_perm, sizeof(int) * m0);
+        if (n0) std::memcpy(pd->col_perm, col_perm, sizeof(int) * n0);
+        for (int i = 0; i < m; ++i) pd->row_inv[i] = -1;
+        for (int j = 0; j < n; ++j) pd->col_inv[j] = -1;
+        for (int ii = 0; ii < m0; ++ii) pd->row_inv[row_perm[ii]] = ii;
+        for (int jj = 0; jj < n0; ++jj) pd->col_inv[col_perm[jj]] = jj;
+        if (X_data && m0 * n0) std::memcpy(pd->X, X_data, sizeof(double) * m0 * n0);
+        pd->impl = new PdImpl();
+        wire_pd(pd);
+        return &pd->base;
+    });
+}
+
+extern "C" matrix *new_permuted_dense_full(int m, int n, const double *data)
+{
+    std::vector<int> rp(std::max(1, m)), cp(std::max(1, n));
+    for (int i = 0; i < m; ++i) rp[i] = i;
+    for (int j = 0; j < n; ++j) cp[j] = j;
+    return new_permuted_dense(m, n, m, n, rp.data(), cp.data(), data);
+}
+
+extern "C" matrix *new_stacked_pd(int m, int n, int n_blocks, permuted_dense **blocks,
+                                  const int *src_block_idx_p, const int *src_block_idx)
+{
+    return guard_upstream<matrix *>("new_stacked_pd", nullptr, [&]() -> matrix * {
+        if ((src_block_idx_p == nullptr) != (src_block_idx == nullptr))
+            fail(SDL_ERR_INVALID, "src_block_idx_p and src_block_idx must both be set or both NULL");
+        sdl_stacked *spd = (sdl_stacked *)sp_calloc(1, sizeof(sdl_stacked));
+        spd->base.m = m;
+        spd->base.n = n;
+        long long nnz = 0;
+        for (int k = 0; k < n_blocks; ++k) nnz += blocks[k]->base.nnz;
+        if (nnz > INT_MAX) fail(SDL_ERR_OVERFLOW, "stacked_pd nnz exceeds INT_MAX");
+        spd->base.nnz = (int)nnz;
+        spd->n_blocks = n_blocks;
+        spd->blocks = (permuted_dense **)sp_malloc(sizeof(permuted_dense *) * std::max(1, n_blocks));
+        if (n_blocks) std::memcpy(spd->blocks, blocks, sizeof(permuted_dense *) * n_blocks);
+        spd->src_block_idx_p = (int *)sp_malloc(sizeof(int) * (n_blocks + 1));
+        spd->src_block_idx_p[0] = 0;
+        if (!src_block_idx_p)
+        {
+            spd->src_block_idx = (int *)sp_malloc(sizeof(int) * std::max(1, n_blocks));
+            for (int k = 0; k < n_blocks; ++k)
+            {
+                spd->src_block_idx_p[k + 1] = k + 1;
+                spd->src_block_idx[k] = k;
+            }
+        }
+        else
+        {
+            int total = src_block_idx_p[n_blocks];
+            std::memcpy(spd->src_block_idx_p, src_block_idx_p, sizeof(int) * (n_blocks + 1));
+            spd->src_block_idx = (int *)sp_malloc(sizeof(int) * std::max(1, total));
+            if (total) std::memcpy(spd->src_block_idx, src_block_idx, sizeof(int) * total);
+        }
+        // one shared block-major value buffer (upstream stacked_pd.c:303-319)
+        spd->values = (double *)sp_malloc(sizeof(double) * std::max<long long>(1, nnz));
+        spd->base.x = spd->values;
+        long long off = 0;
+        for (int k = 0; k < n_blocks; ++k)
+        {
+            permuted_dense *b = spd->blocks[k];
+            int bn = b->base.nnz;
+            if (bn == 0) continue;
+            std::memcpy(spd->values + off, b->X, sizeof(double) * bn);
+            if (b->owns_X) sp_free(b->X);
+            b->X = spd->values + off;
+            b->base.x = b->X;
+            b->owns_X = false;
+            off += bn;
+        }
+        spd->impl = new SpdImpl();
+        wire_spd(spd);
+        return &spd->base;
+    });
+}

@@ -181,6 +181,55 @@ void run_transpose_fill(TransposeRawPlan *plan, const double *x, double *out)
 
 void raw_forget(const void *obj) { drop_plan(obj); }
 
+// ------------------------------------------------------------------ pinning
+namespace {
+struct HostArr
+{
+    size_t bytes = 0;
+    int state = 0; // 0 = pageable, 1 = registered, 2 = registration refused
+};
+std::mutex g_pin_mu;
+std::unordered_map<const void *, HostArr> g_host;
+constexpr size_t PIN_MIN_BYTES = 1u << 20;
+} // namespace
+
+void host_track(void *p, size_t bytes)
+{
+    if (!p || bytes < PIN_MIN_BYTES) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_host[p] = HostArr{bytes, 0};
+}
+
+void host_untrack(void *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_host.find(p);
+    if (it == g_host.end()) return;
+    if (it->second.state == 1)
+    {
+        cudaHostUnregister(p);
+        cudaGetLastError();
+    }
+    g_host.erase(it);
+}
+
+void host_pin_if_owned(const void *p, size_t bytes)
+{
+    if (bytes < PIN_MIN_BYTES) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_host.find(p);
+    if (it == g_host.end() || it->second.state != 0) return;
+    cudaError_t e = cudaHostRegister(const_cast<void *>(p), it->second.bytes, cudaHostRegisterDefault);
+    if (e == cudaSuccess)
+        it->second.state = 1;
+    else
+    {
+        cudaGetLastError();
+        it->second.state = 2;
+    }
+}
+
 } // namespace sdl
 
 using namespace sdl;
@@ -196,6 +245,7 @@ extern "C" CSR_matrix *new_CSR_matrix(int m, int n, int nnz)
     A->m = m;
     A->n = n;
     A->nnz = nnz;
+    if (nnz > 0) host_track(A->x, (size_t)nnz * sizeof(double));
     return A;
 }
 
@@ -215,6 +265,7 @@ extern "C" void free_CSR_matrix(CSR_matrix *matrix)
 {
     if (!matrix) return;
     raw_forget(matrix);
+    host_untrack(matrix->x);
     sp_free(matrix->p);
     sp_free(matrix->i);
     sp_free(matrix->x);
@@ -239,8 +290,10 @@ extern "C" void CSR_trim(CSR_matrix *A)
     int nnz = A->p[A->m];
     A->nnz = nnz;
     if (nnz == 0) return;
+    host_untrack(A->x);
     A->i = (int *)sp_realloc(A->i, (size_t)nnz * sizeof(int));
     A->x = (double *)sp_realloc(A->x, (size_t)nnz * sizeof(double));
+    host_track(A->x, (size_t)nnz * sizeof(double));
 }
 
 extern "C" CSR_matrix *AT_alloc(const CSR_matrix *A, int *iwork)
@@ -310,6 +363,7 @@ extern "C" CSC_matrix *new_CSC_matrix(int m, int n, int nnz)
     A->m = m;
     A->n = n;
     A->nnz = nnz;
+    if (nnz > 0) host_track(A->x, (size_t)nnz * sizeof(double));
     return A;
 }
 
@@ -317,6 +371,7 @@ extern "C" void free_CSC_matrix(CSC_matrix *matrix)
 {
     if (!matrix) return;
     raw_forget(matrix);
+    host_untrack(matrix->x);
     sp_free(matrix->p);
     sp_free(matrix->i);
     sp_free(matrix->x);

@@ -120,7 +120,7 @@ __global__ void k_sym_classify(const long long *__restrict__ ub, int m_out,
 }
 
 __global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp,
-                               int m_out, unsigned char *__restrict__ cls)
+                               int m_out, unsigned char *__restrict__ cls, long long *__restrict__ plan_len)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
          r += (long long)gridDim.x * blockDim.x)
@@ -132,8 +132,12 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
             c = 255;
         else if (u <= 32)
             c = NUM_W32;
+        else if (u <= 64)
+            c = NUM_W64;
         else if (u <= 128)
             c = NUM_W128;
+        else if (u <= 256)
+            c = NUM_W256;
         else if (u <= 512)
             c = NUM_W512;
         else if (nr <= 2048)
@@ -143,6 +147,7 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
         else
             c = NUM_GMEM;
         cls[r] = (unsigned char)c;
+        plan_len[r] = c < NUM_WARP_CLASSES ? u : 0;
     }
 }
 
@@ -407,26 +412,92 @@ __device__ __forceinline__ void warp_ordered_add(double *acc, int pos, double pr
     }
 }
 
+// Plan of a warp-class row, built once per pattern: the terms are visited exactly
+// as k_num_warp_plan visits them (L entries in chunks of 32, their terms in windows
+// of 32), and every term gets its position inside the output row (found by binary
+// search in the sorted row), plus bit 15 when its window has two terms on one
+// position (so the numeric kernel must apply that window in term order).
 template <int CAP>
-__global__ void k_num_warp(const int *__restrict__ rows, int count, NumArgs a)
+__global__ void k_build_plan(const int *__restrict__ rows, int count, NumArgs a,
+                             unsigned short *__restrict__ plan, const long long *__restrict__ plan_off)
 {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int lane = lane_id(), wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
-    double *acc = (double *)smraw + w * CAP;
-    int *ci = (int *)((double *)smraw + wpb * CAP) + w * CAP;
-    for (long long it = blockIdx.x * (long long)wpb + w; it < count;
+    extern __shared__ int sci[];
+    const int lane = lane_id(), wpb = blockDim.x >> 5;
+    int *ci = sci + (threadIdx.x >> 5) * CAP;
+    for (long long it = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); it < count;
          it += (long long)gridDim.x * wpb)
     {
         int row = rows[it];
         int b = row / a.L_m, r = row - b * a.L_m;
         int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
-        for (int q = lane; q < nr; q += 32)
+        for (int q = lane; q < nr; q += 32) ci[q] = a.Ci[cs + q];
+        __syncwarp();
+        long long po = plan_off[row];
+        int ls = a.Lp[r], le = a.Lp[r + 1], cum = 0;
+        for (int c = ls; c < le; c += 32)
         {
-            ci[q] = a.Ci[cs + q];
-            acc[q] = 0.0;
+            int ii = c + lane, s = 0, len = 0;
+            if (ii < le)
+            {
+                int k = a.Li[ii] + b * a.n_L;
+                s = a.Ap[k];
+                len = a.Ap[k + 1] - s;
+            }
+            int incl = warp_incl_scan(len);
+            int total = __shfl_sync(FULL_MASK, incl, 31);
+            for (int base = 0; base < total; base += 32)
+            {
+                int u = base + lane;
+                bool valid = u < total;
+                int e = warp_entry_of(incl, u);
+                int se = __shfl_sync(FULL_MASK, s, e);
+                int ie = __shfl_sync(FULL_MASK, incl, e);
+                int lne = __shfl_sync(FULL_MASK, len, e);
+                int pos = 0;
+                if (valid)
+                {
+                    int j = a.Ai[se + u - (ie - lne)];
+                    pos = lower_bound_dev(ci, nr, j);
+                    if (pos >= nr || ci[pos] != j)
+                    {
+                        atomicOr(a.err, 1);
+                        pos = 0x7fff; // rejected by the numeric kernel's range check
+                    }
+                }
+                unsigned key = valid ? (unsigned)pos : (0x80000000u | (unsigned)lane);
+                unsigned peers = __match_any_sync(FULL_MASK, key);
+                bool dup = __any_sync(FULL_MASK, valid && __popc(peers) > 1);
+                if (valid) plan[po + cum + u] = (unsigned short)(pos | (dup ? 0x8000 : 0));
+            }
+            cum += total;
         }
         __syncwarp();
-        int ls = a.Lp[r], le = a.Lp[r + 1];
+    }
+}
+
+// Warp-class numeric refill through the plan: per term only the value of A is
+// gathered (no column index, no search); the loads of up to BATCH windows are
+// issued before their accumulations so their latencies overlap. Windows without a
+// duplicated position are applied in one step, the others lane by lane in term
+// order.
+template <int CAP, int BATCH>
+__global__ void k_num_warp_plan(const int *__restrict__ rows, int count, NumArgs a,
+                                const unsigned short *__restrict__ plan,
+                                const long long *__restrict__ plan_off)
+{
+    extern __shared__ __align__(16) double sacc[];
+    const int lane = lane_id(), wpb = blockDim.x >> 5;
+    double *acc = sacc + (threadIdx.x >> 5) * CAP;
+    for (long long it = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); it < count;
+         it += (long long)gridDim.x * wpb)
+    {
+        int row = rows[it];
+        int b = row / a.L_m, r = row - b * a.L_m;
+        int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
+        for (int q = lane; q < nr; q += 32) acc[q] = 0.0;
+        __syncwarp();
+        long long po = plan_off[row];
+        int ls = a.Lp[r], le = a.Lp[r + 1], cum = 0;
         for (int c = ls; c < le; c += 32)
         {
             int ii = c + lane, s = 0, len = 0;
@@ -441,31 +512,59 @@ __global__ void k_num_warp(const int *__restrict__ rows, int count, NumArgs a)
             }
             int incl = warp_incl_scan(len);
             int total = __shfl_sync(FULL_MASK, incl, 31);
-            for (int base = 0; base < total; base += 32)
+            for (int b0 = 0; b0 < total; b0 += 32 * BATCH)
             {
-                int u = base + lane;
-                bool valid = u < total;
-                int e = warp_entry_of(incl, u);
-                int se = __shfl_sync(FULL_MASK, s, e);
-                int ie = __shfl_sync(FULL_MASK, incl, e);
-                int lne = __shfl_sync(FULL_MASK, len, e);
-                double ve = __shfl_sync(FULL_MASK, v, e);
-                int pos = 0;
-                double prod = 0.0;
-                if (valid)
+                int pos_r[BATCH];
+                double prod_r[BATCH];
+                unsigned dup_r = 0;
+#pragma unroll
+                for (int k = 0; k < BATCH; ++k)
                 {
-                    int jj = se + u - (ie - lne);
-                    int j = a.Ai[jj];
-                    prod = __dmul_rn(ve, a.Ax[jj]);
-                    pos = lower_bound_dev(ci, nr, j);
-                    if (pos >= nr || ci[pos] != j)
+                    pos_r[k] = -1;
+                    prod_r[k] = 0.0;
+                    int base = b0 + 32 * k;
+                    if (base < total)
                     {
-                        atomicOr(a.err, 1);
-                        valid = false;
+                        int u = base + lane;
+                        int e = warp_entry_of(incl, u);
+                        int se = __shfl_sync(FULL_MASK, s, e);
+                        int ie = __shfl_sync(FULL_MASK, incl, e);
+                        int lne = __shfl_sync(FULL_MASK, len, e);
+                        double ve = __shfl_sync(FULL_MASK, v, e);
+                        if (u < total)
+                        {
+                            unsigned pe = plan[po + cum + u];
+                            prod_r[k] = __dmul_rn(ve, a.Ax[se + u - (ie - lne)]);
+                            pos_r[k] = (int)(pe & 0x7fffu);
+                            dup_r |= (pe >> 15) << k;
+                        }
                     }
                 }
-                warp_ordered_add(acc, pos, prod, valid);
+#pragma unroll
+                for (int k = 0; k < BATCH; ++k)
+                {
+                    if (b0 + 32 * k < total)
+                    {
+                        int pos = pos_r[k];
+                        bool valid = pos >= 0;
+                        if (valid && pos >= nr)
+                        {
+                            atomicOr(a.err, 1);
+                            valid = false;
+                        }
+                        if (__any_sync(FULL_MASK, (dup_r >> k) & 1u))
+                        {
+                            warp_ordered_add(acc, pos, prod_r[k], valid);
+                        }
+                        else
+                        {
+                            if (valid) acc[pos] = __dadd_rn(acc[pos], prod_r[k]);
+                            __syncwarp();
+                        }
+                    }
+                }
             }
+            cum += total;
         }
         __syncwarp();
         for (int q = lane; q < nr; q += 32) a.Cx[cs + q] = acc[q];
@@ -750,9 +849,31 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
         SDL_LAUNCH(k_compact, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, ub_off.get(),
                    row_nnz.get(), P.Cp.get(), tmp.get(), P.Ci.get(), m_out);
 
+    DevBuf<long long> plan_len(m_out);
     SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(),
-               P.Cp.get(), m_out, cls.get());
+               P.Cp.get(), m_out, cls.get(), plan_len.get());
     bin_items(cls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
+    P.plan_off.reset((size_t)m_out + 1);
+    long long plan_total = exclusive_scan_i64(plan_len.get(), P.plan_off.get(), m_out, s);
+    P.plan.reset(std::max<long long>(1, plan_total));
+    {
+        NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, nullptr, nullptr, d.Ap, d.Ai, nullptr,
+                   P.Cp.get(), P.Ci.get(), nullptr, rt.d_error};
+        const int *rows = P.num_rows.get();
+        const int wpb_b = 8;
+#define SDL_BUILD_PLAN(CLS, CAPV)                                                                   \
+    if (P.num_count[CLS])                                                                           \
+        SDL_LAUNCH(k_build_plan<CAPV>, grid_for(P.num_count[CLS], wpb_b, cap), wpb_b * 32,            \
+                   wpb_b * (CAPV) * 4, s, rows + P.num_offset[CLS], P.num_count[CLS], na, P.plan.get(), \
+                   P.plan_off.get());
+        SDL_BUILD_PLAN(NUM_W32, 32)
+        SDL_BUILD_PLAN(NUM_W64, 64)
+        SDL_BUILD_PLAN(NUM_W128, 128)
+        SDL_BUILD_PLAN(NUM_W256, 256)
+        SDL_BUILD_PLAN(NUM_W512, 512)
+#undef SDL_BUILD_PLAN
+    }
+    if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
     if (P.num_count[NUM_GMEM])
     {
         long long per_slot = std::max(1, P.n);
@@ -778,18 +899,16 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
     const int *cnt = P.num_count;
     const int cap = rt.num_sms * 16;
     const int wpb = 8;
-    if (cnt[NUM_W32])
-        SDL_LAUNCH(k_num_warp<32>, grid_for(cnt[NUM_W32], wpb, cap), wpb * 32, wpb * 32 * 12, s,
-                   rows + off[NUM_W32], cnt[NUM_W32], na);
-    if (cnt[NUM_W128])
-        SDL_LAUNCH(k_num_warp<128>, grid_for(cnt[NUM_W128], wpb, cap), wpb * 32, wpb * 128 * 12, s,
-                   rows + off[NUM_W128], cnt[NUM_W128], na);
-    if (cnt[NUM_W512])
-    {
-        const int w5 = 4; // 4 warps x 6 KB
-        SDL_LAUNCH(k_num_warp<512>, grid_for(cnt[NUM_W512], w5, cap), w5 * 32, w5 * 512 * 12, s,
-                   rows + off[NUM_W512], cnt[NUM_W512], na);
-    }
+#define SDL_NUM_WARP(CLS, CAPV, BATCHV)                                                        \
+    if (cnt[CLS])                                                                              \
+        SDL_LAUNCH((k_num_warp_plan<CAPV, BATCHV>), grid_for(cnt[CLS], wpb, cap), wpb * 32,      \
+                   wpb * (CAPV) * 8, s, rows + off[CLS], cnt[CLS], na, P.plan.get(), P.plan_off.get());
+    SDL_NUM_WARP(NUM_W32, 32, 1)
+    SDL_NUM_WARP(NUM_W64, 64, 2)
+    SDL_NUM_WARP(NUM_W128, 128, 4)
+    SDL_NUM_WARP(NUM_W256, 256, 8)
+    SDL_NUM_WARP(NUM_W512, 512, 8)
+#undef SDL_NUM_WARP
     if (cnt[NUM_C2K])
     {
         int th = 256;

@@ -164,13 +164,16 @@ enum
 enum
 {
     NUM_W32 = 0,
+    NUM_W64,
     NUM_W128,
+    NUM_W256,
     NUM_W512,
     NUM_C2K,
     NUM_C8K,
     NUM_GMEM,
     NUM_NBINS
 };
+constexpr int NUM_WARP_CLASSES = 5; // NUM_W32 .. NUM_W512 use the planned warp kernel
 
 struct TuneConfig
 {
@@ -205,6 +208,11 @@ struct Product
     DevBuf<int> num_rows; // row ids grouped by numeric class
     int num_count[NUM_NBINS] = {0};
     int num_offset[NUM_NBINS + 1] = {0};
+    // Plan of the warp-class rows: for every term (in the numeric kernel's visiting
+    // order) its position inside the output row, bit 15 set when the 32-term window
+    // holding it has two terms on one position.
+    DevBuf<unsigned short> plan;
+    DevBuf<long long> plan_off; // m_out + 1
     DevBuf<int> gmem_scratch; // posmap scratch for NUM_GMEM rows (slots x n ints)
     int gmem_slots = 0;
     TuneConfig cfg;

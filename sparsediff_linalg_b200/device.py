@@ -17,9 +17,13 @@ def _ptr(t):
 
 
 def _stream(stream):
+    """cudaStream_t of a torch stream. torch's legacy default stream has handle 0,
+    which the C API reads as "the library's stream", so it is passed as
+    cudaStreamLegacy (0x1) instead: work is then ordered with torch's kernels and
+    events recorded on that stream bracket it."""
     if stream is None:
         stream = torch.cuda.current_stream()
-    return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(stream.cuda_stream or 1)
 
 
 class _DevView:
