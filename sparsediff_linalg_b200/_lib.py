@@ -7,10 +7,13 @@ library has not been built: there is no Python or CPU fallback for any operation
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libsparsediff_linalg_b200.so"
+# SPARSEDIFF_LINALG_B200_LIB selects another build of the library (e.g. one
+# compiled with different tile parameters); default: the in-tree build.
+LIB_PATH = Path(os.environ.get("SPARSEDIFF_LINALG_B200_LIB", str(PKG / "libsparsediff_linalg_b200.so")))
 
 c_int_p = C.POINTER(C.c_int)
 c_double_p = C.POINTER(C.c_double)

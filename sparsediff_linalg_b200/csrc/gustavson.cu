@@ -16,9 +16,10 @@
 //             CTA + shared-memory sort (<= 2048 / 8192), CTA + shared-memory
 //             bitmap over column windows (larger rows; the bitmap yields the
 //             columns already sorted);
-//   numeric:  warp + shared accumulator (<= 512 terms), CTA + shared accumulator
-//             (<= 8192 output entries), CTA + accumulator in C.x itself with a
-//             global column->position map (larger rows).
+//   numeric:  row tiles (rows of <= TILE_T terms, grouped into CTA-sized tiles,
+//             with a per-term position plan built once per pattern), CTA + shared
+//             accumulator (<= 8192 output entries), CTA + accumulator in C.x itself
+//             with a global column->position map (larger rows).
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -120,7 +121,9 @@ __global__ void k_sym_classify(const long long *__restrict__ ub, int m_out,
 }
 
 __global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp,
-                               int m_out, unsigned char *__restrict__ cls, long long *__restrict__ plan_len)
+                               const int *__restrict__ Lp, int L_m, int m_out,
+                               unsigned char *__restrict__ cls, long long *__restrict__ weight,
+                               long long *__restrict__ small_ent, long long *__restrict__ small_terms)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
          r += (long long)gridDim.x * blockDim.x)
@@ -130,16 +133,8 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
         int c;
         if (u == 0)
             c = 255;
-        else if (u <= 32)
-            c = NUM_W32;
-        else if (u <= 64)
-            c = NUM_W64;
-        else if (u <= 128)
-            c = NUM_W128;
-        else if (u <= 256)
-            c = NUM_W256;
-        else if (u <= 512)
-            c = NUM_W512;
+        else if (u <= TILE_T)
+            c = NUM_TILE;
         else if (nr <= 2048)
             c = NUM_C2K;
         else if (nr <= 8192)
@@ -147,8 +142,40 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
         else
             c = NUM_GMEM;
         cls[r] = (unsigned char)c;
-        plan_len[r] = c < NUM_WARP_CLASSES ? u : 0;
+        int rr = (int)(r % L_m);
+        small_ent[r] = c == NUM_TILE ? Lp[rr + 1] - Lp[rr] : 0;
+        small_terms[r] = c == NUM_TILE ? u : 0;
+        weight[r] = c == NUM_TILE ? u + TILE_T / TILE_THREADS : (c == 255 ? TILE_T / TILE_THREADS : TILE_T);
     }
+}
+
+// tile index of every row = floor(exclusive weight prefix / TILE_T); flag rows that
+// start a tile
+__global__ void k_tile_flags(const long long *__restrict__ wpref, int m_out, int *__restrict__ flag)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
+         r += (long long)gridDim.x * blockDim.x)
+        flag[r] = (r == 0 || wpref[r] / TILE_T != wpref[r - 1] / TILE_T) ? 1 : 0;
+}
+
+// padded (to 8 entries = 16 bytes) plan length of every tile
+__global__ void k_tile_plan_sizes(const int *__restrict__ tile_start, const long long *__restrict__ spref,
+                                  int ntiles, long long *__restrict__ padded)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        long long n = spref[tile_start[t + 1]] - spref[tile_start[t]];
+        padded[t] = (n + 7) & ~7LL;
+    }
+}
+
+__global__ void k_tile_starts(const int *__restrict__ flag, const int *__restrict__ tile_of, int m_out,
+                              int *__restrict__ tile_start)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
+         r += (long long)gridDim.x * blockDim.x)
+        if (flag[r]) tile_start[tile_of[r]] = (int)r;
 }
 
 // ------------------------------------------------------------ symbolic kernels
@@ -397,179 +424,461 @@ __global__ void k_compact(const long long *__restrict__ ub_off, const int *__res
 }
 
 // ------------------------------------------------------------ numeric kernels
-// Apply acc[pos] += prod for the valid lanes, lanes sharing a position one after
-// another in lane (= term) order.
-__device__ __forceinline__ void warp_ordered_add(double *acc, int pos, double prod, bool valid)
+// ------------------------------------------------------------ row tiles
+constexpr int TILE_ACC = 2 * TILE_T;
+constexpr int TILE_CLAIM = 1024; // hashed claim slots of the ordered path
+
+// last index q in [0, n) with a[q] <= key (a non-decreasing, a[0] <= key)
+__device__ __forceinline__ int last_le(const int *a, int n, int key)
 {
-    unsigned key = valid ? (unsigned)pos : (0x80000000u | (unsigned)lane_id());
-    unsigned peers = __match_any_sync(FULL_MASK, key);
-    int rank = __popc(peers & lanemask_lt());
-    unsigned rounds = __reduce_max_sync(FULL_MASK, valid ? (unsigned)__popc(peers) : 1u);
-    for (unsigned q = 0; q < rounds; ++q)
+    int lo = 0, hi = n;
+    while (hi - lo > 1)
     {
-        if (valid && rank == (int)q) acc[pos] = __dadd_rn(acc[pos], prod);
-        __syncwarp();
+        int mid = (lo + hi) >> 1;
+        if (a[mid] <= key)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+struct BuildSmem
+{
+    int *cnt; // TILE_ACC multiplicity counters
+    int *row_cs, *row_ls, *row_b, *row_accoff, *row_eoff;
+    int *e_incl, *e_s, *e_len, *e_row;
+    int *scr;
+};
+constexpr size_t build_smem_bytes()
+{
+    return ((size_t)TILE_ACC + 3 * TILE_THREADS + 2 * (TILE_THREADS + 1) + 4 * TILE_THREADS + 32) * 4;
+}
+
+// Compiles the refill schedule of one tile (one CTA per tile, once per pattern):
+// the tile descriptor, one TileEntry per L entry of the tile rows, and the plan:
+// the position of every term inside its output row (binary search in the sorted
+// row) in upstream's visiting order, bit 15 marking a term whose output collects
+// exactly two terms. A tile is marked ordered when one of its output entries
+// collects three or more terms: with at most two terms per entry
+// the order of the additions cannot change the result ((0 + a) + b == (0 + b) + a
+// bit for bit, signed zeros included), so only ordered tiles need upstream's
+// exact order at refill time.
+__global__ void __launch_bounds__(TILE_THREADS) k_tile_build(
+    NumArgs a, const unsigned char *__restrict__ rcls, const int *__restrict__ tile_start,
+    const long long *__restrict__ epref, const long long *__restrict__ plan_begin,
+    TileDesc *__restrict__ tiles, TileEntry *__restrict__ entries, unsigned short *__restrict__ plan)
+{
+    extern __shared__ __align__(16) int bsm[];
+    BuildSmem t;
+    t.cnt = bsm;
+    t.row_cs = t.cnt + TILE_ACC;
+    t.row_ls = t.row_cs + TILE_THREADS;
+    t.row_b = t.row_ls + TILE_THREADS;
+    t.row_accoff = t.row_b + TILE_THREADS;
+    t.row_eoff = t.row_accoff + TILE_THREADS + 1;
+    t.e_incl = t.row_eoff + TILE_THREADS + 1;
+    t.e_s = t.e_incl + TILE_THREADS;
+    t.e_len = t.e_s + TILE_THREADS;
+    t.e_row = t.e_len + TILE_THREADS;
+    t.scr = t.e_row + TILE_THREADS;
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int r0 = tile_start[tile], nrows = tile_start[tile + 1] - r0;
+    for (int q = tid; q < TILE_ACC; q += TILE_THREADS) t.cnt[q] = 0;
+    // rows
+    int nr = 0, ne = 0;
+    if (tid < nrows)
+    {
+        int r = r0 + tid;
+        int b = r / a.L_m, rr = r - b * a.L_m;
+        int cs = a.Cp[r], ls = a.Lp[rr];
+        if (rcls[r] == NUM_TILE)
+        {
+            nr = a.Cp[r + 1] - cs;
+            ne = a.Lp[rr + 1] - ls;
+        }
+        t.row_cs[tid] = cs;
+        t.row_ls[tid] = ls;
+        t.row_b[tid] = b;
+    }
+    int inr = block_incl_scan_int(nr, t.scr);
+    int ine = block_incl_scan_int(ne, t.scr);
+    if (tid < nrows)
+    {
+        t.row_accoff[tid] = inr - nr;
+        t.row_eoff[tid] = ine - ne;
+    }
+    if (tid == TILE_THREADS - 1)
+    {
+        t.row_accoff[nrows] = inr;
+        t.row_eoff[nrows] = ine;
+    }
+    __syncthreads();
+    const int total_out = t.row_accoff[nrows], total_ent = t.row_eoff[nrows];
+    const long long eb = epref[r0], pb = plan_begin[tile];
+    long long cursor = 0;
+    for (int ec = 0; ec < total_ent; ec += TILE_THREADS)
+    {
+        int e = ec + tid, s = 0, len = 0, lrow = 0;
+        if (e < total_ent)
+        {
+            lrow = last_le(t.row_eoff, nrows, e);
+            int ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
+            int k = a.Li[ii] + t.row_b[lrow] * a.n_L;
+            s = a.Ap[k];
+            len = a.Ap[k + 1] - s;
+        }
+        int incl = block_incl_scan_int(len, t.scr);
+        if (e < total_ent)
+        {
+            TileEntry rec;
+            rec.k = a.Li[t.row_ls[lrow] + (e - t.row_eoff[lrow])] + t.row_b[lrow] * a.n_L;
+            int ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
+            rec.lx = a.L_map ? a.L_map[ii] : ii;
+            rec.s = s;
+            rec.toff = (unsigned short)(cursor + incl - len);
+            rec.accbase = (unsigned short)t.row_accoff[lrow];
+            entries[eb + e] = rec;
+        }
+        t.e_incl[tid] = incl;
+        t.e_s[tid] = s;
+        t.e_len[tid] = len;
+        t.e_row[tid] = lrow;
+        __syncthreads();
+        int total = t.e_incl[TILE_THREADS - 1];
+        int nent = min(TILE_THREADS, total_ent - ec);
+        for (int u = tid; u < total; u += TILE_THREADS)
+        {
+            int el = cta_entry_of(t.e_incl, nent, u);
+            int jj = t.e_s[el] + u - (t.e_incl[el] - t.e_len[el]);
+            int j = a.Ai[jj];
+            int lr = t.e_row[el];
+            int w = t.row_accoff[lr + 1] - t.row_accoff[lr];
+            const int *crow = a.Ci + t.row_cs[lr];
+            int pos = lower_bound_dev(crow, w, j);
+            if (pos >= w || crow[pos] != j)
+            {
+                atomicOr(a.err, 1);
+                pos = 0xffff; // rejected by the refill's range check
+            }
+            else
+                atomicAdd(&t.cnt[t.row_accoff[lr] + pos], 1);
+            plan[pb + cursor + u] = (unsigned short)pos;
+        }
+        cursor += total;
+        __syncthreads();
+    }
+    bool many = false;
+    for (int q = tid; q < total_out; q += TILE_THREADS) many |= t.cnt[q] >= 3;
+    many = __syncthreads_or(many);
+    if (!many)
+    {
+        // tag the terms of two-term outputs (bit 15): they accumulate with an atomic
+        // add, every other term is the sole term of its output and is stored
+        for (int e = tid; e < total_ent; e += TILE_THREADS)
+        {
+            const TileEntry rec = entries[eb + e];
+            int end = e + 1 < total_ent ? entries[eb + e + 1].toff : (int)cursor;
+            for (int q = rec.toff; q < end; ++q)
+            {
+                unsigned short pv = plan[pb + q];
+                if (pv != 0xffff && t.cnt[rec.accbase + pv] == 2) plan[pb + q] = pv | 0x8000;
+            }
+        }
+    }
+    if (tid == 0)
+    {
+        TileDesc dsc;
+        dsc.ent_begin = eb;
+        dsc.plan_begin = pb;
+        dsc.nent = total_ent;
+        dsc.out_begin = t.row_cs[0];
+        dsc.nout = total_out;
+        dsc.prod = 0;
+        dsc.ordered = many ? 1 : 0;
+        dsc.nterms = (int)cursor;
+        dsc.pad[0] = dsc.pad[1] = 0;
+        tiles[tile] = dsc;
     }
 }
 
-// Plan of a warp-class row, built once per pattern: the terms are visited exactly
-// as k_num_warp_plan visits them (L entries in chunks of 32, their terms in windows
-// of 32), and every term gets its position inside the output row (found by binary
-// search in the sorted row), plus bit 15 when its window has two terms on one
-// position (so the numeric kernel must apply that window in term order).
-template <int CAP>
-__global__ void k_build_plan(const int *__restrict__ rows, int count, NumArgs a,
-                             unsigned short *__restrict__ plan, const long long *__restrict__ plan_off)
+#ifndef SDL_GROUP
+#define SDL_GROUP 4
+#endif
+#ifndef SDL_UNROLL
+#define SDL_UNROLL 2
+#endif
+#ifndef SDL_QPL
+#define SDL_QPL 2
+#endif
+#ifndef SDL_REFILL_MINB
+#define SDL_REFILL_MINB 4
+#endif
+constexpr int GROUP = SDL_GROUP; // lanes per L entry
+constexpr int NGROUP = TILE_THREADS / GROUP;
+constexpr int UNROLL = SDL_UNROLL; // entries per group whose loads are in flight together
+constexpr int QPL = SDL_QPL;       // terms per lane issued with the batch (GROUP * QPL per entry)
+constexpr int REC_BUF = 256;       // entry records staged per tile (more: read from global)
+
+struct RefillSmem
 {
-    extern __shared__ int sci[];
-    const int lane = lane_id(), wpb = blockDim.x >> 5;
-    int *ci = sci + (threadIdx.x >> 5) * CAP;
-    for (long long it = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); it < count;
-         it += (long long)gridDim.x * wpb)
-    {
-        int row = rows[it];
-        int b = row / a.L_m, r = row - b * a.L_m;
-        int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
-        for (int q = lane; q < nr; q += 32) ci[q] = a.Ci[cs + q];
-        __syncwarp();
-        long long po = plan_off[row];
-        int ls = a.Lp[r], le = a.Lp[r + 1], cum = 0;
-        for (int c = ls; c < le; c += 32)
-        {
-            int ii = c + lane, s = 0, len = 0;
-            if (ii < le)
-            {
-                int k = a.Li[ii] + b * a.n_L;
-                s = a.Ap[k];
-                len = a.Ap[k + 1] - s;
-            }
-            int incl = warp_incl_scan(len);
-            int total = __shfl_sync(FULL_MASK, incl, 31);
-            for (int base = 0; base < total; base += 32)
-            {
-                int u = base + lane;
-                bool valid = u < total;
-                int e = warp_entry_of(incl, u);
-                int se = __shfl_sync(FULL_MASK, s, e);
-                int ie = __shfl_sync(FULL_MASK, incl, e);
-                int lne = __shfl_sync(FULL_MASK, len, e);
-                int pos = 0;
-                if (valid)
-                {
-                    int j = a.Ai[se + u - (ie - lne)];
-                    pos = lower_bound_dev(ci, nr, j);
-                    if (pos >= nr || ci[pos] != j)
-                    {
-                        atomicOr(a.err, 1);
-                        pos = 0x7fff; // rejected by the numeric kernel's range check
-                    }
-                }
-                unsigned key = valid ? (unsigned)pos : (0x80000000u | (unsigned)lane);
-                unsigned peers = __match_any_sync(FULL_MASK, key);
-                bool dup = __any_sync(FULL_MASK, valid && __popc(peers) > 1);
-                if (valid) plan[po + cum + u] = (unsigned short)(pos | (dup ? 0x8000 : 0));
-            }
-            cum += total;
-        }
-        __syncwarp();
-    }
+    double *acc;                // TILE_ACC
+    double *e_v;                // TILE_THREADS (ordered path)
+    TileEntry *rec;             // 2 x REC_BUF
+    unsigned short *pln;        // 2 x TILE_ACC
+    TileDesc *desc;             // 3 (tile k uses desc[k % 3])
+    int *claim;                 // TILE_CLAIM
+    int *e_incl, *e_s, *e_len, *e_acc, *scr;
+};
+
+__host__ __device__ constexpr size_t refill_smem_bytes()
+{
+    return (size_t)TILE_ACC * 8 + TILE_THREADS * 8 + 2 * REC_BUF * sizeof(TileEntry) +
+           2 * (size_t)TILE_ACC * 2 + 3 * sizeof(TileDesc) +
+           ((size_t)TILE_CLAIM + 4 * TILE_THREADS + 32) * 4;
 }
 
-// Warp-class numeric refill through the plan: per term only the value of A is
-// gathered (no column index, no search); the loads of up to BATCH windows are
-// issued before their accumulations so their latencies overlap. Windows without a
-// duplicated position are applied in one step, the others lane by lane in term
-// order.
-template <int CAP, int BATCH>
-__global__ void k_num_warp_plan(const int *__restrict__ rows, int count, NumArgs a,
-                                const unsigned short *__restrict__ plan,
-                                const long long *__restrict__ plan_off)
+__device__ __forceinline__ RefillSmem refill_smem(unsigned char *raw)
 {
-    extern __shared__ __align__(16) double sacc[];
-    const int lane = lane_id(), wpb = blockDim.x >> 5;
-    double *acc = sacc + (threadIdx.x >> 5) * CAP;
-    for (long long it = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); it < count;
-         it += (long long)gridDim.x * wpb)
+    RefillSmem t;
+    t.acc = (double *)raw;
+    t.e_v = t.acc + TILE_ACC;
+    t.rec = (TileEntry *)(t.e_v + TILE_THREADS);
+    t.pln = (unsigned short *)(t.rec + 2 * REC_BUF);
+    t.desc = (TileDesc *)(t.pln + 2 * TILE_ACC);
+    t.claim = (int *)(t.desc + 3);
+    t.e_incl = t.claim + TILE_CLAIM;
+    t.e_s = t.e_incl + TILE_THREADS;
+    t.e_len = t.e_s + TILE_THREADS;
+    t.e_acc = t.e_len + TILE_THREADS;
+    t.scr = t.e_acc + TILE_THREADS;
+    return t;
+}
+
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
+{
+    unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Stage a tile's entry records (when they fit) and plan into shared buffer b.
+__device__ __forceinline__ void stage_tile(const RefillSmem &t, int b, const TileDesc &D,
+                                           const TileEntry *__restrict__ entries,
+                                           const unsigned short *__restrict__ plan)
+{
+    if (D.nent <= REC_BUF)
+        for (int e = threadIdx.x; e < D.nent; e += TILE_THREADS)
+            cp_async16(t.rec + b * REC_BUF + e, entries + D.ent_begin + e);
+    const int n16 = (D.nterms + 7) >> 3;
+    for (int c = threadIdx.x; c < n16; c += TILE_THREADS)
+        cp_async16(t.pln + b * TILE_ACC + 8 * c, plan + D.plan_begin + 8 * c);
+}
+
+__device__ __forceinline__ void stage_desc(const RefillSmem &t, int b, const TileDesc *__restrict__ tiles,
+                                           int tile)
+{
+    if (threadIdx.x < (int)(sizeof(TileDesc) / 16))
+        cp_async16((char *)(t.desc + b) + 16 * threadIdx.x, (const char *)(tiles + tile) + 16 * threadIdx.x);
+}
+
+__device__ __forceinline__ void put_term(double *acc, int nout, int ab, unsigned pe, double prod, int *err)
+{
+    const int idx = ab + (int)(pe & 0x7fffu);
+    if (idx >= nout)
+        atomicOr(err, 1);
+    else if (pe & 0x8000u)
+        atomicAdd(&acc[idx], prod);
+    else
+        acc[idx] = __dadd_rn(0.0, prod);
+}
+
+// Refill of the tile rows from the compiled schedule: a persistent CTA walks its
+// tiles while cp.async stages the next tile's descriptor, entry records and plan
+// in shared memory, so only the value reads of the current tile are exposed.
+// Each group of GROUP lanes takes UNROLL entries at once and issues every value
+// they need (L's and d's per entry, A's row per term) together. Terms land in a
+// shared window over the tile's outputs, written back to one contiguous range of
+// C.x.
+//   unordered tiles: the sole term of an output is stored (0.0 + prod, as upstream
+//     starts from +0.0); the two terms of a two-term output are atomically added
+//     (their order cannot change the result);
+//   ordered tiles: each 256-term window goes through a hashed claim table,
+//     smallest term index first, which is upstream's order.
+__global__ void __launch_bounds__(TILE_THREADS, SDL_REFILL_MINB) k_tile_refill(
+    const TileDesc *__restrict__ tiles, int ntiles, const TileEntry *__restrict__ entries,
+    const unsigned short *__restrict__ plan, const ProdPtrs *__restrict__ ptrs, ProdPtrs single,
+    int *__restrict__ err)
+{
+    extern __shared__ __align__(16) unsigned char rraw[];
+    RefillSmem t = refill_smem(rraw);
+    __shared__ int chunk_total;
+    const int tid = threadIdx.x;
+    const int stride = gridDim.x;
+    int tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    for (int q = tid; q < TILE_ACC; q += TILE_THREADS) t.acc[q] = 0.0;
+    // prologue: descriptor of the first tile, its records / plan, the next descriptor
+    stage_desc(t, 0, tiles, tile);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    stage_tile(t, 0, t.desc[0], entries, plan);
+    if (tile + stride < ntiles) stage_desc(t, 1, tiles, tile + stride);
+    cp_async_commit();
+    for (int k = 0; tile < ntiles; ++k, tile += stride)
     {
-        int row = rows[it];
-        int b = row / a.L_m, r = row - b * a.L_m;
-        int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
-        for (int q = lane; q < nr; q += 32) acc[q] = 0.0;
-        __syncwarp();
-        long long po = plan_off[row];
-        int ls = a.Lp[r], le = a.Lp[r + 1], cum = 0;
-        for (int c = ls; c < le; c += 32)
+        const int b = k & 1, nb = b ^ 1;
+        const TileDesc &D = t.desc[k % 3];
+        cp_async_wait_all();
+        __syncthreads();
+        if (tile + stride < ntiles)
         {
-            int ii = c + lane, s = 0, len = 0;
-            double v = 0.0;
-            if (ii < le)
-            {
-                int k = a.Li[ii] + b * a.n_L;
-                s = a.Ap[k];
-                len = a.Ap[k + 1] - s;
-                double lx = a.Lx ? a.Lx[a.L_map ? a.L_map[ii] : ii] : 1.0;
-                v = a.d ? __dmul_rn(lx, a.d[k]) : lx;
-            }
-            int incl = warp_incl_scan(len);
-            int total = __shfl_sync(FULL_MASK, incl, 31);
-            for (int b0 = 0; b0 < total; b0 += 32 * BATCH)
-            {
-                int pos_r[BATCH];
-                double prod_r[BATCH];
-                unsigned dup_r = 0;
-#pragma unroll
-                for (int k = 0; k < BATCH; ++k)
-                {
-                    pos_r[k] = -1;
-                    prod_r[k] = 0.0;
-                    int base = b0 + 32 * k;
-                    if (base < total)
-                    {
-                        int u = base + lane;
-                        int e = warp_entry_of(incl, u);
-                        int se = __shfl_sync(FULL_MASK, s, e);
-                        int ie = __shfl_sync(FULL_MASK, incl, e);
-                        int lne = __shfl_sync(FULL_MASK, len, e);
-                        double ve = __shfl_sync(FULL_MASK, v, e);
-                        if (u < total)
-                        {
-                            unsigned pe = plan[po + cum + u];
-                            prod_r[k] = __dmul_rn(ve, a.Ax[se + u - (ie - lne)]);
-                            pos_r[k] = (int)(pe & 0x7fffu);
-                            dup_r |= (pe >> 15) << k;
-                        }
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < BATCH; ++k)
-                {
-                    if (b0 + 32 * k < total)
-                    {
-                        int pos = pos_r[k];
-                        bool valid = pos >= 0;
-                        if (valid && pos >= nr)
-                        {
-                            atomicOr(a.err, 1);
-                            valid = false;
-                        }
-                        if (__any_sync(FULL_MASK, (dup_r >> k) & 1u))
-                        {
-                            warp_ordered_add(acc, pos, prod_r[k], valid);
-                        }
-                        else
-                        {
-                            if (valid) acc[pos] = __dadd_rn(acc[pos], prod_r[k]);
-                            __syncwarp();
-                        }
-                    }
-                }
-            }
-            cum += total;
+            stage_tile(t, nb, t.desc[(k + 1) % 3], entries, plan);
+            if (tile + 2 * stride < ntiles) stage_desc(t, (k + 2) % 3, tiles, tile + 2 * stride);
         }
-        __syncwarp();
-        for (int q = lane; q < nr; q += 32) a.Cx[cs + q] = acc[q];
-        __syncwarp();
+        cp_async_commit();
+
+        const ProdPtrs P = ptrs ? ptrs[D.prod] : single;
+        const TileEntry *E = D.nent <= REC_BUF ? t.rec + b * REC_BUF : entries + D.ent_begin;
+        const unsigned short *PL = t.pln + b * TILE_ACC;
+        if (D.ordered)
+            for (int q = tid; q < TILE_CLAIM; q += TILE_THREADS) t.claim[q] = INT_MAX;
+        if (!D.ordered)
+        {
+            const int g = tid / GROUP, gl = tid % GROUP;
+            for (int e0 = g; e0 < D.nent; e0 += NGROUP * UNROLL)
+            {
+                TileEntry rec[UNROLL];
+                int len[UNROLL];
+#pragma unroll
+                for (int j = 0; j < UNROLL; ++j)
+                {
+                    const int e = e0 + j * NGROUP;
+                    len[j] = 0;
+                    if (e < D.nent)
+                    {
+                        rec[j] = E[e];
+                        const int end = e + 1 < D.nent ? (int)E[e + 1].toff : D.nterms;
+                        len[j] = end - rec[j].toff;
+                    }
+                }
+                double lx[UNROLL], dk[UNROLL], xv[UNROLL][QPL];
+                unsigned pe[UNROLL][QPL];
+#pragma unroll
+                for (int j = 0; j < UNROLL; ++j)
+                {
+                    if (len[j] > 0)
+                    {
+                        lx[j] = P.Lx ? P.Lx[rec[j].lx] : 1.0;
+                        dk[j] = P.d ? P.d[rec[j].k] : 1.0;
+                    }
+#pragma unroll
+                    for (int qq = 0; qq < QPL; ++qq)
+                    {
+                        const int q = gl + qq * GROUP;
+                        if (q < len[j])
+                        {
+                            pe[j][qq] = PL[rec[j].toff + q];
+                            xv[j][qq] = P.Ax[rec[j].s + q];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < UNROLL; ++j)
+                {
+                    if (len[j] <= 0) continue;
+                    const double v = P.d ? __dmul_rn(lx[j], dk[j]) : lx[j];
+#pragma unroll
+                    for (int qq = 0; qq < QPL; ++qq)
+                    {
+                        const int q = gl + qq * GROUP;
+                        if (q < len[j])
+                            put_term(t.acc, D.nout, rec[j].accbase, pe[j][qq], __dmul_rn(v, xv[j][qq]), err);
+                    }
+                    for (int q = gl + QPL * GROUP; q < len[j]; q += GROUP)
+                        put_term(t.acc, D.nout, rec[j].accbase, PL[rec[j].toff + q],
+                                 __dmul_rn(v, P.Ax[rec[j].s + q]), err);
+                }
+            }
+        }
+        else
+        {
+            long long cursor = 0;
+            for (int ec = 0; ec < D.nent; ec += TILE_THREADS)
+            {
+                int e = ec + tid;
+                int len = 0, s = 0, accb = 0;
+                double v = 0.0;
+                if (e < D.nent)
+                {
+                    const TileEntry rec = E[e];
+                    const int end = e + 1 < D.nent ? (int)E[e + 1].toff : D.nterms;
+                    len = end - rec.toff;
+                    s = rec.s;
+                    accb = rec.accbase;
+                    double lxv = P.Lx ? P.Lx[rec.lx] : 1.0;
+                    v = P.d ? __dmul_rn(lxv, P.d[rec.k]) : lxv;
+                }
+                int incl = block_incl_scan_int(len, t.scr);
+                t.e_incl[tid] = incl;
+                t.e_s[tid] = s;
+                t.e_len[tid] = len;
+                t.e_acc[tid] = accb;
+                t.e_v[tid] = v;
+                if (tid == TILE_THREADS - 1) chunk_total = incl;
+                __syncthreads();
+                const int total = chunk_total;
+                const int nent = min(TILE_THREADS, D.nent - ec);
+                for (int base = 0; base < total; base += TILE_THREADS)
+                {
+                    int u = base + tid;
+                    bool pending = u < total;
+                    int idx = 0;
+                    double prod = 0.0;
+                    if (pending)
+                    {
+                        int el = cta_entry_of(t.e_incl, nent, u);
+                        int q = u - (t.e_incl[el] - t.e_len[el]);
+                        idx = t.e_acc[el] + PL[cursor + u];
+                        prod = __dmul_rn(t.e_v[el], P.Ax[t.e_s[el] + q]);
+                        if (idx >= D.nout)
+                        {
+                            atomicOr(err, 1);
+                            pending = false;
+                        }
+                    }
+                    const int slot = idx & (TILE_CLAIM - 1);
+                    while (true)
+                    {
+                        if (pending) atomicMin(&t.claim[slot], u);
+                        __syncthreads();
+                        bool won = pending && t.claim[slot] == u;
+                        if (won) t.acc[idx] = __dadd_rn(t.acc[idx], prod);
+                        __syncthreads();
+                        if (won)
+                        {
+                            t.claim[slot] = INT_MAX;
+                            pending = false;
+                        }
+                        if (!__syncthreads_or(pending)) break;
+                    }
+                }
+                cursor += total;
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        double *dst = P.Cx + D.out_begin;
+        for (int q = tid; q < D.nout; q += TILE_THREADS)
+        {
+            dst[q] = t.acc[q];
+            t.acc[q] = 0.0;
+        }
     }
+    cp_async_wait_all();
 }
 
 // Medium rows: one CTA per row, shared accumulator indexed by output position;
@@ -849,31 +1158,43 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
         SDL_LAUNCH(k_compact, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, ub_off.get(),
                    row_nnz.get(), P.Cp.get(), tmp.get(), P.Ci.get(), m_out);
 
-    DevBuf<long long> plan_len(m_out);
-    SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(),
-               P.Cp.get(), m_out, cls.get(), plan_len.get());
-    bin_items(cls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
-    P.plan_off.reset((size_t)m_out + 1);
-    long long plan_total = exclusive_scan_i64(plan_len.get(), P.plan_off.get(), m_out, s);
-    P.plan.reset(std::max<long long>(1, plan_total));
     {
+        DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1), small_ent(m_out),
+            epref((size_t)m_out + 1), small_terms(m_out), spref((size_t)m_out + 1);
+        DevBuf<unsigned char> rcls(m_out);
+        SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(),
+                   P.Cp.get(), d.Lp, d.L_m, m_out, rcls.get(), weight.get(), small_ent.get(),
+                   small_terms.get());
+        bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
+        exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
+        long long ent_total = exclusive_scan_i64(small_ent.get(), epref.get(), m_out, s);
+        long long plan_total = exclusive_scan_i64(small_terms.get(), spref.get(), m_out, s);
+        DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
+        SDL_LAUNCH(k_tile_flags, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, wpref.get(), m_out,
+                   flag.get());
+        P.ntiles = exclusive_scan_i32_checked(flag.get(), tile_of.get(), m_out, s);
+        DevBuf<int> tile_start((size_t)P.ntiles + 1);
+        SDL_LAUNCH(k_tile_starts, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, flag.get(),
+                   tile_of.get(), m_out, tile_start.get());
+        SDL_CUDA(cudaMemcpyAsync(tile_start.get() + P.ntiles, &m_out, sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+        DevBuf<long long> padded(std::max(1, P.ntiles)), plan_begin((size_t)P.ntiles + 1);
+        SDL_LAUNCH(k_tile_plan_sizes, grid_for(std::max(1, P.ntiles), 256, rt.num_sms * 8), 256, 0, s,
+                   tile_start.get(), spref.get(), P.ntiles, padded.get());
+        long long plan_padded = exclusive_scan_i64(padded.get(), plan_begin.get(), P.ntiles, s);
+        (void)plan_total;
+        P.tiles.reset(std::max(1, P.ntiles));
+        P.entries.reset(std::max<long long>(1, ent_total));
+        P.plan.reset(plan_padded + 16); // slack for the 16-byte staging copies
+        P.ptrs.reset(1);
         NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, nullptr, nullptr, d.Ap, d.Ai, nullptr,
                    P.Cp.get(), P.Ci.get(), nullptr, rt.d_error};
-        const int *rows = P.num_rows.get();
-        const int wpb_b = 8;
-#define SDL_BUILD_PLAN(CLS, CAPV)                                                                   \
-    if (P.num_count[CLS])                                                                           \
-        SDL_LAUNCH(k_build_plan<CAPV>, grid_for(P.num_count[CLS], wpb_b, cap), wpb_b * 32,            \
-                   wpb_b * (CAPV) * 4, s, rows + P.num_offset[CLS], P.num_count[CLS], na, P.plan.get(), \
-                   P.plan_off.get());
-        SDL_BUILD_PLAN(NUM_W32, 32)
-        SDL_BUILD_PLAN(NUM_W64, 64)
-        SDL_BUILD_PLAN(NUM_W128, 128)
-        SDL_BUILD_PLAN(NUM_W256, 256)
-        SDL_BUILD_PLAN(NUM_W512, 512)
-#undef SDL_BUILD_PLAN
+        set_smem(k_tile_build, build_smem_bytes());
+        SDL_LAUNCH(k_tile_build, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
+                   tile_start.get(), epref.get(), plan_begin.get(), P.tiles.get(), P.entries.get(),
+                   P.plan.get());
+        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
     }
-    if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
     if (P.num_count[NUM_GMEM])
     {
         long long per_slot = std::max(1, P.n);
@@ -886,11 +1207,28 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     SDL_CUDA(cudaStreamSynchronize(s));
 }
 
-void product_numeric(const Product &P, const double *Lx, const double *dvec, const double *Ax,
+void tile_refill(const TileDesc *tiles, int ntiles, const TileEntry *entries,
+                 const unsigned short *plan, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs single)
+{
+    if (ntiles <= 0) return;
+    Runtime &rt = runtime();
+    static int per_sm = 0;
+    if (!per_sm)
+    {
+        set_smem(k_tile_refill, refill_smem_bytes());
+        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_refill, TILE_THREADS,
+                                                               refill_smem_bytes()));
+        per_sm = std::max(1, per_sm);
+    }
+    int grid = std::min(ntiles, rt.num_sms * per_sm);
+    SDL_LAUNCH(k_tile_refill, grid, TILE_THREADS, refill_smem_bytes(), s, tiles, ntiles, entries, plan,
+               ptrs, single, rt.d_error);
+}
+
+void big_rows_refill(const Product &P, const double *Lx, const double *dvec, const double *Ax,
                      double *Cx, cudaStream_t s)
 {
     Runtime &rt = runtime();
-    if (P.nnz == 0) return;
     const ProductDesc &d = P.desc;
     NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(),
                Cx, rt.d_error};
@@ -898,17 +1236,6 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
     const int *off = P.num_offset;
     const int *cnt = P.num_count;
     const int cap = rt.num_sms * 16;
-    const int wpb = 8;
-#define SDL_NUM_WARP(CLS, CAPV, BATCHV)                                                        \
-    if (cnt[CLS])                                                                              \
-        SDL_LAUNCH((k_num_warp_plan<CAPV, BATCHV>), grid_for(cnt[CLS], wpb, cap), wpb * 32,      \
-                   wpb * (CAPV) * 8, s, rows + off[CLS], cnt[CLS], na, P.plan.get(), P.plan_off.get());
-    SDL_NUM_WARP(NUM_W32, 32, 1)
-    SDL_NUM_WARP(NUM_W64, 64, 2)
-    SDL_NUM_WARP(NUM_W128, 128, 4)
-    SDL_NUM_WARP(NUM_W256, 256, 8)
-    SDL_NUM_WARP(NUM_W512, 512, 8)
-#undef SDL_NUM_WARP
     if (cnt[NUM_C2K])
     {
         int th = 256;
@@ -933,6 +1260,20 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
         SDL_LAUNCH(k_num_gmem, P.gmem_slots, th, sm, s, rows + off[NUM_GMEM], cnt[NUM_GMEM], na,
                    P.gmem_scratch.get(), P.n);
     }
+}
+
+void product_numeric(const Product &P, const double *Lx, const double *dvec, const double *Ax,
+                     double *Cx, cudaStream_t s)
+{
+    if (P.nnz == 0) return;
+    if (P.num_count[NUM_TILE])
+    {
+        const ProductDesc &d = P.desc;
+        long long nLx = Lx ? d.L_nnz : 0; // prefetch hint only: L_map permutes L_nnz values
+        tile_refill(P.tiles.get(), P.ntiles, P.entries.get(), P.plan.get(), nullptr, s,
+                    ProdPtrs{Lx, dvec, Ax, Cx, nLx, dvec ? d.A_m : 0, d.A_nnz});
+    }
+    big_rows_refill(P, Lx, dvec, Ax, Cx, s);
 }
 
 } // namespace sdl

@@ -163,17 +163,53 @@ enum
 };
 enum
 {
-    NUM_W32 = 0,
-    NUM_W64,
-    NUM_W128,
-    NUM_W256,
-    NUM_W512,
-    NUM_C2K,
+    NUM_TILE = 0, // rows with at most TILE_T terms: row-tile kernel
+    NUM_C2K,      // larger rows with <= 2048 / 8192 entries: CTA per row
     NUM_C8K,
-    NUM_GMEM,
+    NUM_GMEM, // larger rows: CTA per row, accumulator in C.x itself
     NUM_NBINS
 };
-constexpr int NUM_WARP_CLASSES = 5; // NUM_W32 .. NUM_W512 use the planned warp kernel
+// Term budget of a row tile. A tile row costs TILE_T / 256 extra units and a larger
+// row TILE_T, so a tile holds at most 256 rows, at most 2 * TILE_T terms and
+// outputs, and a larger row is always the last row of its tile (the outputs of a
+// tile's rows are one contiguous range of C).
+#ifndef SDL_TILE_T
+#define SDL_TILE_T 1024
+#endif
+constexpr int TILE_T = SDL_TILE_T;
+constexpr int TILE_THREADS = 256;
+
+// Compiled refill schedule of the tile rows (built once per pattern).
+// One record per L entry of a tile row, in upstream's visiting order.
+struct __align__(16) TileEntry
+{
+    int k;                   // row of A (block offset included)
+    int lx;                  // index into the L value array
+    int s;                   // A.p[k]: first entry of A's row k
+    unsigned short toff;     // offset of the entry's first term among the tile's terms
+    unsigned short accbase;  // offset of the entry's output row inside the tile window
+};
+// An entry's term count is the next entry's toff minus its own (the tile's term
+// count for the last entry).
+struct TileDesc
+{
+    long long ent_begin;  // first TileEntry
+    long long plan_begin; // first plan entry (a multiple of 8: 16-byte aligned)
+    int nent;             // entries of the tile
+    int out_begin;        // first output of the tile in C.x
+    int nout;             // outputs of the tile
+    int prod;             // product index (batched refills), 0 for a single product
+    int ordered;          // 1: some output collects >= 3 terms, apply in term order
+    int nterms;           // terms of the tile
+    int pad[2];           // 48 bytes: copied to shared memory as three 16-byte chunks
+};
+// Per-product value pointers read by the refill kernels.
+struct ProdPtrs
+{
+    const double *Lx, *d, *Ax;
+    double *Cx;
+    long long nLx, nd, nAx; // lengths, for the L2 prefetch of the value arrays
+};
 
 struct TuneConfig
 {
@@ -208,11 +244,12 @@ struct Product
     DevBuf<int> num_rows; // row ids grouped by numeric class
     int num_count[NUM_NBINS] = {0};
     int num_offset[NUM_NBINS + 1] = {0};
-    // Plan of the warp-class rows: for every term (in the numeric kernel's visiting
-    // order) its position inside the output row, bit 15 set when the 32-term window
-    // holding it has two terms on one position.
-    DevBuf<unsigned short> plan;
-    DevBuf<long long> plan_off; // m_out + 1
+    // Compiled refill schedule of the tile rows.
+    int ntiles = 0;
+    DevBuf<TileDesc> tiles;
+    DevBuf<TileEntry> entries;
+    DevBuf<unsigned short> plan; // per term: its position inside its output row
+    DevBuf<ProdPtrs> ptrs;       // one slot, rewritten by each refill
     DevBuf<int> gmem_scratch; // posmap scratch for NUM_GMEM rows (slots x n ints)
     int gmem_slots = 0;
     TuneConfig cfg;
@@ -227,5 +264,13 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P,
 // a unit L (every L value 1.0). d: A_m values or nullptr. Never allocates.
 void product_numeric(const Product &P, const double *Lx, const double *d,
                      const double *Ax, double *Cx, cudaStream_t s);
+// The tile refill over a descriptor list that may mix products (batched refills):
+// tile t reads its values through ptrs[tiles[t].prod].
+void tile_refill(const TileDesc *tiles, int ntiles, const TileEntry *entries,
+                 const unsigned short *plan, const ProdPtrs *ptrs, cudaStream_t s,
+                 ProdPtrs single = ProdPtrs{nullptr, nullptr, nullptr, nullptr, 0, 0, 0});
+// The larger rows of one product (CTA kernels), for the given values.
+void big_rows_refill(const Product &P, const double *Lx, const double *d, const double *Ax,
+                     double *Cx, cudaStream_t s);
 
 } // namespace sdl

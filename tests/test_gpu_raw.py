@@ -284,3 +284,25 @@ def test_invalid_input_is_rejected_not_run(sdl):
         assert sdl.sdl_last_status() == 3
     finally:
         sdl.sdl_set_fatal_errors(1)
+
+
+def test_btda_signed_zeros_and_pairs(sdl, orc):
+    """Entries with exactly two terms are added in either order by the fast tile
+    path; with +0.0 / -0.0 / tiny values mixed in, results must still be
+    bit-identical to upstream's ordered sum (0 + a) + b."""
+    rng = np.random.default_rng(91)
+    m, nA, nB = 3000, 400, 300
+    A = wl.fixed_rowlen_csr(m, nA, 6, rng)
+    B = wl.fixed_rowlen_csr(m, nB, 4, rng)
+    ax = A[2].copy()
+    ax[::3] = -0.0
+    ax[1::7] = 0.0
+    ax[2::11] = 1e-300
+    bx = B[2].copy()
+    bx[::5] = -0.0
+    A = (A[0], A[1], ax, A[3], A[4])
+    B = (B[0], B[1], bx, B[3], B[4])
+    d = rng.uniform(0.1, 10, m)
+    d[::13] = -0.0
+    got = gpu_btda(sdl, A, B, d)
+    assert_same(got[0], orc.btda(A, B, d))
