@@ -99,6 +99,21 @@ sdl_status sdl_product_fill(const sdl_product *P, const double *Lx, const double
                             const double *Ax, double *Cx, void *stream);
 void sdl_product_destroy(sdl_product *P);
 
+/* No upstream counterpart. Same result as sdl_product_fill, bit for bit, for
+   callers that cannot call cudaMalloc while they refill: device memory wholly
+   owned by another allocator, a fixed device-memory budget that may not grow, or
+   a latency-critical loop that must not pay cudaMalloc's implicit
+   synchronisation. It allocates nothing: the scratch of the rows with more than
+   8192 outputs is a 16 MiB array inside the library (held by every GPU that
+   loads the library until the process exits), so A may have at most 4194304
+   (4 Mi) columns; larger products are rejected with SDL_ERR_INVALID. The first
+   call on a device looks the array's address up once (with that device
+   current); make that first call before any stream capture. Every call shares
+   the array, so calls that overlap on the GPU race; it needs no clearing between
+   calls. */
+sdl_status sdl_product_fill_noalloc(const sdl_product *P, const double *Lx, const double *d,
+                                    const double *Ax, double *Cx, void *stream);
+
 /* ------------------------------------------------------------------------
    Device-resident stable transpose of a compressed structure (CSR -> CSC,
    CSC -> CSR, A -> A^T). The source is rows x cols with nnz entries; the result

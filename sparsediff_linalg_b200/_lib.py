@@ -100,6 +100,7 @@ EXTENSION_SIGNATURES = {
                                    C.POINTER(vp), C.POINTER(vp)]),
     "sdl_product_fill": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "sdl_product_destroy": (None, [vp]),
+    "sdl_product_fill_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "sdl_transpose_create": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp, C.POINTER(vp)]),
     "sdl_transpose_info": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "sdl_transpose_fill": (C.c_int, [vp, vp, vp, vp]),

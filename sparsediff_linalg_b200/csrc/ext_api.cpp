@@ -115,6 +115,10 @@ extern "C" sdl_status sdl_product_fill(const sdl_product *P, const double *Lx, c
 
 extern "C" void sdl_product_destroy(sdl_product *P) { delete P; }
 
+namespace sdl {
+const Product *product_of(const sdl_product *P) { return P ? &P->P : nullptr; }
+} // namespace sdl
+
 // ------------------------------------------------------------------ transpose
 extern "C" sdl_status sdl_transpose_create(const int *p, const int *idx, int rows, int cols, int nnz,
                                            void *stream, sdl_transpose **out)

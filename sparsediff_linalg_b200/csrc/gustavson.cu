@@ -1262,6 +1262,43 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
     }
 }
 
+void big_rows_refill_scratch(const Product &P, const double *Lx, const double *dvec, const double *Ax,
+                             double *Cx, int *posmap, int slots, cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    const ProductDesc &d = P.desc;
+    NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(),
+               Cx, rt.d_error};
+    const int *rows = P.num_rows.get();
+    const int *off = P.num_offset;
+    const int *cnt = P.num_count;
+    const int cap = rt.num_sms * 16;
+    if (cnt[NUM_C2K])
+    {
+        int th = 256;
+        size_t sm = 2048 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
+        set_smem(k_num_cta<2048>, sm);
+        SDL_LAUNCH(k_num_cta<2048>, grid_for(cnt[NUM_C2K], 1, cap), th, sm, s, rows + off[NUM_C2K],
+                   cnt[NUM_C2K], na);
+    }
+    if (cnt[NUM_C8K])
+    {
+        int th = 512;
+        size_t sm = 8192 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
+        set_smem(k_num_cta<8192>, sm);
+        SDL_LAUNCH(k_num_cta<8192>, grid_for(cnt[NUM_C8K], 1, cap), th, sm, s, rows + off[NUM_C8K],
+                   cnt[NUM_C8K], na);
+    }
+    if (cnt[NUM_GMEM])
+    {
+        int th = 512;
+        size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
+        set_smem(k_num_gmem, sm);
+        SDL_LAUNCH(k_num_gmem, std::min(slots, cnt[NUM_GMEM]), th, sm, s, rows + off[NUM_GMEM],
+                   cnt[NUM_GMEM], na, posmap, P.n);
+    }
+}
+
 void product_numeric(const Product &P, const double *Lx, const double *dvec, const double *Ax,
                      double *Cx, cudaStream_t s)
 {
