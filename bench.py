@@ -49,6 +49,7 @@ def parse():
                     help="budget of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -308,6 +309,10 @@ def run_b200(args, world, rank, local):
     torch.cuda.synchronize()
     sp_num_us = e0.elapsed_time(e1) / 50 * 1e3
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args, dev)
+
     # ---- e2e through the upstream C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -334,6 +339,8 @@ def run_b200(args, world, rank, local):
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if batched is not None:
+        line["batched_512"] = batched
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg)
     if rank == 0:
@@ -376,6 +383,80 @@ def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world):
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": round(t * 1e3, 4),
             "api": "BTDA_matrices_fill_values (host buffers, pageable)"}
+
+
+def run_batched(args, dev, refills=20):
+    """512 uneven B^T D A instances (rows log-uniform 1k..64k, cols = rows / 2, 4..16
+    nnz per row), fixed patterns, `refills` value refills: batched (one persistent
+    launch per refill, replayed from a CUDA graph) vs plain (one refill launch per
+    product). Inputs total several GB, far above L2, so no flush is needed."""
+    import torch
+    from sparsediff_linalg_b200 import workloads as wl
+    from sparsediff_linalg_b200.device import Batch, btda_product
+    t0 = time.perf_counter()
+    inst = wl.batched_device(seed=3, count=512)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    prods, outs = [], []
+    B_alg = 0
+    for k in inst:
+        P, T = btda_product(k["Ap"], k["Ai"], k["n"], k["Bp"], k["Bi"], k["n"])
+        prods.append((P, T))
+        outs.append(torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev))
+        B_alg += algorithmic_bytes_refill(k["Ai"].numel(), k["m"], k["Bi"].numel(), k["n"], k["m"],
+                                          P.nnz, k["n"])
+    torch.cuda.synchronize()
+    sym_s = time.perf_counter() - t0
+    Bt = Batch([p for p, _ in prods])
+    # two value sets per instance, alternated across refills
+    vals = []
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    for k in inst:
+        sets = []
+        for _ in range(2):
+            sets.append((torch.randn(k["Ai"].numel(), generator=g, device=dev, dtype=torch.float64),
+                         torch.randn(k["Bi"].numel(), generator=g, device=dev, dtype=torch.float64),
+                         torch.rand(k["m"], generator=g, device=dev, dtype=torch.float64) * 9.9 + 0.1))
+        vals.append(sets)
+    s = torch.cuda.Stream()
+
+    def bind(which):
+        for i, k in enumerate(inst):
+            ax, bx, d = vals[i][which]
+            Bt.bind(i, bx, d, ax, outs[i])
+
+    def timed(fn):
+        evs = []
+        for r in range(refills):
+            bind(r % 2)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                e0.record(s)
+                fn(s)
+                e1.record(s)
+            evs.append((e0, e1))
+        s.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / refills
+
+    for w in range(3):
+        bind(w % 2)
+        with torch.cuda.stream(s):
+            Bt.refill(stream=s)
+            Bt.refill_unbatched(stream=s)
+    s.synchronize()
+    ms_batched = timed(lambda st: Bt.refill(stream=st))
+    ms_plain = timed(lambda st: Bt.refill_unbatched(stream=st))
+    terms = sum(p.terms for p, _ in prods)
+    return {"instances": len(inst), "refills": refills, "tiles": Bt.tiles,
+            "rows": int(sum(k["m"] for k in inst)),
+            "nnz_A": int(sum(k["Ai"].numel() for k in inst)), "terms": int(terms),
+            "nnz_C": int(sum(p.nnz for p, _ in prods)), "algorithmic_bytes": int(B_alg),
+            "batched_ms_per_refill": round(ms_batched, 4), "plain_ms_per_refill": round(ms_plain, 4),
+            "batched_gbs": round(B_alg / (ms_batched * 1e-3) / 1e9, 2),
+            "plain_gbs": round(B_alg / (ms_plain * 1e-3) / 1e9, 2),
+            "speedup_vs_plain": round(ms_plain / ms_batched, 3),
+            "generate_s": round(gen_s, 2), "symbolic_s": round(sym_s, 2)}
 
 
 def cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg):

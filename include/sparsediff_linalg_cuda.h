@@ -115,6 +115,31 @@ sdl_status sdl_product_fill_noalloc(const sdl_product *P, const double *Lx, cons
                                     const double *Ax, double *Cx, void *stream);
 
 /* ------------------------------------------------------------------------
+   Batched refill: many products (uneven sizes, fixed patterns) refilled by one
+   persistent launch over the union of their compiled tile schedules, captured
+   into a CUDA graph on the first refill and replayed afterwards. Rows with more
+   than the tile budget of terms are refilled by per-product launches inside the
+   same graph.
+   ------------------------------------------------------------------------ */
+typedef struct sdl_batch sdl_batch;
+/* The products must outlive the batch. Synchronises the stream. */
+sdl_status sdl_batch_create(sdl_product *const *products, int count, void *stream,
+                            sdl_batch **out);
+/* Device value arrays of product i used by the following refills (as in
+   sdl_product_fill). Rebinding after the first refill is allowed: the graph reads
+   the pointers from a device table. */
+sdl_status sdl_batch_bind(sdl_batch *B, int i, const double *Lx, const double *d,
+                          const double *Ax, double *Cx);
+/* One refill of every product of the batch, asynchronous on the stream. */
+sdl_status sdl_batch_refill(sdl_batch *B, void *stream);
+/* The same refill as sdl_batch_refill done the plain way: one sdl_product_fill
+   per product (separate launches, no graph). For comparisons. */
+sdl_status sdl_batch_refill_unbatched(sdl_batch *B, void *stream);
+/* Tiles / larger rows of the batch (for reporting). */
+sdl_status sdl_batch_info(const sdl_batch *B, int *tiles, int *big_rows, long long *terms);
+void sdl_batch_destroy(sdl_batch *B);
+
+/* ------------------------------------------------------------------------
    Device-resident stable transpose of a compressed structure (CSR -> CSC,
    CSC -> CSR, A -> A^T). The source is rows x cols with nnz entries; the result
    has cols + 1 offsets, the source row of each entry (ascending within each

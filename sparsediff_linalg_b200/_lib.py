@@ -101,6 +101,12 @@ EXTENSION_SIGNATURES = {
     "sdl_product_fill": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "sdl_product_destroy": (None, [vp]),
     "sdl_product_fill_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "sdl_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, vp, C.POINTER(vp)]),
+    "sdl_batch_bind": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+    "sdl_batch_refill": (C.c_int, [vp, vp]),
+    "sdl_batch_refill_unbatched": (C.c_int, [vp, vp]),
+    "sdl_batch_info": (C.c_int, [vp, c_int_p, c_int_p, C.POINTER(C.c_longlong)]),
+    "sdl_batch_destroy": (None, [vp]),
     "sdl_transpose_create": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp, C.POINTER(vp)]),
     "sdl_transpose_info": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "sdl_transpose_fill": (C.c_int, [vp, vp, vp, vp]),

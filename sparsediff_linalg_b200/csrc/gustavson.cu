@@ -1207,20 +1207,49 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     SDL_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+int g_refill_per_sm = 0;
+
+__global__ void k_rebase_tiles(const TileDesc *__restrict__ src, int n, long long ent_shift,
+                               long long plan_shift, int prod, TileDesc *__restrict__ dst)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+    {
+        TileDesc d = src[t];
+        d.ent_begin += ent_shift;
+        d.plan_begin += plan_shift;
+        d.prod = prod;
+        dst[t] = d;
+    }
+}
+} // namespace
+
+void tile_refill_prepare()
+{
+    if (g_refill_per_sm) return;
+    set_smem(k_tile_refill, refill_smem_bytes());
+    int per_sm = 0;
+    SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_refill, TILE_THREADS,
+                                                           refill_smem_bytes()));
+    g_refill_per_sm = std::max(1, per_sm);
+}
+
+void rebase_tiles(const TileDesc *src, int n, long long ent_shift, long long plan_shift, int prod,
+                  TileDesc *dst, cudaStream_t s)
+{
+    if (n <= 0) return;
+    SDL_LAUNCH(k_rebase_tiles, grid_for(n, 256, runtime().num_sms * 4), 256, 0, s, src, n, ent_shift,
+               plan_shift, prod, dst);
+}
+
 void tile_refill(const TileDesc *tiles, int ntiles, const TileEntry *entries,
                  const unsigned short *plan, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs single)
 {
     if (ntiles <= 0) return;
     Runtime &rt = runtime();
-    static int per_sm = 0;
-    if (!per_sm)
-    {
-        set_smem(k_tile_refill, refill_smem_bytes());
-        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_refill, TILE_THREADS,
-                                                               refill_smem_bytes()));
-        per_sm = std::max(1, per_sm);
-    }
-    int grid = std::min(ntiles, rt.num_sms * per_sm);
+    tile_refill_prepare();
+    int grid = std::min(ntiles, rt.num_sms * g_refill_per_sm);
     SDL_LAUNCH(k_tile_refill, grid, TILE_THREADS, refill_smem_bytes(), s, tiles, ntiles, entries, plan,
                ptrs, single, rt.d_error);
 }

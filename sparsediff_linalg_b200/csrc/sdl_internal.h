@@ -269,6 +269,11 @@ void product_numeric(const Product &P, const double *Lx, const double *d,
 void tile_refill(const TileDesc *tiles, int ntiles, const TileEntry *entries,
                  const unsigned short *plan, const ProdPtrs *ptrs, cudaStream_t s,
                  ProdPtrs single = ProdPtrs{nullptr, nullptr, nullptr, nullptr, 0, 0, 0});
+// One-time kernel attributes of the tile refill (call outside any stream capture).
+void tile_refill_prepare();
+// Copies `n` descriptors, shifting their entry / plan offsets and setting `prod`.
+void rebase_tiles(const TileDesc *src, int n, long long ent_shift, long long plan_shift, int prod,
+                  TileDesc *dst, cudaStream_t s);
 // The larger rows of one product (CTA kernels), for the given values.
 void big_rows_refill(const Product &P, const double *Lx, const double *d, const double *Ax,
                      double *Cx, cudaStream_t s);

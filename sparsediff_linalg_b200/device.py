@@ -138,6 +138,41 @@ class Coalesce:
             pass
 
 
+class Batch:
+    """Batched refill of many products: one persistent launch over all their tiles,
+    replayed from a CUDA graph (sdl_batch_*)."""
+
+    def __init__(self, products, stream=None):
+        L = lib()
+        self._keep = list(products)
+        arr = (C.c_void_p * max(1, len(products)))(*[p.handle for p in products])
+        h = C.c_void_p()
+        check(L.sdl_batch_create(arr, len(products), _stream(stream), C.byref(h)))
+        self.handle = h
+        t, b, n = C.c_int(), C.c_int(), C.c_longlong()
+        check(L.sdl_batch_info(h, C.byref(t), C.byref(b), C.byref(n)))
+        self.tiles, self.big_rows, self.terms = t.value, b.value, n.value
+        self._bound = {}
+
+    def bind(self, i, Lx, d, Ax, Cx):
+        self._bound[i] = (Lx, d, Ax, Cx)
+        check(lib().sdl_batch_bind(self.handle, i, _ptr(Lx), _ptr(d), _ptr(Ax), _ptr(Cx)))
+
+    def refill(self, stream=None):
+        check(lib().sdl_batch_refill(self.handle, _stream(stream)))
+
+    def refill_unbatched(self, stream=None):
+        check(lib().sdl_batch_refill_unbatched(self.handle, _stream(stream)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().sdl_batch_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 def btda_product(A_p, A_i, A_n, B_p, B_i, B_n, stream=None):
     """Device plan of C = B^T D A with A, B given as device CSR structures: B's CSC is
     built by a transpose plan and its values are read through the CSR positions

@@ -152,3 +152,43 @@ def small_random_csr(m, n, density, rng, dist="normal"):
     i = np.nonzero(mask)[1].astype(np.int32)
     x = _values(rng, int(p[-1]), dist, -1.0, 1.0)
     return p, i, x, m, n
+
+
+def batched_device(seed=3, count=512, lo=1_000, hi=64_000, device="cuda"):
+    """The batched configuration generated on the GPU (torch, seeded): `count`
+    instances with rows r ~ log-uniform[lo, hi], cols = r // 2, and for A and B of
+    every instance 4..16 (uniform) distinct uniform columns per row (sorted), N(0,1)
+    values; d ~ U[0.1, 10]. Returns a list of dicts of device tensors
+    (Ap, Ai, Ax, Bp, Bi, Bx, d, m, n)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    gc = torch.Generator()
+    gc.manual_seed(seed)
+    rows = torch.exp(torch.empty(count, dtype=torch.float64).uniform_(
+        float(np.log(lo)), float(np.log(hi)), generator=gc)).long().tolist()
+    out = []
+
+    def one(m, n):
+        draws = 20
+        cols = torch.floor(torch.rand((m, draws), generator=g, device=device, dtype=torch.float64) * n).long()
+        cols, _ = torch.sort(cols, dim=1)
+        uniq = torch.ones_like(cols, dtype=torch.bool)
+        uniq[:, 1:] = cols[:, 1:] != cols[:, :-1]
+        want = torch.randint(4, 17, (m, 1), generator=g, device=device)
+        rank = torch.cumsum(uniq.int(), dim=1)
+        keep = uniq & (rank <= want)
+        lens = keep.sum(dim=1)
+        p = torch.zeros(m + 1, dtype=torch.int32, device=device)
+        p[1:] = torch.cumsum(lens, 0).int()
+        i = cols[keep].int()
+        x = torch.randn(i.numel(), generator=g, device=device, dtype=torch.float64)
+        return p, i, x
+
+    for r in rows:
+        m, n = int(r), max(1, int(r) // 2)
+        Ap, Ai, Ax = one(m, n)
+        Bp, Bi, Bx = one(m, n)
+        d = torch.rand(m, generator=g, device=device, dtype=torch.float64) * 9.9 + 0.1
+        out.append(dict(Ap=Ap, Ai=Ai, Ax=Ax, Bp=Bp, Bi=Bi, Bx=Bx, d=d, m=m, n=n))
+    return out
