@@ -140,6 +140,56 @@ sdl_status sdl_batch_info(const sdl_batch *B, int *tiles, int *big_rows, long lo
 void sdl_batch_destroy(sdl_batch *B);
 
 /* ------------------------------------------------------------------------
+   Learned row scheduler. An 8 -> 32 -> 32 -> 4 FP32 MLP over per-row statistics
+   (L-row length, term count, longest referenced A row, A's width, and ratios of
+   them) predicts each output row's nnz (log1p, regression) and its accumulator
+   class (<= 512, <= 8192, > 8192 outputs). It is trained on the labels the exact
+   symbolic pass produces, by the library's own CUDA forward / backward / Adam
+   kernels. It only changes the schedule: sdl_product_create_learned sizes each
+   row's column scratch from the prediction and redoes the rows that do not fit
+   with the exact pass, so the product is exactly the one sdl_product_create
+   builds.
+   ------------------------------------------------------------------------ */
+#define SDL_MLP_INPUTS 8
+#define SDL_MLP_OUTPUTS 4
+#define SDL_MLP_NPARAMS 1476
+typedef struct sdl_mlp sdl_mlp;
+sdl_status sdl_mlp_create(unsigned long long seed, sdl_mlp **out);
+void sdl_mlp_destroy(sdl_mlp *net);
+/* Parameters as SDL_MLP_NPARAMS host floats: W1[32][8], b1[32], W2[32][32], b2[32],
+   W3[4][32], b3[4]. */
+sdl_status sdl_mlp_get_params(const sdl_mlp *net, float *host_params);
+sdl_status sdl_mlp_set_params(sdl_mlp *net, const float *host_params);
+/* Row statistics of a product: features (device, rows x 8) and, from its exact
+   structure, labels (device, rows x 2: log1p(nnz), class). */
+sdl_status sdl_product_row_stats(const sdl_product *P, float *feat, float *label, void *stream);
+/* Mean loss and its gradient (host, SDL_MLP_NPARAMS floats) over n samples. */
+sdl_status sdl_mlp_gradient(const sdl_mlp *net, const float *feat, const float *label, int n,
+                            float *host_grad, float *loss);
+/* Adam over shuffled mini-batches; *final_loss = mean loss of the last epoch. */
+sdl_status sdl_mlp_train(sdl_mlp *net, const float *feat, const float *label, long long n,
+                         int epochs, int batch, float lr, unsigned long long seed,
+                         float *final_loss);
+/* out (device, n x 4): log1p(nnz) prediction and the three class logits. */
+sdl_status sdl_mlp_predict(const sdl_mlp *net, const float *feat, long long n, float *out,
+                           void *stream);
+typedef struct sdl_learned_stats
+{
+    long long rows;           /* output rows */
+    long long term_bound;     /* sum of the rows' term counts (the plain scratch size) */
+    long long capacity;       /* sum of the learned capacities (the learned scratch size) */
+    long long fallback_rows;  /* rows redone by the exact pass */
+    long long fallback_terms; /* their term counts */
+    long long class_hits;     /* rows whose predicted class was right */
+    long long scratch_bytes;  /* column scratch used, fallback included */
+} sdl_learned_stats;
+sdl_status sdl_product_create_learned(const sdl_product_desc *desc, const sdl_mlp *net,
+                                      float margin, void *stream, sdl_product **out,
+                                      sdl_learned_stats *stats);
+/* Column scratch bytes the symbolic pass of a product used. */
+sdl_status sdl_product_scratch_bytes(const sdl_product *P, long long *bytes);
+
+/* ------------------------------------------------------------------------
    Device-resident stable transpose of a compressed structure (CSR -> CSC,
    CSC -> CSR, A -> A^T). The source is rows x cols with nnz entries; the result
    has cols + 1 offsets, the source row of each entry (ascending within each

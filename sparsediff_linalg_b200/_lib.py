@@ -107,6 +107,18 @@ EXTENSION_SIGNATURES = {
     "sdl_batch_refill_unbatched": (C.c_int, [vp, vp]),
     "sdl_batch_info": (C.c_int, [vp, c_int_p, c_int_p, C.POINTER(C.c_longlong)]),
     "sdl_batch_destroy": (None, [vp]),
+    "sdl_mlp_create": (C.c_int, [C.c_ulonglong, C.POINTER(vp)]),
+    "sdl_mlp_destroy": (None, [vp]),
+    "sdl_mlp_get_params": (C.c_int, [vp, vp]),
+    "sdl_mlp_set_params": (C.c_int, [vp, vp]),
+    "sdl_product_row_stats": (C.c_int, [vp, vp, vp, vp]),
+    "sdl_mlp_gradient": (C.c_int, [vp, vp, vp, C.c_int, vp, C.POINTER(C.c_float)]),
+    "sdl_mlp_train": (C.c_int, [vp, vp, vp, C.c_longlong, C.c_int, C.c_int, C.c_float, C.c_ulonglong,
+                                C.POINTER(C.c_float)]),
+    "sdl_mlp_predict": (C.c_int, [vp, vp, C.c_longlong, vp, vp]),
+    "sdl_product_create_learned": (C.c_int, [C.POINTER(sdl_product_desc), vp, C.c_float, vp, C.POINTER(vp),
+                                             vp]),
+    "sdl_product_scratch_bytes": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
     "sdl_transpose_create": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, vp, C.POINTER(vp)]),
     "sdl_transpose_info": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "sdl_transpose_fill": (C.c_int, [vp, vp, vp, vp]),

@@ -117,6 +117,14 @@ extern "C" void sdl_product_destroy(sdl_product *P) { delete P; }
 
 namespace sdl {
 const Product *product_of(const sdl_product *P) { return P ? &P->P : nullptr; }
+
+sdl_product *product_new_learned(const ProductDesc &d, const Mlp &net, float margin, LearnedStats &st,
+                                 cudaStream_t s)
+{
+    auto p = std::make_unique<sdl_product>();
+    product_symbolic_learned(d, TuneConfig{}, net, margin, p->P, st, s);
+    return p.release();
+}
 } // namespace sdl
 
 // ------------------------------------------------------------------ transpose

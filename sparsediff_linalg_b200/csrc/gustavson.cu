@@ -27,6 +27,7 @@
 
 #include "sdl_device.cuh"
 #include "sdl_internal.h"
+#include "sdl_mlp.h"
 
 namespace sdl {
 
@@ -40,10 +41,17 @@ struct SymArgs
     const int *Lp, *Li;
     int L_m, n_L, n;
     const int *Ap, *Ai;
-    const long long *ub_off;
+    const long long *ub_off; // offset of each row's column scratch
     int *tmp;
     int *row_nnz;
+    const long long *cap;    // learned capacity of each row's scratch (null: its term count)
+    unsigned char *overflow; // set to 1 for a row whose columns did not fit its capacity
 };
+
+__device__ __forceinline__ long long sym_cap(const SymArgs &a, int row)
+{
+    return a.cap ? a.cap[row] : 0x7fffffffffffffffLL;
+}
 
 struct NumArgs
 {
@@ -118,6 +126,14 @@ __global__ void k_sym_classify(const long long *__restrict__ ub, int m_out,
                          : u <= 2048 ? SYM_C2K : u <= 8192 ? SYM_C8K : SYM_BITMAP;
         cls[r] = (unsigned char)c;
     }
+}
+
+// keep the class of the rows flagged in `mask`, drop the others
+__global__ void k_mask_classes(const unsigned char *__restrict__ mask, int m_out, unsigned char *__restrict__ cls)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
+         r += (long long)gridDim.x * blockDim.x)
+        if (!mask[r]) cls[r] = 255;
 }
 
 __global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp,
@@ -226,17 +242,22 @@ __global__ void k_sym_warp(const int *__restrict__ rows, int count, SymArgs a)
         for (int q = cnt + lane; q < P; q += 32) buf[q] = INT_MAX;
         __syncwarp();
         warp_bitonic_sort(buf, P);
-        long long off = a.ub_off[row];
+        long long off = a.ub_off[row], cap = sym_cap(a, row);
         int nn = 0;
         for (int base = 0; base < cnt; base += 32)
         {
             int q = base + lane;
             bool flag = q < cnt && (q == 0 || buf[q] != buf[q - 1]);
             unsigned bal = __ballot_sync(FULL_MASK, flag);
-            if (flag) a.tmp[off + nn + __popc(bal & lanemask_lt())] = buf[q];
+            long long at = nn + __popc(bal & lanemask_lt());
+            if (flag && at < cap) a.tmp[off + at] = buf[q];
             nn += __popc(bal);
         }
-        if (lane == 0) a.row_nnz[row] = nn;
+        if (lane == 0)
+        {
+            a.row_nnz[row] = nn;
+            if (nn > cap) a.overflow[row] = 1;
+        }
         __syncwarp();
     }
 }
@@ -326,20 +347,24 @@ __global__ void k_sym_cta(const int *__restrict__ rows, int count, SymArgs a)
         for (int q = cnt + threadIdx.x; q < P; q += blockDim.x) buf[q] = INT_MAX;
         __syncthreads();
         block_bitonic_sort(buf, P);
-        long long off = a.ub_off[row];
+        long long off = a.ub_off[row], cap = sym_cap(a, row);
         int nn = 0;
         for (int base = 0; base < cnt; base += blockDim.x)
         {
             int q = base + threadIdx.x;
             int flag = (q < cnt && (q == 0 || buf[q] != buf[q - 1])) ? 1 : 0;
             int incl = block_incl_scan_int(flag, ch.scr);
-            if (flag) a.tmp[off + nn + incl - 1] = buf[q];
+            if (flag && nn + incl - 1 < cap) a.tmp[off + nn + incl - 1] = buf[q];
             if (threadIdx.x == blockDim.x - 1) tot_sh = incl;
             __syncthreads();
             nn += tot_sh;
             __syncthreads();
         }
-        if (threadIdx.x == 0) a.row_nnz[row] = nn;
+        if (threadIdx.x == 0)
+        {
+            a.row_nnz[row] = nn;
+            if (nn > cap) a.overflow[row] = 1;
+        }
         __syncthreads();
     }
 }
@@ -363,7 +388,7 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
         int row = rows[it];
         int b = row / a.L_m, r = row - b * a.L_m;
         int ls = a.Lp[r], le = a.Lp[r + 1];
-        long long off = a.ub_off[row];
+        long long off = a.ub_off[row], cap = sym_cap(a, row);
         int running = 0;
         for (long long ws = 0; ws < a.n; ws += wbits)
         {
@@ -394,7 +419,8 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
                 while (word)
                 {
                     int bit = __ffs(word) - 1;
-                    a.tmp[pos++] = (int)(ws + q * 32 + bit);
+                    if (pos - off < cap) a.tmp[pos] = (int)(ws + q * 32 + bit);
+                    ++pos;
                     word &= word - 1;
                 }
             }
@@ -403,7 +429,11 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
             running += tot_sh;
             __syncthreads();
         }
-        if (threadIdx.x == 0) a.row_nnz[row] = running;
+        if (threadIdx.x == 0)
+        {
+            a.row_nnz[row] = running;
+            if (running > cap) a.overflow[row] = 1;
+        }
         __syncthreads();
     }
 }
@@ -1067,10 +1097,56 @@ void set_smem(K kernel, size_t bytes)
 
 } // namespace
 
-void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, cudaStream_t s,
-                      bool keep_row_terms)
+namespace {
+
+// Launches the symbolic kernel of every row class over the binned row lists.
+void sym_launch(const SymArgs &sa, const int *lists, const int *cnt, const int *off,
+                const ProductDesc &d, cudaStream_t s)
 {
     Runtime &rt = runtime();
+    const int cap = rt.num_sms * 16;
+    const int wpb = 8;
+    if (cnt[SYM_W32])
+        SDL_LAUNCH(k_sym_warp<32>, grid_for(cnt[SYM_W32], wpb, cap), wpb * 32, wpb * 32 * 4, s,
+                   lists + off[SYM_W32], cnt[SYM_W32], sa);
+    if (cnt[SYM_W128])
+        SDL_LAUNCH(k_sym_warp<128>, grid_for(cnt[SYM_W128], wpb, cap), wpb * 32, wpb * 128 * 4, s,
+                   lists + off[SYM_W128], cnt[SYM_W128], sa);
+    if (cnt[SYM_W512])
+        SDL_LAUNCH(k_sym_warp<512>, grid_for(cnt[SYM_W512], wpb, cap), wpb * 32, wpb * 512 * 4, s,
+                   lists + off[SYM_W512], cnt[SYM_W512], sa);
+    if (cnt[SYM_C2K])
+    {
+        int th = 256;
+        size_t sm = 2048 * 4 + (3 * th + 32) * 4;
+        SDL_LAUNCH(k_sym_cta<2048>, grid_for(cnt[SYM_C2K], 1, cap), th, sm, s, lists + off[SYM_C2K],
+                   cnt[SYM_C2K], sa);
+    }
+    if (cnt[SYM_C8K])
+    {
+        int th = 512;
+        size_t sm = 8192 * 4 + (3 * th + 32) * 4;
+        set_smem(k_sym_cta<8192>, sm);
+        SDL_LAUNCH(k_sym_cta<8192>, grid_for(cnt[SYM_C8K], 1, cap), th, sm, s, lists + off[SYM_C8K],
+                   cnt[SYM_C8K], sa);
+    }
+    if (cnt[SYM_BITMAP])
+    {
+        int th = 1024;
+        size_t fixed = (3 * th + 32) * 4;
+        long long want_words = ((long long)d.A_n + 31) / 32;
+        long long max_words = (rt.smem_optin - (long long)fixed - 1024) / 4;
+        long long w = std::min((want_words + 31) / 32 * 32, max_words / 32 * 32);
+        int words = (int)std::max<long long>(32, w);
+        size_t sm = (size_t)words * 4 + fixed;
+        set_smem(k_sym_bitmap, sm);
+        SDL_LAUNCH(k_sym_bitmap, grid_for(cnt[SYM_BITMAP], 1, rt.num_sms * 2), th, sm, s,
+                   lists + off[SYM_BITMAP], cnt[SYM_BITMAP], sa, words);
+    }
+}
+
+void validate_product(const ProductDesc &d, const TuneConfig &cfg, Product &P, cudaStream_t s)
+{
     if (d.blocks < 1) fail(SDL_ERR_INVALID, "product: blocks must be >= 1");
     if (d.L_m < 0 || d.A_m < 0 || d.A_n < 0) fail(SDL_ERR_INVALID, "product: negative size");
     if (d.A_m % d.blocks != 0)
@@ -1085,7 +1161,157 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     validate_compressed(d.Lp, d.Li, d.L_m, P.n_L, d.L_nnz, "product operand L", s);
     validate_compressed(d.Ap, d.Ai, d.A_m, d.A_n, d.A_nnz, "product operand A", s);
     if (d.L_map) validate_compressed(nullptr, d.L_map, 0, INT_MAX, d.L_nnz, "product L_map", s);
+}
 
+// Everything the refill needs once C's structure is known: row classes, the
+// compiled tile schedule and the larger rows' scratch.
+void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    const int m_out = P.m_out;
+    DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1), small_ent(m_out),
+        epref((size_t)m_out + 1), small_terms(m_out), spref((size_t)m_out + 1);
+    DevBuf<unsigned char> rcls(m_out);
+    SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub, P.Cp.get(), d.Lp,
+               d.L_m, m_out, rcls.get(), weight.get(), small_ent.get(), small_terms.get());
+    bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
+    exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
+    long long ent_total = exclusive_scan_i64(small_ent.get(), epref.get(), m_out, s);
+    exclusive_scan_i64(small_terms.get(), spref.get(), m_out, s);
+    DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
+    SDL_LAUNCH(k_tile_flags, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, wpref.get(), m_out,
+               flag.get());
+    P.ntiles = exclusive_scan_i32_checked(flag.get(), tile_of.get(), m_out, s);
+    DevBuf<int> tile_start((size_t)P.ntiles + 1);
+    SDL_LAUNCH(k_tile_starts, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, flag.get(),
+               tile_of.get(), m_out, tile_start.get());
+    SDL_CUDA(cudaMemcpyAsync(tile_start.get() + P.ntiles, &P.m_out, sizeof(int), cudaMemcpyHostToDevice, s));
+    DevBuf<long long> padded(std::max(1, P.ntiles)), plan_begin((size_t)P.ntiles + 1);
+    SDL_LAUNCH(k_tile_plan_sizes, grid_for(std::max(1, P.ntiles), 256, rt.num_sms * 8), 256, 0, s,
+               tile_start.get(), spref.get(), P.ntiles, padded.get());
+    long long plan_padded = exclusive_scan_i64(padded.get(), plan_begin.get(), P.ntiles, s);
+    P.tiles.reset(std::max(1, P.ntiles));
+    P.entries.reset(std::max<long long>(1, ent_total));
+    P.plan.reset(plan_padded + 16); // slack for the 16-byte staging copies
+    P.ptrs.reset(1);
+    NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, nullptr, nullptr, d.Ap, d.Ai, nullptr,
+               P.Cp.get(), P.Ci.get(), nullptr, rt.d_error};
+    set_smem(k_tile_build, build_smem_bytes());
+    SDL_LAUNCH(k_tile_build, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
+               tile_start.get(), epref.get(), plan_begin.get(), P.tiles.get(), P.entries.get(),
+               P.plan.get());
+    if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
+    if (P.num_count[NUM_GMEM])
+    {
+        long long per_slot = std::max(1, P.n);
+        long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
+        P.gmem_slots = (int)std::min<long long>({(long long)rt.num_sms, max_slots,
+                                                 (long long)P.num_count[NUM_GMEM]});
+        P.gmem_scratch.reset((size_t)P.gmem_slots * per_slot);
+    }
+}
+
+// Learned row statistics: term count, and from the network the row's capacity
+// (predicted nnz with a margin, never above the term count) and predicted class.
+__global__ void k_row_terms_learned(const int *__restrict__ Lp, const int *__restrict__ Li, int L_m,
+                                    int n_L, int m_out, const int *__restrict__ Ap, int n,
+                                    const float *__restrict__ P, float margin, long long *__restrict__ ub,
+                                    long long *__restrict__ cap, unsigned char *__restrict__ pcls)
+{
+    __shared__ float sp[MLP_NPARAMS];
+    for (int q = threadIdx.x; q < MLP_NPARAMS; q += blockDim.x) sp[q] = P[q];
+    __syncthreads();
+    const int lane = lane_id(), wpb = blockDim.x >> 5;
+    for (long long row = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); row < m_out;
+         row += (long long)gridDim.x * wpb)
+    {
+        int b = (int)(row / L_m), r = (int)(row - (long long)b * L_m);
+        long long sum = 0;
+        int mx = 0;
+        for (int ii = Lp[r] + lane; ii < Lp[r + 1]; ii += 32)
+        {
+            int k = Li[ii] + b * n_L;
+            int len = Ap[k + 1] - Ap[k];
+            sum += len;
+            mx = max(mx, len);
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1)
+        {
+            sum += __shfl_xor_sync(FULL_MASK, sum, o);
+            mx = max(mx, __shfl_xor_sync(FULL_MASK, mx, o));
+        }
+        float f[MLP_IN];
+        {
+            float lu = log1pf((float)sum), lm = log1pf((float)mx), ln = log1pf((float)n);
+            f[0] = log1pf((float)(Lp[r + 1] - Lp[r]));
+            f[1] = lu;
+            f[2] = lm;
+            f[3] = ln;
+            f[4] = fminf(4.f, (float)sum / (float)max(1, n));
+            f[5] = lu - lm;
+            f[6] = lu - ln;
+            f[7] = 1.f;
+        }
+        float mine = 0.f;
+#pragma unroll
+        for (int q = 0; q < MLP_IN; ++q)
+            if (lane == q) mine = f[q];
+        float y = mlp_row_forward(sp, mine);
+        float y1 = __shfl_sync(FULL_MASK, y, 1), y2 = __shfl_sync(FULL_MASK, y, 2),
+              y3 = __shfl_sync(FULL_MASK, y, 3);
+        if (lane == 0)
+        {
+            ub[row] = sum;
+            double pred = expm1((double)fminf(y, 40.f));
+            long long c = (long long)ceil(fmax(0.0, pred) * (1.0 + margin)) + 8;
+            cap[row] = c < sum ? c : sum;
+            pcls[row] = (unsigned char)(y1 >= y2 && y1 >= y3 ? 0 : (y2 >= y3 ? 1 : 2));
+        }
+    }
+}
+
+__global__ void k_overflow_terms(const unsigned char *__restrict__ overflow, const long long *__restrict__ ub,
+                                 int m_out, long long *__restrict__ fb_len)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
+         r += (long long)gridDim.x * blockDim.x)
+        fb_len[r] = overflow[r] ? ub[r] : 0;
+}
+
+__global__ void k_compact_learned(const long long *__restrict__ cap_off, const long long *__restrict__ fb_off,
+                                  const unsigned char *__restrict__ overflow, const int *__restrict__ row_nnz,
+                                  const int *__restrict__ Cp, const int *__restrict__ tmp,
+                                  const int *__restrict__ fb, int *__restrict__ Ci, int m_out)
+{
+    const int lane = lane_id(), wpb = blockDim.x >> 5;
+    for (long long row = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); row < m_out;
+         row += (long long)gridDim.x * wpb)
+    {
+        int nn = row_nnz[row];
+        const int *src = overflow[row] ? fb + fb_off[row] : tmp + cap_off[row];
+        int *dst = Ci + Cp[row];
+        for (int q = lane; q < nn; q += 32) dst[q] = src[q];
+    }
+}
+
+__global__ void k_class_hits(const unsigned char *__restrict__ pcls, const int *__restrict__ Cp, int m_out,
+                             unsigned long long *__restrict__ hits)
+{
+    unsigned long long h = 0;
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
+         r += (long long)gridDim.x * blockDim.x)
+        h += pcls[r] == mlp_class_of(Cp[r + 1] - Cp[r]) ? 1 : 0;
+    atomicAdd(hits, h);
+}
+
+} // namespace
+
+void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, cudaStream_t s,
+                      bool keep_row_terms)
+{
+    Runtime &rt = runtime();
+    validate_product(d, cfg, P, s);
     const int m_out = P.m_out;
     P.Cp.reset((size_t)m_out + 1);
     DevBuf<long long> ub(std::max(1, m_out)), ub_off((size_t)m_out + 1);
@@ -1110,100 +1336,98 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     DevBuf<int> lists;
     int cnt[SYM_NBINS], off[SYM_NBINS + 1];
     bin_items(cls.get(), m_out, SYM_NBINS, lists, cnt, off, s);
-
-    SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, ub_off.get(), tmp.get(), row_nnz.get()};
-    const int cap = rt.num_sms * 16;
-    const int wpb = 8;
-    if (cnt[SYM_W32])
-        SDL_LAUNCH(k_sym_warp<32>, grid_for(cnt[SYM_W32], wpb, cap), wpb * 32, wpb * 32 * 4, s,
-                   lists.get() + off[SYM_W32], cnt[SYM_W32], sa);
-    if (cnt[SYM_W128])
-        SDL_LAUNCH(k_sym_warp<128>, grid_for(cnt[SYM_W128], wpb, cap), wpb * 32, wpb * 128 * 4, s,
-                   lists.get() + off[SYM_W128], cnt[SYM_W128], sa);
-    if (cnt[SYM_W512])
-        SDL_LAUNCH(k_sym_warp<512>, grid_for(cnt[SYM_W512], wpb, cap), wpb * 32, wpb * 512 * 4, s,
-                   lists.get() + off[SYM_W512], cnt[SYM_W512], sa);
-    if (cnt[SYM_C2K])
-    {
-        int th = 256;
-        size_t sm = 2048 * 4 + (3 * th + 32) * 4;
-        SDL_LAUNCH(k_sym_cta<2048>, grid_for(cnt[SYM_C2K], 1, cap), th, sm, s,
-                   lists.get() + off[SYM_C2K], cnt[SYM_C2K], sa);
-    }
-    if (cnt[SYM_C8K])
-    {
-        int th = 512;
-        size_t sm = 8192 * 4 + (3 * th + 32) * 4;
-        set_smem(k_sym_cta<8192>, sm);
-        SDL_LAUNCH(k_sym_cta<8192>, grid_for(cnt[SYM_C8K], 1, cap), th, sm, s,
-                   lists.get() + off[SYM_C8K], cnt[SYM_C8K], sa);
-    }
-    if (cnt[SYM_BITMAP])
-    {
-        int th = 1024;
-        size_t fixed = (3 * th + 32) * 4;
-        long long want_words = ((long long)d.A_n + 31) / 32;
-        long long max_words = (rt.smem_optin - (long long)fixed - 1024) / 4;
-        long long w = std::min((want_words + 31) / 32 * 32, max_words / 32 * 32);
-        int words = (int)std::max<long long>(32, w);
-        size_t sm = (size_t)words * 4 + fixed;
-        set_smem(k_sym_bitmap, sm);
-        SDL_LAUNCH(k_sym_bitmap, grid_for(cnt[SYM_BITMAP], 1, rt.num_sms * 2), th, sm, s,
-                   lists.get() + off[SYM_BITMAP], cnt[SYM_BITMAP], sa, words);
-    }
+    SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, ub_off.get(), tmp.get(), row_nnz.get(),
+               nullptr, nullptr};
+    sym_launch(sa, lists.get(), cnt, off, d, s);
 
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
     if (P.nnz > 0)
         SDL_LAUNCH(k_compact, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, ub_off.get(),
                    row_nnz.get(), P.Cp.get(), tmp.get(), P.Ci.get(), m_out);
-
-    {
-        DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1), small_ent(m_out),
-            epref((size_t)m_out + 1), small_terms(m_out), spref((size_t)m_out + 1);
-        DevBuf<unsigned char> rcls(m_out);
-        SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(),
-                   P.Cp.get(), d.Lp, d.L_m, m_out, rcls.get(), weight.get(), small_ent.get(),
-                   small_terms.get());
-        bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
-        exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
-        long long ent_total = exclusive_scan_i64(small_ent.get(), epref.get(), m_out, s);
-        long long plan_total = exclusive_scan_i64(small_terms.get(), spref.get(), m_out, s);
-        DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
-        SDL_LAUNCH(k_tile_flags, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, wpref.get(), m_out,
-                   flag.get());
-        P.ntiles = exclusive_scan_i32_checked(flag.get(), tile_of.get(), m_out, s);
-        DevBuf<int> tile_start((size_t)P.ntiles + 1);
-        SDL_LAUNCH(k_tile_starts, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, flag.get(),
-                   tile_of.get(), m_out, tile_start.get());
-        SDL_CUDA(cudaMemcpyAsync(tile_start.get() + P.ntiles, &m_out, sizeof(int),
-                                 cudaMemcpyHostToDevice, s));
-        DevBuf<long long> padded(std::max(1, P.ntiles)), plan_begin((size_t)P.ntiles + 1);
-        SDL_LAUNCH(k_tile_plan_sizes, grid_for(std::max(1, P.ntiles), 256, rt.num_sms * 8), 256, 0, s,
-                   tile_start.get(), spref.get(), P.ntiles, padded.get());
-        long long plan_padded = exclusive_scan_i64(padded.get(), plan_begin.get(), P.ntiles, s);
-        (void)plan_total;
-        P.tiles.reset(std::max(1, P.ntiles));
-        P.entries.reset(std::max<long long>(1, ent_total));
-        P.plan.reset(plan_padded + 16); // slack for the 16-byte staging copies
-        P.ptrs.reset(1);
-        NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, nullptr, nullptr, d.Ap, d.Ai, nullptr,
-                   P.Cp.get(), P.Ci.get(), nullptr, rt.d_error};
-        set_smem(k_tile_build, build_smem_bytes());
-        SDL_LAUNCH(k_tile_build, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
-                   tile_start.get(), epref.get(), plan_begin.get(), P.tiles.get(), P.entries.get(),
-                   P.plan.get());
-        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
-    }
-    if (P.num_count[NUM_GMEM])
-    {
-        long long per_slot = std::max(1, P.n);
-        long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
-        P.gmem_slots = (int)std::min<long long>({(long long)rt.num_sms, max_slots,
-                                                 (long long)P.num_count[NUM_GMEM]});
-        P.gmem_scratch.reset((size_t)P.gmem_slots * per_slot);
-    }
+    P.scratch_bytes = (long long)tmp.bytes();
+    build_schedule(d, P, ub.get(), s);
     if (keep_row_terms) P.row_terms = std::move(ub);
+    SDL_CUDA(cudaStreamSynchronize(s));
+}
+
+void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const Mlp &net, float margin,
+                              Product &P, LearnedStats &st, cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    validate_product(d, cfg, P, s);
+    const int m_out = P.m_out;
+    st = LearnedStats{};
+    P.Cp.reset((size_t)m_out + 1);
+    if (m_out == 0)
+    {
+        SDL_CUDA(cudaMemsetAsync(P.Cp.get(), 0, sizeof(int), s));
+        P.nnz = 0;
+        P.terms = 0;
+        SDL_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    DevBuf<long long> ub(m_out), cap(m_out), cap_off((size_t)m_out + 1), ub_off((size_t)m_out + 1);
+    DevBuf<unsigned char> pcls(m_out), overflow(m_out);
+    SDL_LAUNCH(k_row_terms_learned, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, d.Lp, d.Li, d.L_m,
+               P.n_L, m_out, d.Ap, d.A_n, net.params.get(), margin, ub.get(), cap.get(), pcls.get());
+    P.terms = exclusive_scan_i64(ub.get(), ub_off.get(), m_out, s);
+    st.cap_total = exclusive_scan_i64(cap.get(), cap_off.get(), m_out, s);
+    st.ub_total = P.terms;
+
+    DevBuf<int> row_nnz(m_out);
+    SDL_CUDA(cudaMemsetAsync(row_nnz.get(), 0, row_nnz.bytes(), s));
+    SDL_CUDA(cudaMemsetAsync(overflow.get(), 0, overflow.bytes(), s));
+    DevBuf<int> tmp(std::max<long long>(1, st.cap_total));
+    DevBuf<unsigned char> cls(m_out);
+    SDL_LAUNCH(k_sym_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(), m_out, cls.get());
+    DevBuf<int> lists;
+    int cnt[SYM_NBINS], off[SYM_NBINS + 1];
+    bin_items(cls.get(), m_out, SYM_NBINS, lists, cnt, off, s);
+    SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, cap_off.get(), tmp.get(), row_nnz.get(),
+               cap.get(), overflow.get()};
+    sym_launch(sa, lists.get(), cnt, off, d, s);
+
+    // rows whose columns did not fit: the exact pass again, into term-count space
+    DevBuf<long long> fb_len(m_out), fb_off((size_t)m_out + 1);
+    SDL_LAUNCH(k_overflow_terms, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, overflow.get(), ub.get(),
+               m_out, fb_len.get());
+    st.fallback_terms = exclusive_scan_i64(fb_len.get(), fb_off.get(), m_out, s);
+    DevBuf<int> fb(std::max<long long>(1, st.fallback_terms));
+    if (st.fallback_terms > 0)
+    {
+        // classes of the overflowing rows only
+        DevBuf<unsigned char> fcls(m_out);
+        SDL_CUDA(cudaMemcpyAsync(fcls.get(), cls.get(), m_out, cudaMemcpyDeviceToDevice, s));
+        SDL_LAUNCH(k_mask_classes, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, overflow.get(), m_out,
+                   fcls.get());
+        DevBuf<int> flists;
+        int fcnt[SYM_NBINS], foff[SYM_NBINS + 1];
+        bin_items(fcls.get(), m_out, SYM_NBINS, flists, fcnt, foff, s);
+        for (int c = 0; c < SYM_NBINS; ++c) st.fallback_rows += fcnt[c];
+        SymArgs fa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, fb_off.get(), fb.get(), row_nnz.get(),
+                   nullptr, nullptr};
+        sym_launch(fa, flists.get(), fcnt, foff, d, s);
+    }
+    P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
+    P.Ci.reset(std::max(1, P.nnz));
+    if (P.nnz > 0)
+        SDL_LAUNCH(k_compact_learned, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, cap_off.get(),
+                   fb_off.get(), overflow.get(), row_nnz.get(), P.Cp.get(), tmp.get(), fb.get(), P.Ci.get(),
+                   m_out);
+    {
+        DevBuf<unsigned long long> hits(1);
+        SDL_CUDA(cudaMemsetAsync(hits.get(), 0, 8, s));
+        SDL_LAUNCH(k_class_hits, grid_for(m_out, 256, rt.num_sms * 4), 256, 0, s, pcls.get(), P.Cp.get(),
+                   m_out, hits.get());
+        unsigned long long h = 0;
+        SDL_CUDA(cudaMemcpyAsync(&h, hits.get(), 8, cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaStreamSynchronize(s));
+        st.class_hits = (long long)h;
+        st.rows = m_out;
+    }
+    P.scratch_bytes = (long long)tmp.bytes() + (long long)fb.bytes();
+    build_schedule(d, P, ub.get(), s);
     SDL_CUDA(cudaStreamSynchronize(s));
 }
 

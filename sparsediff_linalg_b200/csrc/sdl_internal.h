@@ -240,6 +240,7 @@ struct Product
     ProductDesc desc;
     int m_out = 0, n = 0, nnz = 0, n_L = 0;
     long long terms = 0;
+    long long scratch_bytes = 0; // column scratch the symbolic pass used
     DevBuf<int> Cp, Ci;
     DevBuf<int> num_rows; // row ids grouped by numeric class
     int num_count[NUM_NBINS] = {0};
@@ -260,6 +261,20 @@ struct Product
 // Symbolic phase: fills P.Cp, P.Ci, P.nnz and the numeric schedule.
 void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P,
                       cudaStream_t s, bool keep_row_terms = false);
+// Statistics of a learned symbolic pass.
+struct LearnedStats
+{
+    long long rows = 0, ub_total = 0, cap_total = 0, fallback_terms = 0, fallback_rows = 0,
+              class_hits = 0;
+};
+struct Mlp;
+// Symbolic phase with the learned row scheduler: each row's column scratch is
+// sized from the network's predicted nnz (times 1 + margin) instead of its term
+// count; rows that do not fit are redone by the exact pass. The structure is the
+// exact one in every case.
+void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const Mlp &net, float margin,
+                              Product &P, LearnedStats &st, cudaStream_t s);
+
 // Numeric phase. Lx: values of L (indexed through L_map when set), or nullptr for
 // a unit L (every L value 1.0). d: A_m values or nullptr. Never allocates.
 void product_numeric(const Product &P, const double *Lx, const double *d,

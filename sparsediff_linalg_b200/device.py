@@ -58,6 +58,10 @@ class Product:
             Ap.numel() - 1, A_n, Ai.numel())
         h = C.c_void_p()
         check(L.sdl_product_create(C.byref(desc), _stream(stream), C.byref(h)))
+        self._init_from_handle(h)
+
+    def _init_from_handle(self, h):
+        L = lib()
         self.handle = h
         m, n, nnz = C.c_int(), C.c_int(), C.c_int()
         terms = C.c_longlong()

@@ -192,3 +192,45 @@ def batched_device(seed=3, count=512, lo=1_000, hi=64_000, device="cuda"):
         d = torch.rand(m, generator=g, device=device, dtype=torch.float64) * 9.9 + 0.1
         out.append(dict(Ap=Ap, Ai=Ai, Ax=Ax, Bp=Bp, Bi=Bi, Bx=Bx, d=d, m=m, n=n))
     return out
+
+
+def skewed_device(seed=0, m=1_000_000, n=1_000_000, alpha=1.5, target=20_000_000, cap=50_000,
+                  device="cuda"):
+    """A, B (m x n) generated on the GPU with Zipf(alpha) row lengths
+    min(cap, ceil(s * z)) (s found by bisection so the total is ~target) and
+    distinct uniform columns per row (sorted), N(0, 1) values. Returns
+    ((Ap, Ai, Ax), (Bp, Bi, Bx), scales) as device tensors. The Zipf draws use
+    numpy (seeded); columns and values use a seeded torch generator."""
+    import torch
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+
+    def one():
+        lens, sc = zipf_lengths(m, alpha, target, cap, rng)
+        lens_t = torch.as_tensor(lens, device=device)
+        nnz = int(lens.sum())
+        p = torch.zeros(m + 1, dtype=torch.int64, device=device)
+        p[1:] = torch.cumsum(lens_t, 0)
+        row = torch.repeat_interleave(torch.arange(m, device=device), lens_t)
+        # draw, sort within rows, redraw duplicates until every row is distinct
+        col = torch.randint(0, n, (nnz,), generator=g, device=device)
+        for _ in range(64):
+            key = row * n + col
+            key, order = torch.sort(key)
+            col = col[order]
+            dup = torch.zeros(nnz, dtype=torch.bool, device=device)
+            dup[1:] = key[1:] == key[:-1]
+            nd = int(dup.sum())
+            if nd == 0:
+                break
+            col[dup] = torch.randint(0, n, (nd,), generator=g, device=device)
+        key = row * n + col
+        key, _ = torch.sort(key)
+        col = (key % n).int()
+        x = torch.randn(nnz, generator=g, device=device, dtype=torch.float64)
+        return (p.int(), col, x), sc
+
+    A, sa = one()
+    B, sb = one()
+    return A, B, (sa, sb)
