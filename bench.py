@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-matrices", type=int, default=200)
     return ap.parse_args()
 
 
@@ -312,6 +314,9 @@ def run_b200(args, world, rank, local):
     batched = None
     if not args.no_batched:
         batched = run_batched(args, dev)
+    learned = None
+    if not args.no_learned:
+        learned = run_learned(args, dev)
 
     # ---- e2e through the upstream C ABI with host buffers
     e2e = None
@@ -341,6 +346,8 @@ def run_b200(args, world, rank, local):
         line["e2e"] = e2e
     if batched is not None:
         line["batched_512"] = batched
+    if learned is not None:
+        line["learned_skewed"] = learned
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg)
     if rank == 0:
@@ -457,6 +464,61 @@ def run_batched(args, dev, refills=20):
             "plain_gbs": round(B_alg / (ms_plain * 1e-3) / 1e9, 2),
             "speedup_vs_plain": round(ms_plain / ms_batched, 3),
             "generate_s": round(gen_s, 2), "symbolic_s": round(sym_s, 2)}
+
+
+def run_learned(args, dev):
+    """Skewed SpGEMM C = A B, A and B 1M x 1M with Zipf(1.5) row lengths (~20M nnz
+    each, rows capped at 50k): the plain exact symbolic pass + refill against the
+    learned one (scratch sized by the network, exact fallback) + refill. The
+    network is trained first on the row statistics of 200 seeded smaller matrices
+    of the same recipe. Structures are compared for equality."""
+    import torch
+    from sparsediff_linalg_b200 import workloads as wl
+    from sparsediff_linalg_b200.device import Product
+    from sparsediff_linalg_b200.learned import LearnedProduct, scratch_bytes
+    from sparsediff_linalg_b200.train_scheduler import train
+    net, info = train(matrices=args.learned_matrices, epochs=8)
+    t0 = time.perf_counter()
+    (Ap, Ai, Ax), (Bp, Bi, Bx), scales = wl.skewed_device(seed=0)
+    gen_s = time.perf_counter() - t0
+
+    def once(make):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        P = make()
+        torch.cuda.synchronize()
+        t_sym = time.perf_counter() - t0
+        Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev)
+        P.fill(Ax, None, Bx, Cx)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.fill(Ax, None, Bx, Cx)
+        e1.record()
+        torch.cuda.synchronize()
+        return P, t_sym * 1e3, e0.elapsed_time(e1), Cx
+
+    m = Ap.numel() - 1
+    plain, ps, pn, cx_plain = once(lambda: Product(Ap, Ai, Bp, Bi, m))
+    plain_scratch = scratch_bytes(plain)
+    plain_cp, plain_ci = plain.Cp.clone(), plain.Ci.clone()
+    del plain
+    torch.cuda.empty_cache()
+    learned, ls, ln, cx_learned = once(lambda: LearnedProduct(Ap, Ai, Bp, Bi, m, net, margin=0.25))
+    same = bool(torch.equal(plain_cp, learned.Cp) and torch.equal(plain_ci, learned.Ci) and
+                torch.equal(cx_plain.view(torch.int64), cx_learned.view(torch.int64)))
+    st = learned.stats
+    return {"workload": "C = A B, A and B 1M x 1M, Zipf(1.5) row lengths scaled to ~20M nnz, cap 50k",
+            "nnz_A": int(Ai.numel()), "nnz_B": int(Bi.numel()), "terms": int(learned.terms),
+            "nnz_C": int(learned.nnz), "zipf_scale": [round(x, 6) for x in scales],
+            "plain": {"symbolic_ms": round(ps, 2), "numeric_ms": round(pn, 3),
+                      "scratch_bytes": int(plain_scratch)},
+            "learned": {"symbolic_ms": round(ls, 2), "numeric_ms": round(ln, 3),
+                        "scratch_bytes": int(st["scratch_bytes"]), "fallback_rows": st["fallback_rows"],
+                        "class_accuracy": round(st["class_hits"] / max(1, st["rows"]), 4),
+                        "capacity_over_nnz": round(st["capacity"] / max(1, learned.nnz), 4),
+                        "term_bound_over_nnz": round(st["term_bound"] / max(1, learned.nnz), 4)},
+            "identical_structure_and_values": same, "training": info, "generate_s": round(gen_s, 2)}
 
 
 def cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg):
