@@ -1,8 +1,10 @@
-// Batched refill engine (sdl_batch_*): many products refilled by one persistent
-// launch over the union of their compiled tile schedules, replayed from a CUDA
-// graph. The plain alternative -- one sdl_product_fill per product -- pays one
-// launch (and its ramp-up and tail) per product; here all products' tiles share
-// one grid of resident CTAs and one graph launch.
+// Batched refill engine (sdl_batch_*): many products refilled by two launches over
+// the union of their compiled schedules (the entry values of every product, then
+// every product's tiles), replayed from a CUDA graph. The plain alternative -- one
+// sdl_product_fill per product -- pays two launches (and their ramp-up and tail)
+// per product; here all products share one grid and one graph launch. Each
+// product's schedule and entry-value scratch stay where the product keeps them;
+// the kernels find them through per-product pointer tables.
 #include <memory>
 #include <vector>
 
@@ -21,8 +23,10 @@ struct sdl_batch
     long long terms = 0;
     int big_rows = 0;
     DevBuf<TileDesc> tiles;
-    DevBuf<TileEntry> entries;
-    DevBuf<unsigned short> plan;
+    DevBuf<ProdSched> scheds;
+    DevBuf<EntChunk> chunks;
+    int nchunks = 0;
+    unsigned long long launches_per_refill = 0; // kernels one refill launches (graph replays)
     DevBuf<ProdPtrs> ptrs;
     std::vector<ProdPtrs> host_ptrs;
     std::vector<int> with_big; // products that have rows beyond the tile budget
@@ -44,48 +48,45 @@ extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, 
         *out = nullptr;
         cudaStream_t s = pick_stream(stream);
         auto B = std::make_unique<sdl_batch>();
-        long long ents = 0, plans = 0;
         for (int i = 0; i < count; ++i)
         {
             const Product *P = product_of(products[i]);
             if (!P) fail(SDL_ERR_INVALID, "NULL product in batch");
+            for (const Product *Q : B->prods)
+                if (Q == P) fail(SDL_ERR_INVALID, "a product appears twice in the batch");
             B->prods.push_back(P);
             B->ntiles += P->num_count[NUM_TILE] ? P->ntiles : 0;
-            ents += (long long)P->entries.n;
-            plans += ((long long)P->plan.n + 7) & ~7LL;
             B->terms += P->terms;
             int big = P->num_count[NUM_C2K] + P->num_count[NUM_C8K] + P->num_count[NUM_GMEM];
             B->big_rows += big;
             if (big) B->with_big.push_back(i);
         }
         B->tiles.reset(std::max(1, B->ntiles));
-        B->entries.reset(std::max<long long>(1, ents));
-        B->plan.reset(std::max<long long>(16, plans));
         B->ptrs.reset(std::max(1, count));
-        B->host_ptrs.assign(count, ProdPtrs{nullptr, nullptr, nullptr, nullptr, 0, 0, 0});
-        long long e_off = 0, p_off = 0;
+        B->scheds.reset(std::max(1, count));
+        B->host_ptrs.assign(count, ProdPtrs{nullptr, nullptr, nullptr, nullptr});
+        std::vector<ProdSched> hs(count);
+        std::vector<EntChunk> chunks;
         int t_off = 0;
         for (int i = 0; i < count; ++i)
         {
             const Product *P = B->prods[i];
-            if (P->entries.n)
-                SDL_CUDA(cudaMemcpyAsync(B->entries.get() + e_off, P->entries.get(), P->entries.bytes(),
-                                         cudaMemcpyDeviceToDevice, s));
-            if (P->plan.n)
-                SDL_CUDA(cudaMemcpyAsync(B->plan.get() + p_off, P->plan.get(), P->plan.bytes(),
-                                         cudaMemcpyDeviceToDevice, s));
+            hs[i] = sched_of(*P);
             if (P->num_count[NUM_TILE] && P->ntiles)
             {
-                rebase_tiles(P->tiles.get(), P->ntiles, e_off, p_off, i, B->tiles.get() + t_off, s);
+                rebase_tiles(P->tiles.get(), P->ntiles, i, B->tiles.get() + t_off, s);
                 t_off += P->ntiles;
+                append_entry_chunks(hs[i].nV, i, 2048, chunks);
             }
-            e_off += (long long)P->entries.n;
-            // plan blocks keep their 16-byte alignment: every product's plan length
-            // is padded to a multiple of 8 entries
-            p_off += ((long long)P->plan.n + 7) & ~7LL;
-            if (p_off > plans) fail(SDL_ERR_INTERNAL, "batch plan layout");
         }
-        tile_refill_prepare();
+        if (count)
+            SDL_CUDA(cudaMemcpyAsync(B->scheds.get(), hs.data(), count * sizeof(ProdSched),
+                                     cudaMemcpyHostToDevice, s));
+        B->nchunks = (int)chunks.size();
+        B->chunks.reset(std::max<size_t>(1, chunks.size()));
+        if (!chunks.empty())
+            SDL_CUDA(cudaMemcpyAsync(B->chunks.get(), chunks.data(), chunks.size() * sizeof(EntChunk),
+                                     cudaMemcpyHostToDevice, s));
         SDL_CUDA(cudaStreamSynchronize(s));
         *out = B.release();
     });
@@ -98,8 +99,7 @@ extern "C" sdl_status sdl_batch_bind(sdl_batch *B, int i, const double *Lx, cons
         if (!B || i < 0 || i >= (int)B->prods.size()) fail(SDL_ERR_INVALID, "bad batch index");
         const Product *P = B->prods[i];
         if (P->nnz > 0 && (!Ax || !Cx)) fail(SDL_ERR_INVALID, "NULL value pointer");
-        const ProductDesc &dd = P->desc;
-        B->host_ptrs[i] = ProdPtrs{Lx, d, Ax, Cx, Lx ? dd.L_nnz : 0, d ? dd.A_m : 0, dd.A_nnz};
+        B->host_ptrs[i] = ProdPtrs{Lx, d, Ax, Cx};
         SDL_CUDA(cudaMemcpy(B->ptrs.get() + i, &B->host_ptrs[i], sizeof(ProdPtrs), cudaMemcpyHostToDevice));
     });
 }
@@ -115,18 +115,21 @@ extern "C" sdl_status sdl_batch_refill(sdl_batch *B, void *stream)
         if (s == cudaStreamLegacy)
             fail(SDL_ERR_INVALID, "batched refills need a non-default stream (graph capture)");
         auto enqueue = [&]() {
-            tile_refill(B->tiles.get(), B->ntiles, B->entries.get(), B->plan.get(), B->ptrs.get(), s);
+            entry_values_batched(B->chunks.get(), B->nchunks, B->ptrs.get(), B->scheds.get(), s);
+            tile_refill(B->tiles.get(), B->ntiles, B->ptrs.get(), B->scheds.get(), s);
             for (int i : B->with_big)
             {
                 const ProdPtrs &pp = B->host_ptrs[i];
-                big_rows_refill(*B->prods[i], pp.Lx, pp.d, pp.Ax, pp.Cx, s);
+                big_rows_refill(*B->prods[i], pp.Lx, pp.d, pp.Ax, pp.Cx, s, B->ptrs.get() + i);
             }
         };
         if (!B->exec)
         {
             // first refill runs eagerly (every lazily set kernel attribute is set
             // outside any capture), then the same launches are captured once
+            const unsigned long long l0 = g_launches.load();
             enqueue();
+            B->launches_per_refill = g_launches.load() - l0;
             SDL_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             try
             {
@@ -140,11 +143,13 @@ extern "C" sdl_status sdl_batch_refill(sdl_batch *B, void *stream)
                 throw;
             }
             SDL_CUDA(cudaStreamEndCapture(s, &B->graph));
+            // captured launches are not executions: only replays count
+            g_launches.fetch_sub(B->launches_per_refill, std::memory_order_relaxed);
             SDL_CUDA(cudaGraphInstantiate(&B->exec, B->graph, 0));
             return;
         }
         SDL_CUDA(cudaGraphLaunch(B->exec, s));
-        g_launches.fetch_add(1 + B->with_big.size(), std::memory_order_relaxed);
+        g_launches.fetch_add(B->launches_per_refill, std::memory_order_relaxed);
     });
 }
 

@@ -17,7 +17,7 @@
 //             bitmap over column windows (larger rows; the bitmap yields the
 //             columns already sorted);
 //   numeric:  row tiles (rows of <= TILE_T terms, grouped into CTA-sized tiles,
-//             with a per-term position plan built once per pattern), CTA + shared
+//             with an output-major schedule built once per pattern), CTA + shared
 //             accumulator (<= 8192 output entries), CTA + accumulator in C.x itself
 //             with a global column->position map (larger rows).
 #include <algorithm>
@@ -63,6 +63,7 @@ struct NumArgs
     const int *Cp, *Ci;
     double *Cx;
     int *err;
+    int L_nnz; // entries of L (schedule build: entry index b * L_nnz + ii)
 };
 
 // ------------------------------------------------------------ row statistics
@@ -136,10 +137,8 @@ __global__ void k_mask_classes(const unsigned char *__restrict__ mask, int m_out
         if (!mask[r]) cls[r] = 255;
 }
 
-__global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp,
-                               const int *__restrict__ Lp, int L_m, int m_out,
-                               unsigned char *__restrict__ cls, long long *__restrict__ weight,
-                               long long *__restrict__ small_ent, long long *__restrict__ small_terms)
+__global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp, int m_out,
+                               unsigned char *__restrict__ cls, long long *__restrict__ weight)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
          r += (long long)gridDim.x * blockDim.x)
@@ -158,9 +157,6 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
         else
             c = NUM_GMEM;
         cls[r] = (unsigned char)c;
-        int rr = (int)(r % L_m);
-        small_ent[r] = c == NUM_TILE ? Lp[rr + 1] - Lp[rr] : 0;
-        small_terms[r] = c == NUM_TILE ? u : 0;
         weight[r] = c == NUM_TILE ? u + TILE_T / TILE_THREADS : (c == 255 ? TILE_T / TILE_THREADS : TILE_T);
     }
 }
@@ -172,18 +168,6 @@ __global__ void k_tile_flags(const long long *__restrict__ wpref, int m_out, int
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
          r += (long long)gridDim.x * blockDim.x)
         flag[r] = (r == 0 || wpref[r] / TILE_T != wpref[r - 1] / TILE_T) ? 1 : 0;
-}
-
-// padded (to 8 entries = 16 bytes) plan length of every tile
-__global__ void k_tile_plan_sizes(const int *__restrict__ tile_start, const long long *__restrict__ spref,
-                                  int ntiles, long long *__restrict__ padded)
-{
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles;
-         t += (long long)gridDim.x * blockDim.x)
-    {
-        long long n = spref[tile_start[t + 1]] - spref[tile_start[t]];
-        padded[t] = (n + 7) & ~7LL;
-    }
 }
 
 __global__ void k_tile_starts(const int *__restrict__ flag, const int *__restrict__ tile_of, int m_out,
@@ -455,8 +439,8 @@ __global__ void k_compact(const long long *__restrict__ ub_off, const int *__res
 
 // ------------------------------------------------------------ numeric kernels
 // ------------------------------------------------------------ row tiles
+// Outputs and terms of a tile are each below 2 * TILE_T.
 constexpr int TILE_ACC = 2 * TILE_T;
-constexpr int TILE_CLAIM = 1024; // hashed claim slots of the ordered path
 
 // last index q in [0, n) with a[q] <= key (a non-decreasing, a[0] <= key)
 __device__ __forceinline__ int last_le(const int *a, int n, int key)
@@ -475,447 +459,516 @@ __device__ __forceinline__ int last_le(const int *a, int n, int key)
 
 struct BuildSmem
 {
-    int *cnt; // TILE_ACC multiplicity counters
-    int *row_cs, *row_ls, *row_b, *row_accoff, *row_eoff;
-    int *e_incl, *e_s, *e_len, *e_row;
+    int *cnt;  // TILE_ACC: terms per output (pass A)
+    int *cur;  // TILE_ACC: term-list cursor of a multi-term output, -1 otherwise
+    int *row_cs, *row_nr, *row_ls, *row_b, *row_outoff, *row_eoff;
+    int *e_incl, *e_s, *e_len, *e_row, *e_ii;
     int *scr;
+    int *misc; // [1]: multi-term outputs of a chunk, [2]: their terms
 };
 constexpr size_t build_smem_bytes()
 {
-    return ((size_t)TILE_ACC + 3 * TILE_THREADS + 2 * (TILE_THREADS + 1) + 4 * TILE_THREADS + 32) * 4;
+    return ((size_t)2 * TILE_ACC + 4 * TILE_THREADS + 2 * (TILE_THREADS + 1) + 5 * TILE_THREADS + 32 + 4) * 4;
 }
 
-// Compiles the refill schedule of one tile (one CTA per tile, once per pattern):
-// the tile descriptor, one TileEntry per L entry of the tile rows, and the plan:
-// the position of every term inside its output row (binary search in the sorted
-// row) in upstream's visiting order, bit 15 marking a term whose output collects
-// exactly two terms. A tile is marked ordered when one of its output entries
-// collects three or more terms: with at most two terms per entry
-// the order of the additions cannot change the result ((0 + a) + b == (0 + b) + a
-// bit for bit, signed zeros included), so only ordered tiles need upstream's
-// exact order at refill time.
-__global__ void __launch_bounds__(TILE_THREADS) k_tile_build(
+// Term enumeration of one tile, shared by both passes of the schedule build: calls
+// f(valid, e, jj, o) for every term of the tile in upstream's visiting order, 256
+// consecutive terms per step (valid false for the idle threads of the last step,
+// so every thread takes every barrier). e is the term's entry of kron(I_blocks, L)
+// (b * L_nnz + ii), jj its position in A, o its output inside the tile window.
+template <class F>
+__device__ __forceinline__ void tile_terms(const NumArgs &a, const BuildSmem &t, int nrows, int total_raw, F f)
+{
+    const int tid = threadIdx.x;
+    for (int ec = 0; ec < total_raw; ec += TILE_THREADS)
+    {
+        const int e = ec + tid;
+        int s = 0, len = 0, lrow = 0, ii = 0;
+        if (e < total_raw)
+        {
+            lrow = last_le(t.row_eoff, nrows, e);
+            ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
+            const int k = a.Li[ii] + t.row_b[lrow] * a.n_L;
+            s = a.Ap[k];
+            len = a.Ap[k + 1] - s;
+        }
+        const int inc_t = block_incl_scan_int(len, t.scr);
+        t.e_incl[tid] = inc_t;
+        t.e_s[tid] = s;
+        t.e_len[tid] = len;
+        t.e_row[tid] = lrow;
+        t.e_ii[tid] = ii;
+        __syncthreads();
+        const int total = t.e_incl[TILE_THREADS - 1];
+        const int nent = min(TILE_THREADS, total_raw - ec);
+        for (int base = 0; base < total; base += TILE_THREADS)
+        {
+            const int u = base + tid;
+            bool valid = u < total;
+            int el = 0, jj = 0, o = 0;
+            unsigned eg = 0;
+            if (valid)
+            {
+                el = cta_entry_of(t.e_incl, nent, u);
+                jj = t.e_s[el] + u - (t.e_incl[el] - t.e_len[el]);
+                const int j = a.Ai[jj];
+                const int lr = t.e_row[el];
+                const int w = t.row_nr[lr];
+                const int *crow = a.Ci + t.row_cs[lr];
+                const int pos = lower_bound_dev(crow, w, j);
+                if (pos >= w || crow[pos] != j)
+                {
+                    atomicOr(a.err, 1);
+                    valid = false;
+                }
+                o = t.row_outoff[lr] + pos;
+                eg = (unsigned)t.row_b[lr] * (unsigned)a.L_nnz + (unsigned)t.e_ii[el];
+            }
+            f(valid, eg, jj, o);
+        }
+        __syncthreads();
+    }
+}
+
+// Compiles the output-major refill schedule of one tile (one CTA per tile, once
+// per pattern). Every output of the tile window gets one 8-byte word:
+//   {jj, e}                       its only term is V[e] * A.x[jj];
+//   {start, MULTI_BIT | count}    it collects count >= 2 terms, the {jj, e} pairs
+//                                 X[start .. start + count - 1] in upstream's
+//                                 visiting order.
+// COUNT pass: the numbers of output words and list pairs of every tile. BUILD pass:
+// writes the descriptor, the words and the lists at the offsets the scans gave.
+template <bool BUILD>
+__global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
     NumArgs a, const unsigned char *__restrict__ rcls, const int *__restrict__ tile_start,
-    const long long *__restrict__ epref, const long long *__restrict__ plan_begin,
-    TileDesc *__restrict__ tiles, TileEntry *__restrict__ entries, unsigned short *__restrict__ plan)
+    long long *__restrict__ tile_nwords, long long *__restrict__ tile_nx,
+    const long long *__restrict__ word_begin, const long long *__restrict__ x_begin,
+    TileDesc *__restrict__ tiles, uint2 *__restrict__ W, uint2 *__restrict__ X)
 {
     extern __shared__ __align__(16) int bsm[];
     BuildSmem t;
     t.cnt = bsm;
-    t.row_cs = t.cnt + TILE_ACC;
-    t.row_ls = t.row_cs + TILE_THREADS;
+    t.cur = t.cnt + TILE_ACC;
+    t.row_cs = t.cur + TILE_ACC;
+    t.row_nr = t.row_cs + TILE_THREADS;
+    t.row_ls = t.row_nr + TILE_THREADS;
     t.row_b = t.row_ls + TILE_THREADS;
-    t.row_accoff = t.row_b + TILE_THREADS;
-    t.row_eoff = t.row_accoff + TILE_THREADS + 1;
+    t.row_outoff = t.row_b + TILE_THREADS;
+    t.row_eoff = t.row_outoff + TILE_THREADS + 1;
     t.e_incl = t.row_eoff + TILE_THREADS + 1;
     t.e_s = t.e_incl + TILE_THREADS;
     t.e_len = t.e_s + TILE_THREADS;
     t.e_row = t.e_len + TILE_THREADS;
-    t.scr = t.e_row + TILE_THREADS;
+    t.e_ii = t.e_row + TILE_THREADS;
+    t.scr = t.e_ii + TILE_THREADS;
+    t.misc = t.scr + 32;
     const int tid = threadIdx.x;
     const int tile = blockIdx.x;
     const int r0 = tile_start[tile], nrows = tile_start[tile + 1] - r0;
     for (int q = tid; q < TILE_ACC; q += TILE_THREADS) t.cnt[q] = 0;
-    // rows
     int nr = 0, ne = 0;
     if (tid < nrows)
     {
-        int r = r0 + tid;
-        int b = r / a.L_m, rr = r - b * a.L_m;
-        int cs = a.Cp[r], ls = a.Lp[rr];
+        const int r = r0 + tid;
+        const int b = r / a.L_m, rr = r - b * a.L_m;
+        const int cs = a.Cp[r], ls = a.Lp[rr];
         if (rcls[r] == NUM_TILE)
         {
             nr = a.Cp[r + 1] - cs;
             ne = a.Lp[rr + 1] - ls;
         }
         t.row_cs[tid] = cs;
+        t.row_nr[tid] = nr;
         t.row_ls[tid] = ls;
         t.row_b[tid] = b;
     }
-    int inr = block_incl_scan_int(nr, t.scr);
-    int ine = block_incl_scan_int(ne, t.scr);
+    const int inr = block_incl_scan_int(nr, t.scr);
+    const int ine = block_incl_scan_int(ne, t.scr);
     if (tid < nrows)
     {
-        t.row_accoff[tid] = inr - nr;
+        t.row_outoff[tid] = inr - nr;
         t.row_eoff[tid] = ine - ne;
     }
     if (tid == TILE_THREADS - 1)
     {
-        t.row_accoff[nrows] = inr;
+        t.row_outoff[nrows] = inr;
         t.row_eoff[nrows] = ine;
     }
     __syncthreads();
-    const int total_out = t.row_accoff[nrows], total_ent = t.row_eoff[nrows];
-    const long long eb = epref[r0], pb = plan_begin[tile];
-    long long cursor = 0;
-    for (int ec = 0; ec < total_ent; ec += TILE_THREADS)
+    const int total_out = t.row_outoff[nrows], total_raw = t.row_eoff[nrows];
+    if (total_out > TILE_ACC)
     {
-        int e = ec + tid, s = 0, len = 0, lrow = 0;
-        if (e < total_ent)
+        if (tid == 0) atomicOr(a.err, 2);
+        return; // cannot happen with the tile weights; the host reports it
+    }
+    const long long wb = BUILD ? word_begin[tile] : 0, xb = BUILD ? x_begin[tile] : 0;
+
+    // pass A: terms per output; the word of every output with one term
+    tile_terms(a, t, nrows, total_raw, [&](bool valid, unsigned e, int jj, int o) {
+        if (!valid) return;
+        atomicAdd(&t.cnt[o], 1);
+        if (BUILD) W[wb + o] = make_uint2((unsigned)jj, e);
+    });
+    __syncthreads();
+    // multi-term outputs: their word and list offset
+    int nexc = 0, nxt = 0;
+    for (int oc = 0; oc < total_out; oc += TILE_THREADS)
+    {
+        const int o = oc + tid;
+        const int c = o < total_out ? t.cnt[o] : 0;
+        if (o < total_out && c == 0) atomicOr(a.err, 1); // every output has a term
+        const int m = c >= 2 ? 1 : 0;
+        const int im = block_incl_scan_int(m, t.scr);
+        const int it = block_incl_scan_int(m ? c : 0, t.scr);
+        if (o < total_out)
         {
-            lrow = last_le(t.row_eoff, nrows, e);
-            int ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
-            int k = a.Li[ii] + t.row_b[lrow] * a.n_L;
-            s = a.Ap[k];
-            len = a.Ap[k + 1] - s;
+            t.cur[o] = m ? nxt + it - c : -1;
+            if (BUILD && m) W[wb + o] = make_uint2((unsigned)(xb + nxt + it - c), MULTI_BIT | (unsigned)c);
         }
-        int incl = block_incl_scan_int(len, t.scr);
-        if (e < total_ent)
+        if (tid == TILE_THREADS - 1)
         {
-            TileEntry rec;
-            rec.k = a.Li[t.row_ls[lrow] + (e - t.row_eoff[lrow])] + t.row_b[lrow] * a.n_L;
-            int ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
-            rec.lx = a.L_map ? a.L_map[ii] : ii;
-            rec.s = s;
-            rec.toff = (unsigned short)(cursor + incl - len);
-            rec.accbase = (unsigned short)t.row_accoff[lrow];
-            entries[eb + e] = rec;
+            t.misc[1] = im;
+            t.misc[2] = it;
         }
-        t.e_incl[tid] = incl;
-        t.e_s[tid] = s;
-        t.e_len[tid] = len;
-        t.e_row[tid] = lrow;
         __syncthreads();
-        int total = t.e_incl[TILE_THREADS - 1];
-        int nent = min(TILE_THREADS, total_ent - ec);
-        for (int u = tid; u < total; u += TILE_THREADS)
-        {
-            int el = cta_entry_of(t.e_incl, nent, u);
-            int jj = t.e_s[el] + u - (t.e_incl[el] - t.e_len[el]);
-            int j = a.Ai[jj];
-            int lr = t.e_row[el];
-            int w = t.row_accoff[lr + 1] - t.row_accoff[lr];
-            const int *crow = a.Ci + t.row_cs[lr];
-            int pos = lower_bound_dev(crow, w, j);
-            if (pos >= w || crow[pos] != j)
-            {
-                atomicOr(a.err, 1);
-                pos = 0xffff; // rejected by the refill's range check
-            }
-            else
-                atomicAdd(&t.cnt[t.row_accoff[lr] + pos], 1);
-            plan[pb + cursor + u] = (unsigned short)pos;
-        }
-        cursor += total;
+        nexc += t.misc[1];
+        nxt += t.misc[2];
         __syncthreads();
     }
-    bool many = false;
-    for (int q = tid; q < total_out; q += TILE_THREADS) many |= t.cnt[q] >= 3;
-    many = __syncthreads_or(many);
-    if (!many)
+    if (!BUILD)
     {
-        // tag the terms of two-term outputs (bit 15): they accumulate with an atomic
-        // add, every other term is the sole term of its output and is stored
-        for (int e = tid; e < total_ent; e += TILE_THREADS)
+        if (tid == 0)
         {
-            const TileEntry rec = entries[eb + e];
-            int end = e + 1 < total_ent ? entries[eb + e + 1].toff : (int)cursor;
-            for (int q = rec.toff; q < end; ++q)
-            {
-                unsigned short pv = plan[pb + q];
-                if (pv != 0xffff && t.cnt[rec.accbase + pv] == 2) plan[pb + q] = pv | 0x8000;
-            }
+            tile_nwords[tile] = total_out;
+            tile_nx[tile] = nxt;
         }
+        return;
+    }
+    if (nexc)
+    {
+        // pass B: the terms of multi-term outputs into their lists in visiting order;
+        // warps take turns, and inside a warp equal outputs are ranked by lane
+        uint2 *xt = X + xb;
+        const int warp = tid >> 5, lane = lane_id();
+        tile_terms(a, t, nrows, total_raw, [&](bool valid, unsigned e, int jj, int o) {
+            const bool multi = valid && t.cur[o] >= 0;
+            for (int w = 0; w < TILE_THREADS / 32; ++w)
+            {
+                if (warp == w)
+                {
+                    const int key = multi ? o : -(lane + 1);
+                    const unsigned grp = __match_any_sync(FULL_MASK, key);
+                    int slot = 0;
+                    if (multi) slot = t.cur[o] + __popc(grp & lanemask_lt());
+                    __syncwarp();
+                    if (multi)
+                    {
+                        xt[slot] = make_uint2((unsigned)jj, e);
+                        if (lane == 31 - __clz(grp)) t.cur[o] += __popc(grp);
+                    }
+                }
+                __syncthreads();
+            }
+        });
     }
     if (tid == 0)
     {
         TileDesc dsc;
-        dsc.ent_begin = eb;
-        dsc.plan_begin = pb;
-        dsc.nent = total_ent;
+        dsc.word_begin = (int)wb;
         dsc.out_begin = t.row_cs[0];
         dsc.nout = total_out;
         dsc.prod = 0;
-        dsc.ordered = many ? 1 : 0;
-        dsc.nterms = (int)cursor;
-        dsc.pad[0] = dsc.pad[1] = 0;
         tiles[tile] = dsc;
     }
 }
 
-#ifndef SDL_GROUP
-#define SDL_GROUP 4
-#endif
-#ifndef SDL_UNROLL
-#define SDL_UNROLL 2
-#endif
-#ifndef SDL_QPL
-#define SDL_QPL 2
-#endif
-#ifndef SDL_REFILL_MINB
-#define SDL_REFILL_MINB 4
-#endif
-constexpr int GROUP = SDL_GROUP; // lanes per L entry
-constexpr int NGROUP = TILE_THREADS / GROUP;
-constexpr int UNROLL = SDL_UNROLL; // entries per group whose loads are in flight together
-constexpr int QPL = SDL_QPL;       // terms per lane issued with the batch (GROUP * QPL per entry)
-constexpr int REC_BUF = 256;       // entry records staged per tile (more: read from global)
-
-struct RefillSmem
+// Entry values of one refill: V[e] = L.x * d[k] for every entry e = b * L_nnz + ii
+// of kron(I_blocks, L) (upstream's order of the two factors; L.x alone without d,
+// 1.0 for a unit L). Each thread takes EV_ILP entries, spaced one grid apart, and
+// issues all their loads before the first store.
+constexpr int EV_ILP = 4;
+__device__ __forceinline__ void entry_values_run(const ProdSched &S, const ProdPtrs &P, long long first,
+                                                 long long end, long long step)
 {
-    double *acc;                // TILE_ACC
-    double *e_v;                // TILE_THREADS (ordered path)
-    TileEntry *rec;             // 2 x REC_BUF
-    unsigned short *pln;        // 2 x TILE_ACC
-    TileDesc *desc;             // 3 (tile k uses desc[k % 3])
-    int *claim;                 // TILE_CLAIM
-    int *e_incl, *e_s, *e_len, *e_acc, *scr;
-};
-
-__host__ __device__ constexpr size_t refill_smem_bytes()
-{
-    return (size_t)TILE_ACC * 8 + TILE_THREADS * 8 + 2 * REC_BUF * sizeof(TileEntry) +
-           2 * (size_t)TILE_ACC * 2 + 3 * sizeof(TileDesc) +
-           ((size_t)TILE_CLAIM + 4 * TILE_THREADS + 32) * 4;
-}
-
-__device__ __forceinline__ RefillSmem refill_smem(unsigned char *raw)
-{
-    RefillSmem t;
-    t.acc = (double *)raw;
-    t.e_v = t.acc + TILE_ACC;
-    t.rec = (TileEntry *)(t.e_v + TILE_THREADS);
-    t.pln = (unsigned short *)(t.rec + 2 * REC_BUF);
-    t.desc = (TileDesc *)(t.pln + 2 * TILE_ACC);
-    t.claim = (int *)(t.desc + 3);
-    t.e_incl = t.claim + TILE_CLAIM;
-    t.e_s = t.e_incl + TILE_THREADS;
-    t.e_len = t.e_s + TILE_THREADS;
-    t.e_acc = t.e_len + TILE_THREADS;
-    t.scr = t.e_acc + TILE_THREADS;
-    return t;
-}
-
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src)
-{
-    unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// Stage a tile's entry records (when they fit) and plan into shared buffer b.
-__device__ __forceinline__ void stage_tile(const RefillSmem &t, int b, const TileDesc &D,
-                                           const TileEntry *__restrict__ entries,
-                                           const unsigned short *__restrict__ plan)
-{
-    if (D.nent <= REC_BUF)
-        for (int e = threadIdx.x; e < D.nent; e += TILE_THREADS)
-            cp_async16(t.rec + b * REC_BUF + e, entries + D.ent_begin + e);
-    const int n16 = (D.nterms + 7) >> 3;
-    for (int c = threadIdx.x; c < n16; c += TILE_THREADS)
-        cp_async16(t.pln + b * TILE_ACC + 8 * c, plan + D.plan_begin + 8 * c);
-}
-
-__device__ __forceinline__ void stage_desc(const RefillSmem &t, int b, const TileDesc *__restrict__ tiles,
-                                           int tile)
-{
-    if (threadIdx.x < (int)(sizeof(TileDesc) / 16))
-        cp_async16((char *)(t.desc + b) + 16 * threadIdx.x, (const char *)(tiles + tile) + 16 * threadIdx.x);
-}
-
-__device__ __forceinline__ void put_term(double *acc, int nout, int ab, unsigned pe, double prod, int *err)
-{
-    const int idx = ab + (int)(pe & 0x7fffu);
-    if (idx >= nout)
-        atomicOr(err, 1);
-    else if (pe & 0x8000u)
-        atomicAdd(&acc[idx], prod);
-    else
-        acc[idx] = __dadd_rn(0.0, prod);
-}
-
-// Refill of the tile rows from the compiled schedule: a persistent CTA walks its
-// tiles while cp.async stages the next tile's descriptor, entry records and plan
-// in shared memory, so only the value reads of the current tile are exposed.
-// Each group of GROUP lanes takes UNROLL entries at once and issues every value
-// they need (L's and d's per entry, A's row per term) together. Terms land in a
-// shared window over the tile's outputs, written back to one contiguous range of
-// C.x.
-//   unordered tiles: the sole term of an output is stored (0.0 + prod, as upstream
-//     starts from +0.0); the two terms of a two-term output are atomically added
-//     (their order cannot change the result);
-//   ordered tiles: each 256-term window goes through a hashed claim table,
-//     smallest term index first, which is upstream's order.
-__global__ void __launch_bounds__(TILE_THREADS, SDL_REFILL_MINB) k_tile_refill(
-    const TileDesc *__restrict__ tiles, int ntiles, const TileEntry *__restrict__ entries,
-    const unsigned short *__restrict__ plan, const ProdPtrs *__restrict__ ptrs, ProdPtrs single,
-    int *__restrict__ err)
-{
-    extern __shared__ __align__(16) unsigned char rraw[];
-    RefillSmem t = refill_smem(rraw);
-    __shared__ int chunk_total;
-    const int tid = threadIdx.x;
-    const int stride = gridDim.x;
-    int tile = blockIdx.x;
-    if (tile >= ntiles) return;
-    for (int q = tid; q < TILE_ACC; q += TILE_THREADS) t.acc[q] = 0.0;
-    // prologue: descriptor of the first tile, its records / plan, the next descriptor
-    stage_desc(t, 0, tiles, tile);
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
-    stage_tile(t, 0, t.desc[0], entries, plan);
-    if (tile + stride < ntiles) stage_desc(t, 1, tiles, tile + stride);
-    cp_async_commit();
-    for (int k = 0; tile < ntiles; ++k, tile += stride)
+    for (long long base = first; base < end; base += step * EV_ILP)
     {
-        const int b = k & 1, nb = b ^ 1;
-        const TileDesc &D = t.desc[k % 3];
-        cp_async_wait_all();
-        __syncthreads();
-        if (tile + stride < ntiles)
+        int ii[EV_ILP], k[EV_ILP];
+#pragma unroll
+        for (int j = 0; j < EV_ILP; ++j)
         {
-            stage_tile(t, nb, t.desc[(k + 1) % 3], entries, plan);
-            if (tile + 2 * stride < ntiles) stage_desc(t, (k + 2) % 3, tiles, tile + 2 * stride);
-        }
-        cp_async_commit();
-
-        const ProdPtrs P = ptrs ? ptrs[D.prod] : single;
-        const TileEntry *E = D.nent <= REC_BUF ? t.rec + b * REC_BUF : entries + D.ent_begin;
-        const unsigned short *PL = t.pln + b * TILE_ACC;
-        if (D.ordered)
-            for (int q = tid; q < TILE_CLAIM; q += TILE_THREADS) t.claim[q] = INT_MAX;
-        if (!D.ordered)
-        {
-            const int g = tid / GROUP, gl = tid % GROUP;
-            for (int e0 = g; e0 < D.nent; e0 += NGROUP * UNROLL)
+            const long long i = base + j * step;
+            ii[j] = -1;
+            k[j] = 0;
+            if (i < end)
             {
-                TileEntry rec[UNROLL];
-                int len[UNROLL];
-#pragma unroll
-                for (int j = 0; j < UNROLL; ++j)
-                {
-                    const int e = e0 + j * NGROUP;
-                    len[j] = 0;
-                    if (e < D.nent)
-                    {
-                        rec[j] = E[e];
-                        const int end = e + 1 < D.nent ? (int)E[e + 1].toff : D.nterms;
-                        len[j] = end - rec[j].toff;
-                    }
-                }
-                double lx[UNROLL], dk[UNROLL], xv[UNROLL][QPL];
-                unsigned pe[UNROLL][QPL];
-#pragma unroll
-                for (int j = 0; j < UNROLL; ++j)
-                {
-                    if (len[j] > 0)
-                    {
-                        lx[j] = P.Lx ? P.Lx[rec[j].lx] : 1.0;
-                        dk[j] = P.d ? P.d[rec[j].k] : 1.0;
-                    }
-#pragma unroll
-                    for (int qq = 0; qq < QPL; ++qq)
-                    {
-                        const int q = gl + qq * GROUP;
-                        if (q < len[j])
-                        {
-                            pe[j][qq] = PL[rec[j].toff + q];
-                            xv[j][qq] = P.Ax[rec[j].s + q];
-                        }
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < UNROLL; ++j)
-                {
-                    if (len[j] <= 0) continue;
-                    const double v = P.d ? __dmul_rn(lx[j], dk[j]) : lx[j];
-#pragma unroll
-                    for (int qq = 0; qq < QPL; ++qq)
-                    {
-                        const int q = gl + qq * GROUP;
-                        if (q < len[j])
-                            put_term(t.acc, D.nout, rec[j].accbase, pe[j][qq], __dmul_rn(v, xv[j][qq]), err);
-                    }
-                    for (int q = gl + QPL * GROUP; q < len[j]; q += GROUP)
-                        put_term(t.acc, D.nout, rec[j].accbase, PL[rec[j].toff + q],
-                                 __dmul_rn(v, P.Ax[rec[j].s + q]), err);
-                }
+                const int b = S.blocks > 1 ? (int)(i / S.L_nnz) : 0;
+                ii[j] = (int)(i - (long long)b * S.L_nnz);
+                if (P.d) k[j] = S.Li[ii[j]] + b * S.n_L;
+                if (P.Lx && S.L_map) ii[j] = S.L_map[ii[j]]; // index of the L value
             }
         }
-        else
+        double lx[EV_ILP], dk[EV_ILP];
+#pragma unroll
+        for (int j = 0; j < EV_ILP; ++j)
         {
-            long long cursor = 0;
-            for (int ec = 0; ec < D.nent; ec += TILE_THREADS)
+            lx[j] = 1.0;
+            dk[j] = 1.0;
+            if (ii[j] >= 0)
             {
-                int e = ec + tid;
-                int len = 0, s = 0, accb = 0;
-                double v = 0.0;
-                if (e < D.nent)
-                {
-                    const TileEntry rec = E[e];
-                    const int end = e + 1 < D.nent ? (int)E[e + 1].toff : D.nterms;
-                    len = end - rec.toff;
-                    s = rec.s;
-                    accb = rec.accbase;
-                    double lxv = P.Lx ? P.Lx[rec.lx] : 1.0;
-                    v = P.d ? __dmul_rn(lxv, P.d[rec.k]) : lxv;
-                }
-                int incl = block_incl_scan_int(len, t.scr);
-                t.e_incl[tid] = incl;
-                t.e_s[tid] = s;
-                t.e_len[tid] = len;
-                t.e_acc[tid] = accb;
-                t.e_v[tid] = v;
-                if (tid == TILE_THREADS - 1) chunk_total = incl;
-                __syncthreads();
-                const int total = chunk_total;
-                const int nent = min(TILE_THREADS, D.nent - ec);
-                for (int base = 0; base < total; base += TILE_THREADS)
-                {
-                    int u = base + tid;
-                    bool pending = u < total;
-                    int idx = 0;
-                    double prod = 0.0;
-                    if (pending)
-                    {
-                        int el = cta_entry_of(t.e_incl, nent, u);
-                        int q = u - (t.e_incl[el] - t.e_len[el]);
-                        idx = t.e_acc[el] + PL[cursor + u];
-                        prod = __dmul_rn(t.e_v[el], P.Ax[t.e_s[el] + q]);
-                        if (idx >= D.nout)
-                        {
-                            atomicOr(err, 1);
-                            pending = false;
-                        }
-                    }
-                    const int slot = idx & (TILE_CLAIM - 1);
-                    while (true)
-                    {
-                        if (pending) atomicMin(&t.claim[slot], u);
-                        __syncthreads();
-                        bool won = pending && t.claim[slot] == u;
-                        if (won) t.acc[idx] = __dadd_rn(t.acc[idx], prod);
-                        __syncthreads();
-                        if (won)
-                        {
-                            t.claim[slot] = INT_MAX;
-                            pending = false;
-                        }
-                        if (!__syncthreads_or(pending)) break;
-                    }
-                }
-                cursor += total;
-                __syncthreads();
+                if (P.Lx) lx[j] = P.Lx[ii[j]];
+                if (P.d) dk[j] = P.d[k[j]];
             }
         }
-        __syncthreads();
-        double *dst = P.Cx + D.out_begin;
-        for (int q = tid; q < D.nout; q += TILE_THREADS)
+#pragma unroll
+        for (int j = 0; j < EV_ILP; ++j)
         {
-            dst[q] = t.acc[q];
-            t.acc[q] = 0.0;
+            const long long i = base + j * step;
+            if (i < end) S.V[i] = P.d ? __dmul_rn(lx[j], dk[j]) : lx[j];
         }
     }
-    cp_async_wait_all();
+}
+
+__global__ void __launch_bounds__(256) k_entry_values(ProdSched S, ProdPtrs P)
+{
+    const long long step = (long long)gridDim.x * blockDim.x;
+    entry_values_run(S, P, blockIdx.x * (long long)blockDim.x + threadIdx.x, S.nV, step);
+}
+
+// Batched: one CTA per chunk of one product's entries.
+__global__ void __launch_bounds__(256) k_entry_values_batched(const EntChunk *__restrict__ chunks,
+                                                              const ProdPtrs *__restrict__ ptrs,
+                                                              const ProdSched *__restrict__ scheds)
+{
+    const EntChunk c = chunks[blockIdx.x];
+    const ProdSched S = scheds[c.prod];
+    const ProdPtrs P = ptrs[c.prod];
+    entry_values_run(S, P, c.begin + threadIdx.x, c.begin + c.count, blockDim.x);
+}
+
+#ifndef SDL_REFILL_MINB
+#define SDL_REFILL_MINB 6
+#endif
+#ifndef SDL_REFILL_UNROLL
+#define SDL_REFILL_UNROLL 4
+#endif
+constexpr int REFILL_THREADS = 256;
+constexpr int RUNROLL = SDL_REFILL_UNROLL; // outputs per thread whose loads are in flight together
+
+// Sum of an output's term list from +0.0 in list (upstream's visiting) order; the
+// loads of four terms are in flight together.
+__device__ __forceinline__ double multi_sum(const uint2 *__restrict__ X, long long nX,
+                                         const double *__restrict__ Ax, const double *__restrict__ V, uint2 w,
+                                         unsigned nA, unsigned nV, int *err)
+{
+    const unsigned cnt = w.y & ~MULTI_BIT;
+    const unsigned long long start = w.x;
+    if (start + cnt > (unsigned long long)nX)
+    {
+        atomicOr(err, 1);
+        return 0.0;
+    }
+    const uint2 *L = X + start;
+    double acc = 0.0;
+    for (unsigned i = 0; i < cnt; i += 4)
+    {
+        double xx[4], vv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            xx[j] = 0.0;
+            vv[j] = 0.0;
+            if (i + j < cnt)
+            {
+                const uint2 p = L[i + j];
+                if (p.x < nA && p.y < nV)
+                {
+                    xx[j] = Ax[p.x];
+                    vv[j] = V[p.y];
+                }
+                else
+                    atomicOr(err, 1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (i + j < cnt) acc = __dadd_rn(acc, __dmul_rn(vv[j], xx[j]));
+    }
+    return acc;
+}
+
+// Refill of the tile rows from the output-major schedule. Persistent CTAs walk
+// their tiles (blockIdx.x, + gridDim.x, ...); every thread works on its own
+// outputs, with no shared memory and no barrier: per output a word, then the two
+// gathers V[e] and A.x[jj], then one coalesced store. While the gathers of tile k
+// are in flight, the words of tile k+1 (whose descriptor came one tile earlier) are
+// already being loaded, so a tile exposes about one memory round trip.
+// An output with one term is 0.0 + V[e] * A.x[jj] (upstream's accumulator starts
+// at +0.0); an output with several terms sums its list from +0.0 in upstream's
+// visiting order. Nothing is accumulated with atomics: every output is
+// bit-identical to upstream's.
+// Base pointers of the product a tile belongs to: kernel parameters for a single
+// product, the batch's tables otherwise (re-read where needed: they stay in L1).
+struct ProdBase
+{
+    const uint2 *W, *X;
+    const double *Ax, *V;
+    double *C;
+    long long nX;
+    unsigned nA, nV;
+};
+template <bool BATCHED>
+__device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restrict__ ptrs,
+                                              const ProdSched *__restrict__ scheds, const ProdPtrs &P1,
+                                              const ProdSched &S1)
+{
+    ProdBase r;
+    if (BATCHED)
+    {
+        r.Ax = ptrs[prod].Ax;
+        r.C = ptrs[prod].Cx;
+        r.W = scheds[prod].W;
+        r.X = scheds[prod].X;
+        r.V = scheds[prod].V;
+        r.nX = scheds[prod].nX;
+        r.nA = (unsigned)scheds[prod].nA;
+        r.nV = (unsigned)scheds[prod].nV;
+    }
+    else
+    {
+        r.Ax = P1.Ax;
+        r.C = P1.Cx;
+        r.W = S1.W;
+        r.X = S1.X;
+        r.V = S1.V;
+        r.nX = S1.nX;
+        r.nA = (unsigned)S1.nA;
+        r.nV = (unsigned)S1.nV;
+    }
+    return r;
+}
+
+// (word_begin, out_begin, nout, prod) of tile t
+__device__ __forceinline__ int4 tile_desc(const TileDesc *__restrict__ tiles, int t)
+{
+    return *reinterpret_cast<const int4 *>(tiles + t);
+}
+
+__device__ __forceinline__ void load_words(const uint2 *__restrict__ W, int nout, int base, uint2 (&w)[RUNROLL])
+{
+#pragma unroll
+    for (int u = 0; u < RUNROLL; ++u)
+    {
+        const int o = base + threadIdx.x + u * REFILL_THREADS;
+        w[u] = o < nout ? W[o] : make_uint2(0u, MULTI_BIT);
+    }
+}
+
+// Refill of the tile rows from the output-major schedule. Persistent CTAs walk
+// their tiles (blockIdx.x, + gridDim.x, ...); every thread works on its own
+// outputs, with no shared memory and no barrier: per output a word, then the two
+// gathers V[e] and A.x[jj], then one coalesced store. The words of the next step
+// (the next RUNROLL * REFILL_THREADS outputs of the tile, or the first ones of the
+// next tile, whose descriptor was read two tiles ahead) are loaded while the
+// current step's gathers are in flight, so a step exposes about one round trip.
+// An output with one term is 0.0 + V[e] * A.x[jj] (upstream's accumulator starts
+// at +0.0); an output with several terms sums its list from +0.0 in upstream's
+// visiting order. Nothing is accumulated with atomics: every output is
+// bit-identical to upstream's.
+template <bool BATCHED>
+__global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill(
+    const TileDesc *__restrict__ tiles, int ntiles, const ProdPtrs *__restrict__ ptrs,
+    const ProdSched *__restrict__ scheds, ProdPtrs P1, ProdSched S1, int *__restrict__ err)
+{
+    constexpr int CH = RUNROLL * REFILL_THREADS; // outputs of a tile per step
+    const int G = gridDim.x;
+    int t = blockIdx.x;
+    if (t >= ntiles) return;
+    int4 dc = tile_desc(tiles, t); // (word_begin, out_begin, nout, prod)
+    int4 d1 = t + G < ntiles ? tile_desc(tiles, t + G) : make_int4(0, 0, 0, 0);
+    uint2 w[RUNROLL];
+    load_words(prod_base<BATCHED>(dc.w, ptrs, scheds, P1, S1).W + dc.x, dc.z, 0, w);
+    while (true)
+    {
+        const bool has1 = t + G < ntiles;
+        const int4 d2 = t + 2 * G < ntiles ? tile_desc(tiles, t + 2 * G) : make_int4(0, 0, 0, 0);
+        for (int base = 0;; base += CH)
+        {
+            const bool last = base + CH >= dc.z;
+            // gathers of this step
+            double x[RUNROLL], v[RUNROLL];
+            unsigned one = 0, multi = 0;
+            {
+                const ProdBase pb = prod_base<BATCHED>(dc.w, ptrs, scheds, P1, S1);
+#pragma unroll
+                for (int u = 0; u < RUNROLL; ++u)
+                {
+                    const int o = base + threadIdx.x + u * REFILL_THREADS;
+                    // a multi-term word has y >= MULTI_BIT > nV
+                    const bool ok = w[u].x < pb.nA && w[u].y < pb.nV;
+                    x[u] = ok ? pb.Ax[w[u].x] : 0.0;
+                    v[u] = ok ? pb.V[w[u].y] : 0.0;
+                    if (o < dc.z)
+                    {
+                        if (ok)
+                            one |= 1u << u;
+                        else if (w[u].y & MULTI_BIT)
+                            multi |= 1u << u;
+                        else
+                            atomicOr(err, 1);
+                    }
+                }
+            }
+            // words of the next step
+            const int4 dn = last ? d1 : dc;
+            const int nb = last ? 0 : base + CH;
+            if (!last || has1)
+                load_words(prod_base<BATCHED>(dn.w, ptrs, scheds, P1, S1).W + dn.x, dn.z, nb, w);
+            // results of this step
+            {
+                const ProdBase pb = prod_base<BATCHED>(dc.w, ptrs, scheds, P1, S1);
+                double *C = pb.C + dc.y;
+#pragma unroll
+                for (int u = 0; u < RUNROLL; ++u)
+                    if (one >> u & 1u)
+                        C[base + threadIdx.x + u * REFILL_THREADS] = __dadd_rn(0.0, __dmul_rn(v[u], x[u]));
+                // multi-term outputs (their word is re-read, from L1)
+                const uint2 *Wt = pb.W + dc.x;
+#pragma unroll 1
+                for (; multi; multi &= multi - 1)
+                {
+                    const int o = base + threadIdx.x + (__ffs(multi) - 1) * REFILL_THREADS;
+                    C[o] = multi_sum(pb.X, pb.nX, pb.Ax, pb.V, Wt[o], pb.nA, pb.nV, err);
+                }
+            }
+            if (last) break;
+        }
+        if (!has1) break;
+        dc = d1;
+        d1 = d2;
+        t += G;
+    }
+}
+
+// Value pointers from a device binding table (batched refills replayed from a CUDA
+// graph read the pointers bound at replay time), when given.
+__device__ __forceinline__ void bind_values(NumArgs &a, const ProdPtrs *__restrict__ vals)
+{
+    if (vals)
+    {
+        a.Lx = vals->Lx;
+        a.d = vals->d;
+        a.Ax = vals->Ax;
+        a.Cx = vals->Cx;
+    }
 }
 
 // Medium rows: one CTA per row, shared accumulator indexed by output position;
 // a claim table orders same-position terms of a chunk by term index.
 template <int CAP>
-__global__ void k_num_cta(const int *__restrict__ rows, int count, NumArgs a)
+__global__ void k_num_cta(const int *__restrict__ rows, int count, NumArgs a,
+                          const ProdPtrs *__restrict__ vals)
 {
+    bind_values(a, vals);
     extern __shared__ __align__(16) unsigned char smraw[];
     double *acc = (double *)smraw;
     CtaChunk ch;
@@ -990,8 +1043,9 @@ constexpr int GMEM_CLAIM = 4096;
 // (only this row's columns are ever read, so it never needs clearing) and a hashed
 // claim table keep same-position terms in order.
 __global__ void k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
-                           int *__restrict__ posmap_all, int n)
+                           int *__restrict__ posmap_all, int n, const ProdPtrs *__restrict__ vals)
 {
+    bind_values(a, vals);
     extern __shared__ __align__(16) unsigned char smraw[];
     CtaChunk ch;
     ch.v = (double *)smraw;
@@ -1169,15 +1223,12 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
 {
     Runtime &rt = runtime();
     const int m_out = P.m_out;
-    DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1), small_ent(m_out),
-        epref((size_t)m_out + 1), small_terms(m_out), spref((size_t)m_out + 1);
+    DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1);
     DevBuf<unsigned char> rcls(m_out);
-    SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub, P.Cp.get(), d.Lp,
-               d.L_m, m_out, rcls.get(), weight.get(), small_ent.get(), small_terms.get());
+    SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub, P.Cp.get(), m_out,
+               rcls.get(), weight.get());
     bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
     exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
-    long long ent_total = exclusive_scan_i64(small_ent.get(), epref.get(), m_out, s);
-    exclusive_scan_i64(small_terms.get(), spref.get(), m_out, s);
     DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
     SDL_LAUNCH(k_tile_flags, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, wpref.get(), m_out,
                flag.get());
@@ -1186,20 +1237,29 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     SDL_LAUNCH(k_tile_starts, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, flag.get(),
                tile_of.get(), m_out, tile_start.get());
     SDL_CUDA(cudaMemcpyAsync(tile_start.get() + P.ntiles, &P.m_out, sizeof(int), cudaMemcpyHostToDevice, s));
-    DevBuf<long long> padded(std::max(1, P.ntiles)), plan_begin((size_t)P.ntiles + 1);
-    SDL_LAUNCH(k_tile_plan_sizes, grid_for(std::max(1, P.ntiles), 256, rt.num_sms * 8), 256, 0, s,
-               tile_start.get(), spref.get(), P.ntiles, padded.get());
-    long long plan_padded = exclusive_scan_i64(padded.get(), plan_begin.get(), P.ntiles, s);
-    P.tiles.reset(std::max(1, P.ntiles));
-    P.entries.reset(std::max<long long>(1, ent_total));
-    P.plan.reset(plan_padded + 16); // slack for the 16-byte staging copies
-    P.ptrs.reset(1);
+    const int nt = std::max(1, P.ntiles);
+    const long long nV = (long long)d.L_nnz * d.blocks;
+    if (nV >= (long long)MULTI_BIT || d.A_nnz < 0)
+        fail(SDL_ERR_OVERFLOW, "product: blocks * entries of L exceeds the schedule's 31-bit entry index");
+    DevBuf<long long> tile_nwords(nt), tile_nx(nt), word_begin((size_t)nt + 1), x_begin((size_t)nt + 1);
     NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, nullptr, nullptr, d.Ap, d.Ai, nullptr,
-               P.Cp.get(), P.Ci.get(), nullptr, rt.d_error};
-    set_smem(k_tile_build, build_smem_bytes());
-    SDL_LAUNCH(k_tile_build, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
-               tile_start.get(), epref.get(), plan_begin.get(), P.tiles.get(), P.entries.get(),
-               P.plan.get());
+               P.Cp.get(), P.Ci.get(), nullptr, rt.d_error, d.L_nnz};
+    set_smem(k_tile_schedule<false>, build_smem_bytes());
+    set_smem(k_tile_schedule<true>, build_smem_bytes());
+    SDL_LAUNCH(k_tile_schedule<false>, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
+               tile_start.get(), tile_nwords.get(), tile_nx.get(), nullptr, nullptr, nullptr, nullptr,
+               nullptr);
+    const long long word_total = exclusive_scan_i64(tile_nwords.get(), word_begin.get(), P.ntiles, s);
+    const long long x_total = exclusive_scan_i64(tile_nx.get(), x_begin.get(), P.ntiles, s);
+    if (x_total >= (long long)UINT32_MAX) fail(SDL_ERR_OVERFLOW, "product: term lists exceed 32-bit offsets");
+    if (word_total > INT_MAX) fail(SDL_ERR_OVERFLOW, "product: output words exceed 31-bit offsets");
+    P.tiles.reset(nt);
+    P.W.reset(std::max<long long>(1, word_total));
+    P.X.reset(std::max<long long>(1, x_total));
+    P.V.reset(std::max<long long>(1, nV));
+    SDL_LAUNCH(k_tile_schedule<true>, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
+               tile_start.get(), nullptr, nullptr, word_begin.get(), x_begin.get(), P.tiles.get(),
+               P.W.get(), P.X.get());
     if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
     if (P.num_count[NUM_GMEM])
     {
@@ -1432,54 +1492,90 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
 }
 
 namespace {
-int g_refill_per_sm = 0;
-
-__global__ void k_rebase_tiles(const TileDesc *__restrict__ src, int n, long long ent_shift,
-                               long long plan_shift, int prod, TileDesc *__restrict__ dst)
+__global__ void k_rebase_tiles(const TileDesc *__restrict__ src, int n, int prod, TileDesc *__restrict__ dst)
 {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
     {
         TileDesc d = src[t];
-        d.ent_begin += ent_shift;
-        d.plan_begin += plan_shift;
         d.prod = prod;
         dst[t] = d;
     }
 }
 } // namespace
 
-void tile_refill_prepare()
+ProdSched sched_of(const Product &P)
 {
-    if (g_refill_per_sm) return;
-    set_smem(k_tile_refill, refill_smem_bytes());
-    int per_sm = 0;
-    SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_refill, TILE_THREADS,
-                                                           refill_smem_bytes()));
-    g_refill_per_sm = std::max(1, per_sm);
+    const ProductDesc &d = P.desc;
+    ProdSched S{};
+    S.W = P.W.get();
+    S.X = P.X.get();
+    S.V = P.V.get();
+    S.Li = d.Li;
+    S.L_map = d.L_map;
+    S.nV = (long long)d.L_nnz * d.blocks;
+    S.nX = (long long)P.X.n;
+    S.nA = d.A_nnz;
+    S.L_nnz = d.L_nnz;
+    S.n_L = P.n_L;
+    S.blocks = d.blocks;
+    return S;
 }
 
-void rebase_tiles(const TileDesc *src, int n, long long ent_shift, long long plan_shift, int prod,
-                  TileDesc *dst, cudaStream_t s)
+void entry_values(const ProdSched &S, const ProdPtrs &vals, cudaStream_t s)
+{
+    if (S.nV <= 0) return;
+    SDL_LAUNCH(k_entry_values, grid_for(S.nV, 256 * EV_ILP, runtime().num_sms * 8), 256, 0, s, S, vals);
+}
+
+void entry_values_batched(const EntChunk *chunks, int nchunks, const ProdPtrs *ptrs, const ProdSched *scheds,
+                          cudaStream_t s)
+{
+    if (nchunks <= 0) return;
+    SDL_LAUNCH(k_entry_values_batched, nchunks, 256, 0, s, chunks, ptrs, scheds);
+}
+
+void append_entry_chunks(long long nV, int prod, int chunk, std::vector<EntChunk> &out)
+{
+    for (long long b = 0; b < nV; b += chunk)
+        out.push_back(EntChunk{b, (int)std::min<long long>(chunk, nV - b), prod});
+}
+
+void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s)
 {
     if (n <= 0) return;
-    SDL_LAUNCH(k_rebase_tiles, grid_for(n, 256, runtime().num_sms * 4), 256, 0, s, src, n, ent_shift,
-               plan_shift, prod, dst);
+    SDL_LAUNCH(k_rebase_tiles, grid_for(n, 256, runtime().num_sms * 4), 256, 0, s, src, n, prod, dst);
 }
 
-void tile_refill(const TileDesc *tiles, int ntiles, const TileEntry *entries,
-                 const unsigned short *plan, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs single)
+void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
+                 cudaStream_t s, ProdPtrs vals, ProdSched sched)
 {
     if (ntiles <= 0) return;
-    Runtime &rt = runtime();
-    tile_refill_prepare();
-    int grid = std::min(ntiles, rt.num_sms * g_refill_per_sm);
-    SDL_LAUNCH(k_tile_refill, grid, TILE_THREADS, refill_smem_bytes(), s, tiles, ntiles, entries, plan,
-               ptrs, single, rt.d_error);
+    static int per_sm[2] = {0, 0}; // resident CTAs per SM (set once, outside any capture)
+    const int b = ptrs ? 1 : 0;
+    if (!per_sm[b])
+    {
+        if (b)
+            SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[b], k_tile_refill<true>,
+                                                                   REFILL_THREADS, 0));
+        else
+            SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[b], k_tile_refill<false>,
+                                                                   REFILL_THREADS, 0));
+        per_sm[b] = std::max(1, per_sm[b]);
+    }
+    // a single product: persistent CTAs with word prefetch; a batch (many small
+    // tiles of uneven size): one CTA per tile, the hardware scheduler balances them
+    const int grid = b ? ntiles : std::min(ntiles, runtime().num_sms * per_sm[b]);
+    if (b)
+        SDL_LAUNCH(k_tile_refill<true>, grid, REFILL_THREADS, 0, s, tiles, ntiles, ptrs, scheds, vals, sched,
+                   runtime().d_error);
+    else
+        SDL_LAUNCH(k_tile_refill<false>, grid, REFILL_THREADS, 0, s, tiles, ntiles, ptrs, scheds, vals, sched,
+                   runtime().d_error);
 }
 
 void big_rows_refill(const Product &P, const double *Lx, const double *dvec, const double *Ax,
-                     double *Cx, cudaStream_t s)
+                     double *Cx, cudaStream_t s, const ProdPtrs *vals)
 {
     Runtime &rt = runtime();
     const ProductDesc &d = P.desc;
@@ -1495,7 +1591,7 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
         size_t sm = 2048 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
         set_smem(k_num_cta<2048>, sm);
         SDL_LAUNCH(k_num_cta<2048>, grid_for(cnt[NUM_C2K], 1, cap), th, sm, s, rows + off[NUM_C2K],
-                   cnt[NUM_C2K], na);
+                   cnt[NUM_C2K], na, vals);
     }
     if (cnt[NUM_C8K])
     {
@@ -1503,7 +1599,7 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
         size_t sm = 8192 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
         set_smem(k_num_cta<8192>, sm);
         SDL_LAUNCH(k_num_cta<8192>, grid_for(cnt[NUM_C8K], 1, cap), th, sm, s, rows + off[NUM_C8K],
-                   cnt[NUM_C8K], na);
+                   cnt[NUM_C8K], na, vals);
     }
     if (cnt[NUM_GMEM])
     {
@@ -1511,7 +1607,7 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
         size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
         set_smem(k_num_gmem, sm);
         SDL_LAUNCH(k_num_gmem, P.gmem_slots, th, sm, s, rows + off[NUM_GMEM], cnt[NUM_GMEM], na,
-                   P.gmem_scratch.get(), P.n);
+                   P.gmem_scratch.get(), P.n, vals);
     }
 }
 
@@ -1532,7 +1628,7 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
         size_t sm = 2048 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
         set_smem(k_num_cta<2048>, sm);
         SDL_LAUNCH(k_num_cta<2048>, grid_for(cnt[NUM_C2K], 1, cap), th, sm, s, rows + off[NUM_C2K],
-                   cnt[NUM_C2K], na);
+                   cnt[NUM_C2K], na, nullptr);
     }
     if (cnt[NUM_C8K])
     {
@@ -1540,7 +1636,7 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
         size_t sm = 8192 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
         set_smem(k_num_cta<8192>, sm);
         SDL_LAUNCH(k_num_cta<8192>, grid_for(cnt[NUM_C8K], 1, cap), th, sm, s, rows + off[NUM_C8K],
-                   cnt[NUM_C8K], na);
+                   cnt[NUM_C8K], na, nullptr);
     }
     if (cnt[NUM_GMEM])
     {
@@ -1548,7 +1644,7 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
         size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
         set_smem(k_num_gmem, sm);
         SDL_LAUNCH(k_num_gmem, std::min(slots, cnt[NUM_GMEM]), th, sm, s, rows + off[NUM_GMEM],
-                   cnt[NUM_GMEM], na, posmap, P.n);
+                   cnt[NUM_GMEM], na, posmap, P.n, nullptr);
     }
 }
 
@@ -1558,10 +1654,10 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
     if (P.nnz == 0) return;
     if (P.num_count[NUM_TILE])
     {
-        const ProductDesc &d = P.desc;
-        long long nLx = Lx ? d.L_nnz : 0; // prefetch hint only: L_map permutes L_nnz values
-        tile_refill(P.tiles.get(), P.ntiles, P.entries.get(), P.plan.get(), nullptr, s,
-                    ProdPtrs{Lx, dvec, Ax, Cx, nLx, dvec ? d.A_m : 0, d.A_nnz});
+        const ProdSched S = sched_of(P);
+        const ProdPtrs vals{Lx, dvec, Ax, Cx};
+        entry_values(S, vals, s);
+        tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S);
     }
     big_rows_refill(P, Lx, dvec, Ax, Cx, s);
 }

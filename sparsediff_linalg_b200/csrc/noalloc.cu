@@ -78,10 +78,13 @@ extern "C" sdl_status sdl_product_fill_noalloc(const sdl_product *Ph, const doub
         int *posmap = static_posmap_address();
         const int slots = (int)std::max<long long>(
             1, std::min<long long>(runtime().num_sms, STATIC_POSMAP_INTS / std::max(1, P->n)));
-        const ProductDesc &dd = P->desc;
         if (P->num_count[NUM_TILE])
-            tile_refill(P->tiles.get(), P->ntiles, P->entries.get(), P->plan.get(), nullptr, s,
-                        ProdPtrs{Lx, d, Ax, Cx, Lx ? dd.L_nnz : 0, d ? dd.A_m : 0, dd.A_nnz});
+        {
+            const ProdSched S = sched_of(*P);
+            const ProdPtrs vals{Lx, d, Ax, Cx};
+            entry_values(S, vals, s);
+            tile_refill(P->tiles.get(), P->ntiles, nullptr, nullptr, s, vals, S);
+        }
         big_rows_refill_scratch(*P, Lx, d, Ax, Cx, posmap, slots, s);
     });
 }

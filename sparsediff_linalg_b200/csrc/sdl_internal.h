@@ -14,6 +14,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "sparsediff_linalg_cuda.h"
 
@@ -179,36 +180,44 @@ enum
 constexpr int TILE_T = SDL_TILE_T;
 constexpr int TILE_THREADS = 256;
 
-// Compiled refill schedule of the tile rows (built once per pattern).
-// One record per L entry of a tile row, in upstream's visiting order.
-struct __align__(16) TileEntry
+// Compiled refill schedule of the tile rows (built once per pattern), output-major:
+// every output of a tile row has one 8-byte word,
+//   {jj, e}                      its only term is V[e] * A.x[jj];
+//   {start, MULTI_BIT | count}   it collects count >= 2 terms, the {jj, e} pairs
+//                                X[start .. start + count - 1], in upstream's
+//                                visiting order;
+// where V[e] = L.x * d[k] of entry e = b * L_nnz + ii of kron(I_blocks, L), computed
+// once per refill (entry-value kernel).
+constexpr unsigned MULTI_BIT = 0x80000000u;
+struct __align__(16) TileDesc
 {
-    int k;                   // row of A (block offset included)
-    int lx;                  // index into the L value array
-    int s;                   // A.p[k]: first entry of A's row k
-    unsigned short toff;     // offset of the entry's first term among the tile's terms
-    unsigned short accbase;  // offset of the entry's output row inside the tile window
+    int word_begin; // first output word of the tile
+    int out_begin;  // first output of the tile in C.x
+    int nout;       // outputs of the tile (one word each)
+    int prod;       // product index (batched refills), 0 for a single product
 };
-// An entry's term count is the next entry's toff minus its own (the tile's term
-// count for the last entry).
-struct TileDesc
-{
-    long long ent_begin;  // first TileEntry
-    long long plan_begin; // first plan entry (a multiple of 8: 16-byte aligned)
-    int nent;             // entries of the tile
-    int out_begin;        // first output of the tile in C.x
-    int nout;             // outputs of the tile
-    int prod;             // product index (batched refills), 0 for a single product
-    int ordered;          // 1: some output collects >= 3 terms, apply in term order
-    int nterms;           // terms of the tile
-    int pad[2];           // 48 bytes: copied to shared memory as three 16-byte chunks
-};
-// Per-product value pointers read by the refill kernels.
+// Value arrays of one refill of one product.
 struct ProdPtrs
 {
     const double *Lx, *d, *Ax;
     double *Cx;
-    long long nLx, nd, nAx; // lengths, for the L2 prefetch of the value arrays
+};
+// Refill schedule of one product as the kernels read it.
+struct ProdSched
+{
+    const uint2 *W; // output words of the tile rows
+    const uint2 *X; // term lists of multi-term outputs
+    double *V;      // entry values (refill scratch, nV)
+    const int *Li, *L_map;
+    long long nV, nX, nA; // entries of kron(I_blocks, L), list pairs, entries of A
+    int L_nnz, n_L, blocks, pad;
+};
+// A run of one product's entries (batched entry values).
+struct EntChunk
+{
+    long long begin;
+    int count;
+    int prod;
 };
 
 struct TuneConfig
@@ -248,9 +257,8 @@ struct Product
     // Compiled refill schedule of the tile rows.
     int ntiles = 0;
     DevBuf<TileDesc> tiles;
-    DevBuf<TileEntry> entries;
-    DevBuf<unsigned short> plan; // per term: its position inside its output row
-    DevBuf<ProdPtrs> ptrs;       // one slot, rewritten by each refill
+    DevBuf<uint2> W, X;   // output words, term lists
+    DevBuf<double> V;     // entry values of the current refill (L_nnz * blocks)
     DevBuf<int> gmem_scratch; // posmap scratch for NUM_GMEM rows (slots x n ints)
     int gmem_slots = 0;
     TuneConfig cfg;
@@ -279,18 +287,25 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
 // a unit L (every L value 1.0). d: A_m values or nullptr. Never allocates.
 void product_numeric(const Product &P, const double *Lx, const double *d,
                      const double *Ax, double *Cx, cudaStream_t s);
+// The schedule of a product as the refill kernels read it.
+ProdSched sched_of(const Product &P);
+// Entry values V of one product for the given values (first kernel of a refill).
+void entry_values(const ProdSched &S, const ProdPtrs &vals, cudaStream_t s);
+// Entry values of many products: chunks of their entries, pointers from the tables.
+void entry_values_batched(const EntChunk *chunks, int nchunks, const ProdPtrs *ptrs,
+                          const ProdSched *scheds, cudaStream_t s);
+// Chunks of at most `chunk` entries covering nV entries of product `prod`.
+void append_entry_chunks(long long nV, int prod, int chunk, std::vector<EntChunk> &out);
 // The tile refill over a descriptor list that may mix products (batched refills):
-// tile t reads its values through ptrs[tiles[t].prod].
-void tile_refill(const TileDesc *tiles, int ntiles, const TileEntry *entries,
-                 const unsigned short *plan, const ProdPtrs *ptrs, cudaStream_t s,
-                 ProdPtrs single = ProdPtrs{nullptr, nullptr, nullptr, nullptr, 0, 0, 0});
-// One-time kernel attributes of the tile refill (call outside any stream capture).
-void tile_refill_prepare();
-// Copies `n` descriptors, shifting their entry / plan offsets and setting `prod`.
-void rebase_tiles(const TileDesc *src, int n, long long ent_shift, long long plan_shift, int prod,
-                  TileDesc *dst, cudaStream_t s);
-// The larger rows of one product (CTA kernels), for the given values.
+// tile t reads its pointers from ptrs[tiles[t].prod] / scheds[tiles[t].prod], or,
+// with null tables, from `vals` / `sched`.
+void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
+                 cudaStream_t s, ProdPtrs vals = ProdPtrs{}, ProdSched sched = ProdSched{});
+// Copies `n` descriptors, setting `prod`.
+void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s);
+// The larger rows of one product (CTA kernels), for the given values; with `vals`
+// (a device ProdPtrs) the kernels read the value pointers from there instead.
 void big_rows_refill(const Product &P, const double *Lx, const double *d, const double *Ax,
-                     double *Cx, cudaStream_t s);
+                     double *Cx, cudaStream_t s, const ProdPtrs *vals = nullptr);
 
 } // namespace sdl

@@ -143,6 +143,22 @@ def test_btda_many_collisions(sdl, orc):
     assert_same(got[0], orc.btda(A, B, d))
 
 
+def test_btda_tile_outputs_with_long_term_lists(sdl, orc):
+    """Tile rows whose outputs collect 2 to ~70 terms (every list length modulo the
+    kernel's batch of 4), with values spread over 16 decades so that a change of
+    summation order would show in the bits; thousands of tiles, so the refill's
+    pipeline runs in steady state and wraps its buffers many times."""
+    rng = np.random.default_rng(79)
+    m, nA = 60000, 4
+    A = wl.fixed_rowlen_csr(m, nA, 4, rng)          # every A row hits all 4 columns
+    A = (A[0], A[1], A[2] * 10.0 ** rng.integers(-8, 9, len(A[2])), A[3], A[4])
+    col_lens = list(rng.integers(1, 72, 6000))      # rows of L: 1..71 entries
+    _, B = _skewed_operands(rng, m, nA, len(col_lens), col_lens, 4)
+    d = rng.uniform(0.1, 10, m)
+    got = gpu_btda(sdl, A, B, d)
+    assert_same(got[0], orc.btda(A, B, d))
+
+
 def test_spgemm_config1_bit_exact(sdl, orc):
     """C = A B for the 2000 x 2000, 5 per row case: A's CSR read as CSC is A^T."""
     A, B = wl.spgemm_small(seed=0)
