@@ -63,7 +63,8 @@ struct NumArgs
     const int *Cp, *Ci;
     double *Cx;
     int *err;
-    int L_nnz; // entries of L (schedule build: entry index b * L_nnz + ii)
+    int L_nnz;       // entries of L (schedule build: entry index b * L_nnz + ii)
+    int value_order; // entry values kept in L's value order (L_map a permutation)
 };
 
 // ------------------------------------------------------------ row statistics
@@ -137,18 +138,26 @@ __global__ void k_mask_classes(const unsigned char *__restrict__ mask, int m_out
         if (!mask[r]) cls[r] = 255;
 }
 
-__global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp, int m_out,
+// Numeric class and tile weight of every output row. A tile row costs its terms,
+// one unit per 16 of its L entries and TILE_T / TILE_THREADS units; a larger row
+// costs TILE_T, so it always ends its tile. Rows with more than TILE_MAX_LROW L
+// entries never join a tile (the 18-bit entry index of a term word stays in range).
+constexpr int TILE_MAX_LROW = 131072;
+__global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp,
+                               const int *__restrict__ Lp, int L_m, int m_out,
                                unsigned char *__restrict__ cls, long long *__restrict__ weight)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
          r += (long long)gridDim.x * blockDim.x)
     {
-        long long u = ub[r];
-        int nr = Cp[r + 1] - Cp[r];
+        const long long u = ub[r];
+        const int nr = Cp[r + 1] - Cp[r];
+        const int rr = (int)(r % L_m);
+        const int lenL = Lp[rr + 1] - Lp[rr];
         int c;
         if (u == 0)
             c = 255;
-        else if (u <= TILE_T)
+        else if (u <= TILE_T && lenL <= TILE_MAX_LROW)
             c = NUM_TILE;
         else if (nr <= 2048)
             c = NUM_C2K;
@@ -157,7 +166,8 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
         else
             c = NUM_GMEM;
         cls[r] = (unsigned char)c;
-        weight[r] = c == NUM_TILE ? u + TILE_T / TILE_THREADS : (c == 255 ? TILE_T / TILE_THREADS : TILE_T);
+        const long long lw = (lenL + 15) / 16 + TILE_T / TILE_THREADS;
+        weight[r] = c == NUM_TILE ? u + lw : (c == 255 ? lw : TILE_T);
     }
 }
 
@@ -459,58 +469,64 @@ __device__ __forceinline__ int last_le(const int *a, int n, int key)
 
 struct BuildSmem
 {
-    int *cnt;  // TILE_ACC: terms per output (pass A)
-    int *cur;  // TILE_ACC: term-list cursor of a multi-term output, -1 otherwise
+    int *cnt; // TILE_ACC: terms per output
+    int *cur; // TILE_ACC: list cursor of an output with three or more terms, -1 otherwise
     int *row_cs, *row_nr, *row_ls, *row_b, *row_outoff, *row_eoff;
-    int *e_incl, *e_s, *e_len, *e_row, *e_ii;
+    int *e_incl, *e_s, *e_len, *e_row;
     int *scr;
-    int *misc; // [1]: multi-term outputs of a chunk, [2]: their terms
+    int *misc; // [1]: list outputs of a chunk, [2]: their terms
 };
 constexpr size_t build_smem_bytes()
 {
-    return ((size_t)2 * TILE_ACC + 4 * TILE_THREADS + 2 * (TILE_THREADS + 1) + 5 * TILE_THREADS + 32 + 4) * 4;
+    return ((size_t)2 * TILE_ACC + 4 * TILE_THREADS + 2 * (TILE_THREADS + 1) + 4 * TILE_THREADS + 32 + 4) * 4;
 }
 
-// Term enumeration of one tile, shared by both passes of the schedule build: calls
-// f(valid, e, jj, o) for every term of the tile in upstream's visiting order, 256
+// Term enumeration of one tile, shared by both passes of the schedule build. The
+// tile's L entries (every entry of its rows, in order: entry e is schedule entry
+// vbase + e) are taken 256 at a time; fe(e, s, toff, len, slot) is called for each
+// by its thread (s = A.p[k], toff = offset of its first term in the tile, len = its
+// terms, slot = index of its value in V),
+// then ft(valid, e, u, o) for every term in upstream's visiting order, 256
 // consecutive terms per step (valid false for the idle threads of the last step,
-// so every thread takes every barrier). e is the term's entry of kron(I_blocks, L)
-// (b * L_nnz + ii), jj its position in A, o its output inside the tile window.
-template <class F>
-__device__ __forceinline__ void tile_terms(const NumArgs &a, const BuildSmem &t, int nrows, int total_raw, F f)
+// so every thread takes every barrier): u is the term's index in the tile, o its
+// output inside the tile window.
+template <class FE, class FT>
+__device__ __forceinline__ int tile_terms(const NumArgs &a, const BuildSmem &t, int nrows, int total_raw, FE fe,
+                                           FT ft)
 {
     const int tid = threadIdx.x;
+    int cursor = 0;
     for (int ec = 0; ec < total_raw; ec += TILE_THREADS)
     {
         const int e = ec + tid;
-        int s = 0, len = 0, lrow = 0, ii = 0;
+        int s = 0, len = 0, lrow = 0, slot = 0;
         if (e < total_raw)
         {
             lrow = last_le(t.row_eoff, nrows, e);
-            ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
+            const int ii = t.row_ls[lrow] + (e - t.row_eoff[lrow]);
             const int k = a.Li[ii] + t.row_b[lrow] * a.n_L;
             s = a.Ap[k];
             len = a.Ap[k + 1] - s;
+            slot = t.row_b[lrow] * a.L_nnz + (a.value_order ? a.L_map[ii] : ii);
         }
-        const int inc_t = block_incl_scan_int(len, t.scr);
-        t.e_incl[tid] = inc_t;
+        const int inc = block_incl_scan_int(len, t.scr);
+        if (e < total_raw) fe(e, s, cursor + inc - len, len, slot);
+        t.e_incl[tid] = inc;
         t.e_s[tid] = s;
         t.e_len[tid] = len;
         t.e_row[tid] = lrow;
-        t.e_ii[tid] = ii;
         __syncthreads();
         const int total = t.e_incl[TILE_THREADS - 1];
         const int nent = min(TILE_THREADS, total_raw - ec);
         for (int base = 0; base < total; base += TILE_THREADS)
         {
-            const int u = base + tid;
-            bool valid = u < total;
-            int el = 0, jj = 0, o = 0;
-            unsigned eg = 0;
+            const int uu = base + tid;
+            bool valid = uu < total;
+            int el = 0, o = 0;
             if (valid)
             {
-                el = cta_entry_of(t.e_incl, nent, u);
-                jj = t.e_s[el] + u - (t.e_incl[el] - t.e_len[el]);
+                el = cta_entry_of(t.e_incl, nent, uu);
+                const int jj = t.e_s[el] + uu - (t.e_incl[el] - t.e_len[el]);
                 const int j = a.Ai[jj];
                 const int lr = t.e_row[el];
                 const int w = t.row_nr[lr];
@@ -522,28 +538,43 @@ __device__ __forceinline__ void tile_terms(const NumArgs &a, const BuildSmem &t,
                     valid = false;
                 }
                 o = t.row_outoff[lr] + pos;
-                eg = (unsigned)t.row_b[lr] * (unsigned)a.L_nnz + (unsigned)t.e_ii[el];
             }
-            f(valid, eg, jj, o);
+            ft(valid, ec + el, cursor + uu, o);
         }
+        cursor += total;
         __syncthreads();
+    }
+    return cursor;
+}
+
+// kv[L_map[ii]] = Li[ii]; flags a map that is not a permutation of [0, n).
+__global__ void k_value_rows(const int *__restrict__ L_map, const int *__restrict__ Li, int n,
+                             int *__restrict__ kv, int *__restrict__ cnt, int *__restrict__ bad)
+{
+    for (long long ii = blockIdx.x * (long long)blockDim.x + threadIdx.x; ii < n;
+         ii += (long long)gridDim.x * blockDim.x)
+    {
+        const int m = L_map[ii];
+        if ((unsigned)m >= (unsigned)n || atomicAdd(&cnt[m], 1) != 0)
+            atomicOr(bad, 1);
+        else
+            kv[m] = Li[ii];
     }
 }
 
-// Compiles the output-major refill schedule of one tile (one CTA per tile, once
-// per pattern). Every output of the tile window gets one 8-byte word:
-//   {jj, e}                       its only term is V[e] * A.x[jj];
-//   {start, MULTI_BIT | count}    it collects count >= 2 terms, the {jj, e} pairs
-//                                 X[start .. start + count - 1] in upstream's
-//                                 visiting order.
-// COUNT pass: the numbers of output words and list pairs of every tile. BUILD pass:
-// writes the descriptor, the words and the lists at the offsets the scans gave.
+// Compiles the entry-major refill schedule of one tile (one CTA per tile, once per
+// pattern): the ES records of the tile's entries, one word per term (see TileDesc), and the
+// list section of the outputs with three or more terms: nlist + 1 headers
+// (output | first list item << 12) and the term indices of each such output in
+// upstream's visiting order.
+// COUNT pass: the numbers of term words and list-section words of every tile.
+// BUILD pass: writes everything at the offsets the scans of those numbers gave.
 template <bool BUILD>
 __global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
     NumArgs a, const unsigned char *__restrict__ rcls, const int *__restrict__ tile_start,
-    long long *__restrict__ tile_nwords, long long *__restrict__ tile_nx,
+    long long *__restrict__ tile_nterms, long long *__restrict__ tile_nx,
     const long long *__restrict__ word_begin, const long long *__restrict__ x_begin,
-    TileDesc *__restrict__ tiles, uint2 *__restrict__ W, uint2 *__restrict__ X)
+    TileDesc *__restrict__ tiles, unsigned *__restrict__ W, unsigned *__restrict__ X, int2 *__restrict__ ES)
 {
     extern __shared__ __align__(16) int bsm[];
     BuildSmem t;
@@ -559,8 +590,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
     t.e_s = t.e_incl + TILE_THREADS;
     t.e_len = t.e_s + TILE_THREADS;
     t.e_row = t.e_len + TILE_THREADS;
-    t.e_ii = t.e_row + TILE_THREADS;
-    t.scr = t.e_ii + TILE_THREADS;
+    t.scr = t.e_row + TILE_THREADS;
     t.misc = t.scr + 32;
     const int tid = threadIdx.x;
     const int tile = blockIdx.x;
@@ -572,11 +602,11 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
         const int r = r0 + tid;
         const int b = r / a.L_m, rr = r - b * a.L_m;
         const int cs = a.Cp[r], ls = a.Lp[rr];
-        if (rcls[r] == NUM_TILE)
-        {
-            nr = a.Cp[r + 1] - cs;
-            ne = a.Lp[rr + 1] - ls;
-        }
+        const int c = rcls[r];
+        if (c == NUM_TILE) nr = a.Cp[r + 1] - cs;
+        // every L entry of the tile's rows up to a larger row (always the last row),
+        // so that entry e of the tile is entry vbase + e
+        if (c == NUM_TILE || c == 255) ne = a.Lp[rr + 1] - ls;
         t.row_cs[tid] = cs;
         t.row_nr[tid] = nr;
         t.row_ls[tid] = ls;
@@ -601,29 +631,35 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
         if (tid == 0) atomicOr(a.err, 2);
         return; // cannot happen with the tile weights; the host reports it
     }
+    const int b0 = r0 / a.L_m;
+    const int vb = b0 * a.L_nnz + a.Lp[r0 - b0 * a.L_m];
     const long long wb = BUILD ? word_begin[tile] : 0, xb = BUILD ? x_begin[tile] : 0;
 
-    // pass A: terms per output; the word of every output with one term
-    tile_terms(a, t, nrows, total_raw, [&](bool valid, unsigned e, int jj, int o) {
-        if (!valid) return;
-        atomicAdd(&t.cnt[o], 1);
-        if (BUILD) W[wb + o] = make_uint2((unsigned)jj, e);
-    });
+    // pass A: terms per output; the ES records of the entries
+    const int nterms = tile_terms(
+        a, t, nrows, total_raw,
+        [&](int e, int s, int toff, int len, int slot) {
+            if (BUILD && len > 0) ES[vb + e] = make_int2(s - toff, slot);
+            if (e >= (1 << 18) && len > 0) atomicOr(a.err, 2);
+        },
+        [&](bool valid, int, int, int o) {
+            if (valid) atomicAdd(&t.cnt[o], 1);
+        });
     __syncthreads();
-    // multi-term outputs: their word and list offset
-    int nexc = 0, nxt = 0;
+    // outputs with three or more terms: list index and first item
+    int nlist = 0, nitems = 0;
     for (int oc = 0; oc < total_out; oc += TILE_THREADS)
     {
         const int o = oc + tid;
         const int c = o < total_out ? t.cnt[o] : 0;
         if (o < total_out && c == 0) atomicOr(a.err, 1); // every output has a term
-        const int m = c >= 2 ? 1 : 0;
+        const int m = c >= 3 ? 1 : 0;
         const int im = block_incl_scan_int(m, t.scr);
         const int it = block_incl_scan_int(m ? c : 0, t.scr);
         if (o < total_out)
         {
-            t.cur[o] = m ? nxt + it - c : -1;
-            if (BUILD && m) W[wb + o] = make_uint2((unsigned)(xb + nxt + it - c), MULTI_BIT | (unsigned)c);
+            t.cur[o] = m ? nitems + it - c : -1;
+            if (BUILD && m) X[xb + nlist + im - 1] = (unsigned)o | ((unsigned)(nitems + it - c) << 12);
         }
         if (tid == TILE_THREADS - 1)
         {
@@ -631,80 +667,94 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
             t.misc[2] = it;
         }
         __syncthreads();
-        nexc += t.misc[1];
-        nxt += t.misc[2];
+        nlist += t.misc[1];
+        nitems += t.misc[2];
         __syncthreads();
     }
     if (!BUILD)
     {
         if (tid == 0)
         {
-            tile_nwords[tile] = total_out;
-            tile_nx[tile] = nxt;
+            tile_nterms[tile] = nterms;
+            tile_nx[tile] = nlist ? nlist + 1 + nitems : 0;
         }
         return;
     }
-    if (nexc)
-    {
-        // pass B: the terms of multi-term outputs into their lists in visiting order;
-        // warps take turns, and inside a warp equal outputs are ranked by lane
-        uint2 *xt = X + xb;
-        const int warp = tid >> 5, lane = lane_id();
-        tile_terms(a, t, nrows, total_raw, [&](bool valid, unsigned e, int jj, int o) {
-            const bool multi = valid && t.cur[o] >= 0;
+    if (nlist && tid == 0) X[xb + nlist] = (unsigned)nitems << 12;
+    // pass B: the term words; the term indices of list outputs into their lists in
+    // visiting order (warps take turns, equal outputs inside a warp ranked by lane)
+    unsigned *xl = X + xb + nlist + 1;
+    const int warp = tid >> 5, lane = lane_id();
+    tile_terms(
+        a, t, nrows, total_raw, [&](int, int, int, int, int) {},
+        [&](bool valid, int e, int u, int o) {
+            bool listed = false;
+            if (valid)
+            {
+                const int c = t.cnt[o];
+                const unsigned kind = c == 1 ? TERM_ONE : (c == 2 ? TERM_PAIR : TERM_LIST);
+                W[wb + u] = ((unsigned)e << 14) | (kind << 12) | (unsigned)o;
+                listed = kind == TERM_LIST;
+            }
+            if (!nlist) return; // uniform over the block
             for (int w = 0; w < TILE_THREADS / 32; ++w)
             {
                 if (warp == w)
                 {
-                    const int key = multi ? o : -(lane + 1);
+                    const int key = listed ? o : -(lane + 1);
                     const unsigned grp = __match_any_sync(FULL_MASK, key);
                     int slot = 0;
-                    if (multi) slot = t.cur[o] + __popc(grp & lanemask_lt());
+                    if (listed) slot = t.cur[o] + __popc(grp & lanemask_lt());
                     __syncwarp();
-                    if (multi)
+                    if (listed)
                     {
-                        xt[slot] = make_uint2((unsigned)jj, e);
+                        xl[slot] = (unsigned)u;
                         if (lane == 31 - __clz(grp)) t.cur[o] += __popc(grp);
                     }
                 }
                 __syncthreads();
             }
         });
-    }
     if (tid == 0)
     {
         TileDesc dsc;
+        dsc.vbase = vb;
         dsc.word_begin = (int)wb;
+        dsc.nterms = nterms;
         dsc.out_begin = t.row_cs[0];
         dsc.nout = total_out;
+        dsc.x_begin = nlist ? (int)xb : -1;
+        dsc.nlist = nlist;
         dsc.prod = 0;
         tiles[tile] = dsc;
     }
 }
 
-// Entry values of one refill: V[e] = L.x * d[k] for every entry e = b * L_nnz + ii
-// of kron(I_blocks, L) (upstream's order of the two factors; L.x alone without d,
-// 1.0 for a unit L). Each thread takes EV_ILP entries, spaced one grid apart, and
-// issues all their loads before the first store.
+// Entry values of one refill: V[i] = L.x * d[k] (upstream's order of the two
+// factors; L.x alone without d, 1.0 for a unit L) for every entry of
+// kron(I_blocks, L). With S.kv (L_map a permutation) V is in L's value order,
+// i = b * L_nnz + (index of the value), so L.x is read in order and kv gives the
+// entry's row of A; otherwise i = b * L_nnz + ii. Each thread takes EV_ILP entries,
+// spaced one grid apart, and issues all their loads before the first store.
 constexpr int EV_ILP = 4;
 __device__ __forceinline__ void entry_values_run(const ProdSched &S, const ProdPtrs &P, long long first,
                                                  long long end, long long step)
 {
     for (long long base = first; base < end; base += step * EV_ILP)
     {
-        int ii[EV_ILP], k[EV_ILP];
+        int xi[EV_ILP], k[EV_ILP];
 #pragma unroll
         for (int j = 0; j < EV_ILP; ++j)
         {
             const long long i = base + j * step;
-            ii[j] = -1;
+            xi[j] = -1;
             k[j] = 0;
             if (i < end)
             {
                 const int b = S.blocks > 1 ? (int)(i / S.L_nnz) : 0;
-                ii[j] = (int)(i - (long long)b * S.L_nnz);
-                if (P.d) k[j] = S.Li[ii[j]] + b * S.n_L;
-                if (P.Lx && S.L_map) ii[j] = S.L_map[ii[j]]; // index of the L value
+                const int sl = (int)(i - (long long)b * S.L_nnz);
+                if (P.d) k[j] = (S.kv ? S.kv[sl] : S.Li[sl]) + b * S.n_L;
+                xi[j] = (!S.kv && S.L_map) ? S.L_map[sl] : sl; // index of the L value
             }
         }
         double lx[EV_ILP], dk[EV_ILP];
@@ -713,9 +763,9 @@ __device__ __forceinline__ void entry_values_run(const ProdSched &S, const ProdP
         {
             lx[j] = 1.0;
             dk[j] = 1.0;
-            if (ii[j] >= 0)
+            if (xi[j] >= 0)
             {
-                if (P.Lx) lx[j] = P.Lx[ii[j]];
+                if (P.Lx) lx[j] = P.Lx[xi[j]];
                 if (P.d) dk[j] = P.d[k[j]];
             }
         }
@@ -746,75 +796,27 @@ __global__ void __launch_bounds__(256) k_entry_values_batched(const EntChunk *__
 }
 
 #ifndef SDL_REFILL_MINB
-#define SDL_REFILL_MINB 6
+#define SDL_REFILL_MINB 5
 #endif
 #ifndef SDL_REFILL_UNROLL
 #define SDL_REFILL_UNROLL 4
 #endif
 constexpr int REFILL_THREADS = 256;
-constexpr int RUNROLL = SDL_REFILL_UNROLL; // outputs per thread whose loads are in flight together
+constexpr int RUNROLL = SDL_REFILL_UNROLL; // terms per thread whose loads are in flight together
+constexpr int RSTEP = RUNROLL * REFILL_THREADS;
+constexpr int WIN = TILE_ACC; // outputs of a tile window
 
-// Sum of an output's term list from +0.0 in list (upstream's visiting) order; the
-// loads of four terms are in flight together.
-__device__ __forceinline__ double multi_sum(const uint2 *__restrict__ X, long long nX,
-                                         const double *__restrict__ Ax, const double *__restrict__ V, uint2 w,
-                                         unsigned nA, unsigned nV, int *err)
-{
-    const unsigned cnt = w.y & ~MULTI_BIT;
-    const unsigned long long start = w.x;
-    if (start + cnt > (unsigned long long)nX)
-    {
-        atomicOr(err, 1);
-        return 0.0;
-    }
-    const uint2 *L = X + start;
-    double acc = 0.0;
-    for (unsigned i = 0; i < cnt; i += 4)
-    {
-        double xx[4], vv[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-        {
-            xx[j] = 0.0;
-            vv[j] = 0.0;
-            if (i + j < cnt)
-            {
-                const uint2 p = L[i + j];
-                if (p.x < nA && p.y < nV)
-                {
-                    xx[j] = Ax[p.x];
-                    vv[j] = V[p.y];
-                }
-                else
-                    atomicOr(err, 1);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (i + j < cnt) acc = __dadd_rn(acc, __dmul_rn(vv[j], xx[j]));
-    }
-    return acc;
-}
+__host__ __device__ constexpr size_t refill_smem_bytes() { return 2 * (size_t)WIN * 8 + 4 * sizeof(TileDesc); }
 
-// Refill of the tile rows from the output-major schedule. Persistent CTAs walk
-// their tiles (blockIdx.x, + gridDim.x, ...); every thread works on its own
-// outputs, with no shared memory and no barrier: per output a word, then the two
-// gathers V[e] and A.x[jj], then one coalesced store. While the gathers of tile k
-// are in flight, the words of tile k+1 (whose descriptor came one tile earlier) are
-// already being loaded, so a tile exposes about one memory round trip.
-// An output with one term is 0.0 + V[e] * A.x[jj] (upstream's accumulator starts
-// at +0.0); an output with several terms sums its list from +0.0 in upstream's
-// visiting order. Nothing is accumulated with atomics: every output is
-// bit-identical to upstream's.
 // Base pointers of the product a tile belongs to: kernel parameters for a single
-// product, the batch's tables otherwise (re-read where needed: they stay in L1).
+// product, the batch's tables otherwise.
 struct ProdBase
 {
-    const uint2 *W, *X;
+    const unsigned *W, *X;
     const double *Ax, *V;
+    const int2 *ES;
     double *C;
-    long long nX;
-    unsigned nA, nV;
+    unsigned nV, nA; // both < 2^31
 };
 template <bool BATCHED>
 __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restrict__ ptrs,
@@ -829,9 +831,9 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
         r.W = scheds[prod].W;
         r.X = scheds[prod].X;
         r.V = scheds[prod].V;
-        r.nX = scheds[prod].nX;
-        r.nA = (unsigned)scheds[prod].nA;
+        r.ES = scheds[prod].ES;
         r.nV = (unsigned)scheds[prod].nV;
+        r.nA = (unsigned)scheds[prod].nA;
     }
     else
     {
@@ -840,112 +842,190 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
         r.W = S1.W;
         r.X = S1.X;
         r.V = S1.V;
-        r.nX = S1.nX;
-        r.nA = (unsigned)S1.nA;
+        r.ES = S1.ES;
         r.nV = (unsigned)S1.nV;
+        r.nA = (unsigned)S1.nA;
     }
     return r;
 }
 
-// (word_begin, out_begin, nout, prod) of tile t
-__device__ __forceinline__ int4 tile_desc(const TileDesc *__restrict__ tiles, int t)
-{
-    return *reinterpret_cast<const int4 *>(tiles + t);
-}
-
-__device__ __forceinline__ void load_words(const uint2 *__restrict__ W, int nout, int base, uint2 (&w)[RUNROLL])
+__device__ __forceinline__ void load_terms(const unsigned *__restrict__ W, int nterms, int base,
+                                           unsigned (&w)[RUNROLL])
 {
 #pragma unroll
-    for (int u = 0; u < RUNROLL; ++u)
+    for (int j = 0; j < RUNROLL; ++j)
     {
-        const int o = base + threadIdx.x + u * REFILL_THREADS;
-        w[u] = o < nout ? W[o] : make_uint2(0u, MULTI_BIT);
+        const int u = base + threadIdx.x + j * REFILL_THREADS;
+        w[j] = u < nterms ? W[u] : (TERM_LIST << 12); // a list word is skipped by the term pass
     }
 }
 
-// Refill of the tile rows from the output-major schedule. Persistent CTAs walk
-// their tiles (blockIdx.x, + gridDim.x, ...); every thread works on its own
-// outputs, with no shared memory and no barrier: per output a word, then the two
-// gathers V[e] and A.x[jj], then one coalesced store. The words of the next step
-// (the next RUNROLL * REFILL_THREADS outputs of the tile, or the first ones of the
-// next tile, whose descriptor was read two tiles ahead) are loaded while the
-// current step's gathers are in flight, so a step exposes about one round trip.
-// An output with one term is 0.0 + V[e] * A.x[jj] (upstream's accumulator starts
-// at +0.0); an output with several terms sums its list from +0.0 in upstream's
-// visiting order. Nothing is accumulated with atomics: every output is
-// bit-identical to upstream's.
+// One term u of entry e of a tile: V[slot] * A.x[bq + u]; false if the schedule
+// does not hold a valid entry / position (reported through err by the caller).
+__device__ __forceinline__ bool term_value(const ProdBase &pb, int vbase, unsigned w, int u, double &prod)
+{
+    const unsigned vi = (unsigned)(vbase + (int)(w >> 14));
+    if (vi >= pb.nV) return false;
+    const int2 es = pb.ES[vi];
+    const unsigned a = (unsigned)(es.x + u);
+    if (a >= pb.nA || (unsigned)es.y >= pb.nV) return false;
+    prod = __dmul_rn(pb.V[es.y], pb.Ax[a]);
+    return true;
+}
+
+// Sum of a list output's terms from +0.0 in upstream's visiting order; the loads of
+// four terms are in flight together.
+__device__ __forceinline__ double list_sum(const ProdBase &pb, const TileDesc &D, const unsigned *__restrict__ items,
+                                           int first, int end, int *err)
+{
+    const unsigned *Wt = pb.W + D.word_begin;
+    double acc = 0.0;
+    for (int i = first; i < end; i += 4)
+    {
+        double pr[4];
+        bool ok[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            ok[j] = false;
+            pr[j] = 0.0;
+            if (i + j < end)
+            {
+                const int u = (int)items[i + j];
+                ok[j] = (unsigned)u < (unsigned)D.nterms && term_value(pb, D.vbase, Wt[u], u, pr[j]);
+                if (!ok[j]) atomicOr(err, 1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (ok[j]) acc = __dadd_rn(acc, pr[j]);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void copy_desc(TileDesc *dst, const TileDesc *__restrict__ src)
+{
+    if (threadIdx.x < (int)(sizeof(TileDesc) / 4))
+        reinterpret_cast<int *>(dst)[threadIdx.x] = reinterpret_cast<const int *>(src)[threadIdx.x];
+}
+
+// Refill of the tile rows from the entry-major schedule. Persistent CTAs walk their
+// tiles (blockIdx.x, + gridDim.x, ...). Per step every thread takes RUNROLL terms:
+// word -> the entry's ES record (consecutive terms share entries: a few lines per
+// warp) -> V[slot] and A.x[bq + u] (consecutive terms of an entry read one A row)
+// -> the product into the tile's window in shared memory: stored for an output's
+// only term (0.0 + v * A.x: upstream's accumulator starts at +0.0), atomically
+// added for the two terms of a two-term output ((0 + a) + b == (0 + b) + a, signed
+// zeros included). Outputs with three or more terms are summed afterwards by one
+// thread each, in upstream's visiting order. The window is written back to C once,
+// coalesced, and cleared; two windows alternate, so a tile needs one barrier. The
+// words of the next step -- or of the next tile, whose descriptor is read two
+// tiles ahead -- are loaded while a step's gathers are in flight.
 template <bool BATCHED>
 __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill(
     const TileDesc *__restrict__ tiles, int ntiles, const ProdPtrs *__restrict__ ptrs,
     const ProdSched *__restrict__ scheds, ProdPtrs P1, ProdSched S1, int *__restrict__ err)
 {
-    constexpr int CH = RUNROLL * REFILL_THREADS; // outputs of a tile per step
+    extern __shared__ __align__(16) double rsm[];
+    TileDesc *dsc = reinterpret_cast<TileDesc *>(rsm + 2 * WIN);
+    const int tid = threadIdx.x;
     const int G = gridDim.x;
     int t = blockIdx.x;
     if (t >= ntiles) return;
-    int4 dc = tile_desc(tiles, t); // (word_begin, out_begin, nout, prod)
-    int4 d1 = t + G < ntiles ? tile_desc(tiles, t + G) : make_int4(0, 0, 0, 0);
-    uint2 w[RUNROLL];
-    load_words(prod_base<BATCHED>(dc.w, ptrs, scheds, P1, S1).W + dc.x, dc.z, 0, w);
-    while (true)
+    for (int i = tid; i < 2 * WIN; i += REFILL_THREADS) rsm[i] = 0.0;
+    copy_desc(dsc, tiles + t);
+    if (t + G < ntiles) copy_desc(dsc + 1, tiles + t + G);
+    __syncthreads();
+    unsigned w[RUNROLL];
     {
+        const ProdBase pb = prod_base<BATCHED>(dsc[0].prod, ptrs, scheds, P1, S1);
+        load_terms(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
+    }
+    for (int k = 0;; ++k)
+    {
+        const TileDesc &D = dsc[k & 3];
         const bool has1 = t + G < ntiles;
-        const int4 d2 = t + 2 * G < ntiles ? tile_desc(tiles, t + 2 * G) : make_int4(0, 0, 0, 0);
-        for (int base = 0;; base += CH)
+        if (t + 2 * G < ntiles) copy_desc(dsc + ((k + 2) & 3), tiles + t + 2 * G);
+        double *win = rsm + (k & 1) * WIN;
+        const ProdBase pb = prod_base<BATCHED>(D.prod, ptrs, scheds, P1, S1);
+        const int nterms = D.nterms, nout = D.nout, vbase = D.vbase;
+        for (int base = 0;; base += RSTEP)
         {
-            const bool last = base + CH >= dc.z;
-            // gathers of this step
-            double x[RUNROLL], v[RUNROLL];
-            unsigned one = 0, multi = 0;
-            {
-                const ProdBase pb = prod_base<BATCHED>(dc.w, ptrs, scheds, P1, S1);
+            const bool last = base + RSTEP >= nterms;
+            int2 es[RUNROLL];
+            bool ok[RUNROLL];
 #pragma unroll
-                for (int u = 0; u < RUNROLL; ++u)
-                {
-                    const int o = base + threadIdx.x + u * REFILL_THREADS;
-                    // a multi-term word has y >= MULTI_BIT > nV
-                    const bool ok = w[u].x < pb.nA && w[u].y < pb.nV;
-                    x[u] = ok ? pb.Ax[w[u].x] : 0.0;
-                    v[u] = ok ? pb.V[w[u].y] : 0.0;
-                    if (o < dc.z)
-                    {
-                        if (ok)
-                            one |= 1u << u;
-                        else if (w[u].y & MULTI_BIT)
-                            multi |= 1u << u;
-                        else
-                            atomicOr(err, 1);
-                    }
-                }
-            }
-            // words of the next step
-            const int4 dn = last ? d1 : dc;
-            const int nb = last ? 0 : base + CH;
-            if (!last || has1)
-                load_words(prod_base<BATCHED>(dn.w, ptrs, scheds, P1, S1).W + dn.x, dn.z, nb, w);
-            // results of this step
+            for (int j = 0; j < RUNROLL; ++j)
             {
-                const ProdBase pb = prod_base<BATCHED>(dc.w, ptrs, scheds, P1, S1);
-                double *C = pb.C + dc.y;
-#pragma unroll
-                for (int u = 0; u < RUNROLL; ++u)
-                    if (one >> u & 1u)
-                        C[base + threadIdx.x + u * REFILL_THREADS] = __dadd_rn(0.0, __dmul_rn(v[u], x[u]));
-                // multi-term outputs (their word is re-read, from L1)
-                const uint2 *Wt = pb.W + dc.x;
-#pragma unroll 1
-                for (; multi; multi &= multi - 1)
-                {
-                    const int o = base + threadIdx.x + (__ffs(multi) - 1) * REFILL_THREADS;
-                    C[o] = multi_sum(pb.X, pb.nX, pb.Ax, pb.V, Wt[o], pb.nA, pb.nV, err);
-                }
+                const unsigned vi = (unsigned)(vbase + (int)(w[j] >> 14));
+                ok[j] = !(w[j] & (TERM_LIST << 12)) && vi < pb.nV;
+                es[j] = ok[j] ? pb.ES[vi] : make_int2(0, 0);
             }
+            double v[RUNROLL], x[RUNROLL];
+#pragma unroll
+            for (int j = 0; j < RUNROLL; ++j)
+            {
+                const unsigned a = (unsigned)(es[j].x + base + tid + j * REFILL_THREADS);
+                ok[j] = ok[j] && a < pb.nA && (unsigned)es[j].y < pb.nV;
+                v[j] = ok[j] ? pb.V[es[j].y] : 0.0;
+                x[j] = ok[j] ? pb.Ax[a] : 0.0;
+            }
+            unsigned wn[RUNROLL];
+            if (!last)
+                load_terms(pb.W + D.word_begin, nterms, base + RSTEP, wn);
+            else if (has1)
+            {
+                const TileDesc &Dn = dsc[(k + 1) & 3];
+                const ProdBase pn = prod_base<BATCHED>(Dn.prod, ptrs, scheds, P1, S1);
+                load_terms(pn.W + Dn.word_begin, Dn.nterms, 0, wn);
+            }
+            else
+                load_terms(nullptr, 0, 0, wn); // nothing: list words
+#pragma unroll
+            for (int j = 0; j < RUNROLL; ++j)
+            {
+                if (w[j] & (TERM_LIST << 12)) continue;
+                const int p = (int)(w[j] & 0xfffu);
+                if (!ok[j] || p >= nout)
+                {
+                    atomicOr(err, 1);
+                    continue;
+                }
+                const double prod = __dmul_rn(v[j], x[j]);
+                if (w[j] & (TERM_PAIR << 12))
+                    atomicAdd(&win[p], prod);
+                else
+                    win[p] = __dadd_rn(0.0, prod);
+            }
+#pragma unroll
+            for (int j = 0; j < RUNROLL; ++j) w[j] = wn[j];
             if (last) break;
         }
+        __syncthreads(); // the window is complete
+        if (D.nlist > 0)
+        {
+            const unsigned *hdr = pb.X + D.x_begin;
+            const unsigned *items = hdr + D.nlist + 1;
+            for (int l = tid; l < D.nlist; l += REFILL_THREADS)
+            {
+                const unsigned h = hdr[l];
+                const int p = (int)(h & 0xfffu);
+                const double acc = list_sum(pb, D, items, (int)(h >> 12), (int)(hdr[l + 1] >> 12), err);
+                if (p < nout)
+                    win[p] = acc;
+                else
+                    atomicOr(err, 1);
+            }
+            __syncthreads();
+        }
+        double *C = pb.C + D.out_begin;
+        for (int o = tid; o < nout; o += REFILL_THREADS)
+        {
+            C[o] = win[o];
+            win[o] = 0.0;
+        }
         if (!has1) break;
-        dc = d1;
-        d1 = d2;
-        t += G;
+        t += G; // the words of the next tile were loaded by the last step
     }
 }
 
@@ -1225,8 +1305,8 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     const int m_out = P.m_out;
     DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1);
     DevBuf<unsigned char> rcls(m_out);
-    SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub, P.Cp.get(), m_out,
-               rcls.get(), weight.get());
+    SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub, P.Cp.get(), d.Lp, d.L_m,
+               m_out, rcls.get(), weight.get());
     bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
     exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
     DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
@@ -1239,27 +1319,48 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     SDL_CUDA(cudaMemcpyAsync(tile_start.get() + P.ntiles, &P.m_out, sizeof(int), cudaMemcpyHostToDevice, s));
     const int nt = std::max(1, P.ntiles);
     const long long nV = (long long)d.L_nnz * d.blocks;
-    if (nV >= (long long)MULTI_BIT || d.A_nnz < 0)
+    if (nV > INT_MAX || d.A_nnz < 0)
         fail(SDL_ERR_OVERFLOW, "product: blocks * entries of L exceeds the schedule's 31-bit entry index");
-    DevBuf<long long> tile_nwords(nt), tile_nx(nt), word_begin((size_t)nt + 1), x_begin((size_t)nt + 1);
+    // entry values in L's value order when L_map is a permutation of [0, L_nnz)
+    // (the refill then reads L.x in order); kv gives each value's row of A
+    int value_order = 0;
+    P.kv.release();
+    if (d.L_map && d.L_nnz > 0)
+    {
+        DevBuf<int> cnt(d.L_nnz), bad(1);
+        P.kv.reset(d.L_nnz);
+        SDL_CUDA(cudaMemsetAsync(cnt.get(), 0, cnt.bytes(), s));
+        SDL_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(int), s));
+        SDL_LAUNCH(k_value_rows, grid_for(d.L_nnz, 256, rt.num_sms * 8), 256, 0, s, d.L_map, d.Li, d.L_nnz,
+                   P.kv.get(), cnt.get(), bad.get());
+        int hbad = 1;
+        SDL_CUDA(cudaMemcpyAsync(&hbad, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaStreamSynchronize(s));
+        if (hbad)
+            P.kv.release();
+        else
+            value_order = 1;
+    }
+    DevBuf<long long> tile_nterms(nt), tile_nx(nt), word_begin((size_t)nt + 1), x_begin((size_t)nt + 1);
     NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, nullptr, nullptr, d.Ap, d.Ai, nullptr,
-               P.Cp.get(), P.Ci.get(), nullptr, rt.d_error, d.L_nnz};
+               P.Cp.get(), P.Ci.get(), nullptr, rt.d_error, d.L_nnz, value_order};
     set_smem(k_tile_schedule<false>, build_smem_bytes());
     set_smem(k_tile_schedule<true>, build_smem_bytes());
     SDL_LAUNCH(k_tile_schedule<false>, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
-               tile_start.get(), tile_nwords.get(), tile_nx.get(), nullptr, nullptr, nullptr, nullptr,
-               nullptr);
-    const long long word_total = exclusive_scan_i64(tile_nwords.get(), word_begin.get(), P.ntiles, s);
+               tile_start.get(), tile_nterms.get(), tile_nx.get(), nullptr, nullptr, nullptr, nullptr,
+               nullptr, nullptr);
+    const long long word_total = exclusive_scan_i64(tile_nterms.get(), word_begin.get(), P.ntiles, s);
     const long long x_total = exclusive_scan_i64(tile_nx.get(), x_begin.get(), P.ntiles, s);
-    if (x_total >= (long long)UINT32_MAX) fail(SDL_ERR_OVERFLOW, "product: term lists exceed 32-bit offsets");
-    if (word_total > INT_MAX) fail(SDL_ERR_OVERFLOW, "product: output words exceed 31-bit offsets");
+    if (word_total > INT_MAX || x_total > INT_MAX)
+        fail(SDL_ERR_OVERFLOW, "product: the tile rows' terms exceed the schedule's 31-bit offsets");
     P.tiles.reset(nt);
     P.W.reset(std::max<long long>(1, word_total));
     P.X.reset(std::max<long long>(1, x_total));
     P.V.reset(std::max<long long>(1, nV));
+    P.ES.reset(std::max<long long>(1, nV));
     SDL_LAUNCH(k_tile_schedule<true>, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
                tile_start.get(), nullptr, nullptr, word_begin.get(), x_begin.get(), P.tiles.get(),
-               P.W.get(), P.X.get());
+               P.W.get(), P.X.get(), P.ES.get());
     if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
     if (P.num_count[NUM_GMEM])
     {
@@ -1511,10 +1612,11 @@ ProdSched sched_of(const Product &P)
     S.W = P.W.get();
     S.X = P.X.get();
     S.V = P.V.get();
+    S.ES = P.ES.get();
+    S.kv = P.kv.get();
     S.Li = d.Li;
     S.L_map = d.L_map;
     S.nV = (long long)d.L_nnz * d.blocks;
-    S.nX = (long long)P.X.n;
     S.nA = d.A_nnz;
     S.L_nnz = d.L_nnz;
     S.n_L = P.n_L;
@@ -1551,27 +1653,32 @@ void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const 
                  cudaStream_t s, ProdPtrs vals, ProdSched sched)
 {
     if (ntiles <= 0) return;
-    static int per_sm[2] = {0, 0}; // resident CTAs per SM (set once, outside any capture)
+    // kernel attributes and resident CTAs per SM, set once (outside any capture)
+    static int per_sm[2] = {0, 0};
     const int b = ptrs ? 1 : 0;
     if (!per_sm[b])
     {
         if (b)
+        {
+            set_smem(k_tile_refill<true>, refill_smem_bytes());
             SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[b], k_tile_refill<true>,
-                                                                   REFILL_THREADS, 0));
+                                                                   REFILL_THREADS, refill_smem_bytes()));
+        }
         else
+        {
+            set_smem(k_tile_refill<false>, refill_smem_bytes());
             SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[b], k_tile_refill<false>,
-                                                                   REFILL_THREADS, 0));
+                                                                   REFILL_THREADS, refill_smem_bytes()));
+        }
         per_sm[b] = std::max(1, per_sm[b]);
     }
-    // a single product: persistent CTAs with word prefetch; a batch (many small
-    // tiles of uneven size): one CTA per tile, the hardware scheduler balances them
-    const int grid = b ? ntiles : std::min(ntiles, runtime().num_sms * per_sm[b]);
+    const int grid = std::min(ntiles, runtime().num_sms * per_sm[b]);
     if (b)
-        SDL_LAUNCH(k_tile_refill<true>, grid, REFILL_THREADS, 0, s, tiles, ntiles, ptrs, scheds, vals, sched,
-                   runtime().d_error);
+        SDL_LAUNCH(k_tile_refill<true>, grid, REFILL_THREADS, refill_smem_bytes(), s, tiles, ntiles, ptrs,
+                   scheds, vals, sched, runtime().d_error);
     else
-        SDL_LAUNCH(k_tile_refill<false>, grid, REFILL_THREADS, 0, s, tiles, ntiles, ptrs, scheds, vals, sched,
-                   runtime().d_error);
+        SDL_LAUNCH(k_tile_refill<false>, grid, REFILL_THREADS, refill_smem_bytes(), s, tiles, ntiles, ptrs,
+                   scheds, vals, sched, runtime().d_error);
 }
 
 void big_rows_refill(const Product &P, const double *Lx, const double *dvec, const double *Ax,

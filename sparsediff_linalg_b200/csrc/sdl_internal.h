@@ -180,21 +180,28 @@ enum
 constexpr int TILE_T = SDL_TILE_T;
 constexpr int TILE_THREADS = 256;
 
-// Compiled refill schedule of the tile rows (built once per pattern), output-major:
-// every output of a tile row has one 8-byte word,
-//   {jj, e}                      its only term is V[e] * A.x[jj];
-//   {start, MULTI_BIT | count}   it collects count >= 2 terms, the {jj, e} pairs
-//                                X[start .. start + count - 1], in upstream's
-//                                visiting order;
-// where V[e] = L.x * d[k] of entry e = b * L_nnz + ii of kron(I_blocks, L), computed
-// once per refill (entry-value kernel).
-constexpr unsigned MULTI_BIT = 0x80000000u;
-struct __align__(16) TileDesc
+// Compiled refill schedule of the tile rows (built once per pattern), entry-major:
+// the terms of a tile in upstream's visiting order (the tile's L entries in order,
+// each entry's A row in order), one 32-bit word per term:
+//   bits 0..11   p, the term's output inside the tile window;
+//   bits 12..13  kind: TERM_ONE (the output's only term), TERM_PAIR (one of exactly
+//                two), TERM_LIST (one of three or more: summed by the list pass);
+//   bits 14..31  e, the term's entry among the tile's L entries.
+// With ES[vbase + e] = {bq, slot}, term u of a tile is V[slot] * A.x[bq + u]: V holds
+// the entry values L.x * d[k] of one refill (entry-value kernel), bq = A.p[k] minus
+// the offset of the entry's first term in its tile. A tile's entries are the
+// consecutive entries vbase, vbase + 1, ... (b * L_nnz + ii) of its rows.
+constexpr unsigned TERM_ONE = 0u, TERM_PAIR = 1u, TERM_LIST = 2u;
+struct TileDesc
 {
-    int word_begin; // first output word of the tile
-    int out_begin;  // first output of the tile in C.x
-    int nout;       // outputs of the tile (one word each)
-    int prod;       // product index (batched refills), 0 for a single product
+    int vbase;       // ES index of the tile's first entry
+    int word_begin;  // first term word of the tile
+    int nterms;      // terms of the tile
+    int out_begin;   // first output of the tile in C.x
+    int nout;        // outputs of the tile (the window)
+    int x_begin;     // list section: nlist + 1 headers (p | start << 12), then term indices
+    int nlist;       // outputs with three or more terms
+    int prod;        // product index (batched refills), 0 for a single product
 };
 // Value arrays of one refill of one product.
 struct ProdPtrs
@@ -205,11 +212,13 @@ struct ProdPtrs
 // Refill schedule of one product as the kernels read it.
 struct ProdSched
 {
-    const uint2 *W; // output words of the tile rows
-    const uint2 *X; // term lists of multi-term outputs
-    double *V;      // entry values (refill scratch, nV)
+    const unsigned *W; // term words of the tile rows
+    const unsigned *X; // list sections
+    double *V;         // entry values (refill scratch, nV)
+    const int2 *ES;    // per entry: {A.p[k] - tile term offset, slot of its value in V}
     const int *Li, *L_map;
-    long long nV, nX, nA; // entries of kron(I_blocks, L), list pairs, entries of A
+    const int *kv;     // V in L's value order: row of A of each value (else null)
+    long long nV, nA; // entries of kron(I_blocks, L), entries of A
     int L_nnz, n_L, blocks, pad;
 };
 // A run of one product's entries (batched entry values).
@@ -257,8 +266,10 @@ struct Product
     // Compiled refill schedule of the tile rows.
     int ntiles = 0;
     DevBuf<TileDesc> tiles;
-    DevBuf<uint2> W, X;   // output words, term lists
-    DevBuf<double> V;     // entry values of the current refill (L_nnz * blocks)
+    DevBuf<unsigned> W, X; // term words, list sections
+    DevBuf<int2> ES;       // per entry: {A.p[k] - tile term offset, V slot} (L_nnz * blocks)
+    DevBuf<int> kv;        // V in L's value order (L_map a permutation): row of A per value
+    DevBuf<double> V;      // entry values of the current refill (L_nnz * blocks)
     DevBuf<int> gmem_scratch; // posmap scratch for NUM_GMEM rows (slots x n ints)
     int gmem_slots = 0;
     TuneConfig cfg;
