@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-conversions", action="store_true")
+    ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--learned-matrices", type=int, default=200)
     return ap.parse_args()
 
@@ -181,6 +183,20 @@ def reference_spgemm_times(A, B, reps):
                       c(keep[3], C.c_int), c(keep[4], C.c_int), c(keep[5], C.c_double), B[4], reps,
                       out.ctypes.data_as(C.POINTER(C.c_double)))
     return out
+
+
+def reference_csr_to_csc_times(A, reps):
+    from oracle import oracle
+    L = C.CDLL(str(oracle.REF_DIR / "libsdl_reftime.so"))
+    ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+    L.ref_time_csr_to_csc.argtypes = [ip, ip, dp, C.c_int, C.c_int, C.c_int, dp]
+    L.ref_time_csr_to_csc.restype = None
+    keep = [np.ascontiguousarray(a) for a in (A[0], A[1], A[2])]
+    c = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    out = np.zeros(3)
+    L.ref_time_csr_to_csc(c(keep[0], C.c_int), c(keep[1], C.c_int), c(keep[2], C.c_double), A[3], A[4],
+                          reps, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out  # alloc s, fill s, nnz
 
 
 def workload():
@@ -317,6 +333,12 @@ def run_b200(args, world, rank, local):
     learned = None
     if not args.no_learned:
         learned = run_learned(args, dev)
+    conversions = None
+    if not args.no_conversions and world == 1:
+        conversions = run_conversions(args, dev, peaks()[0])
+    dense = None
+    if not args.no_dense and world == 1:
+        dense = run_dense(args, dev, peaks()[0])
 
     # ---- e2e through the upstream C ABI with host buffers
     e2e = None
@@ -348,6 +370,10 @@ def run_b200(args, world, rank, local):
         line["batched_512"] = batched
     if learned is not None:
         line["learned_skewed"] = learned
+    if conversions is not None:
+        line.update(conversions)
+    if dense is not None:
+        line["stacked_pd_x_csc"] = dense
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg)
     if rank == 0:
@@ -464,6 +490,173 @@ def run_batched(args, dev, refills=20):
             "plain_gbs": round(B_alg / (ms_plain * 1e-3) / 1e9, 2),
             "speedup_vs_plain": round(ms_plain / ms_batched, 3),
             "generate_s": round(gen_s, 2), "symbolic_s": round(sym_s, 2)}
+
+
+def _event_ms(fn, stream, steps, flush=None):
+    """Mean device ms of fn(stream) over `steps` runs (CUDA events on `stream`), with
+    an L2 flush (256 MiB write) before each run when `flush` is given."""
+    import torch
+    evs = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(stream)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs) / steps
+
+
+def run_conversions(args, dev, peak):
+    """CSR -> CSC of a 1M x 1M matrix with 10 distinct uniform columns per row, and
+    coalescing of 50M COO triplets over 1M x 1M (35M distinct pairs plus 15M repeats,
+    shuffled) into CSR with duplicates summed in input order. Structure (once per
+    pattern) and value refill are timed separately; the refill is the recurring cost.
+    Algorithmic bytes (int32 = 4 B, FP64 = 8 B): conversion 24 nnz + 4 (m + 1) +
+    4 (n + 1); its value refill 20 nnz (x read, CSC values written, position map
+    read); coalescing 16 N_in + 12 nnz_out + 4 (m + 1); its value refill 12 N_in +
+    8 nnz_out."""
+    import torch
+    from sparsediff_linalg_b200 import workloads as wl
+    from sparsediff_linalg_b200.device import Coalesce, Transpose
+    s = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    out = {}
+    # ---- 4b: CSR -> CSC
+    A = wl.transpose_big(seed=4)
+    m, n, nnz = A[3], A[4], len(A[1])
+    Ap = torch.as_tensor(A[0], device=dev)
+    Ai = torch.as_tensor(A[1], device=dev)
+    Ax = torch.as_tensor(A[2], device=dev)
+    Tx = torch.empty(nnz, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    T = Transpose(Ap, Ai, m, n, stream=s)
+    T.fill(Ax, Tx, stream=s)
+    torch.cuda.synchronize()
+    struct_ms = (time.perf_counter() - t0) * 1e3
+    for _ in range(3):
+        T.fill(Ax, Tx, stream=s)
+    fill_ms = _event_ms(lambda st: T.fill(Ax, Tx, stream=st), s, args.steps, flush)
+    b_fill = 20 * nnz
+    b_full = 24 * nnz + 4 * (m + 1) + 4 * (n + 1)
+    out["csr_to_csc_1M"] = {
+        "workload": "CSR -> CSC, 1M x 1M, 10 distinct uniform columns per row, FP64",
+        "nnz": nnz, "structure_ms": round(struct_ms, 3), "fill_us": round(fill_ms * 1e3, 2),
+        "fill_gbs": round(b_fill / (fill_ms * 1e-3) / 1e9, 1),
+        "fill_frac_of_hbm": round(b_fill / (fill_ms * 1e-3) / 1e9 / peak, 4),
+        "conversion_ms": round(struct_ms, 3),
+        "conversion_gbs": round(b_full / (struct_ms * 1e-3) / 1e9, 1),
+        "algorithmic_bytes_fill": b_fill, "algorithmic_bytes_conversion": b_full}
+    if not args.no_cpu_baseline:
+        try:
+            r = reference_csr_to_csc_times(A, 3)
+            out["csr_to_csc_1M"]["upstream_cpu"] = {"alloc_ms": round(r[0] * 1e3, 1),
+                                                    "fill_ms": round(r[1] * 1e3, 2), "cores": 1}
+        except Exception as e:  # noqa: BLE001
+            out["csr_to_csc_1M"]["upstream_cpu"] = {"unavailable": str(e)[:200]}
+    del T, Ap, Ai, Ax, Tx, A
+    torch.cuda.empty_cache()
+    # ---- 4c: COO coalescing
+    rows, cols, x, m, n = wl.coalesce_big(seed=5)
+    N = len(rows)
+    R = torch.as_tensor(rows, device=dev)
+    Cc = torch.as_tensor(cols, device=dev)
+    X = torch.as_tensor(x, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    CO = Coalesce(R, Cc, m, n, stream=s)
+    Cx = torch.empty(max(1, CO.nnz), dtype=torch.float64, device=dev)
+    CO.fill(X, Cx, stream=s)
+    torch.cuda.synchronize()
+    struct_ms = (time.perf_counter() - t0) * 1e3
+    for _ in range(3):
+        CO.fill(X, Cx, stream=s)
+    fill_ms = _event_ms(lambda st: CO.fill(X, Cx, stream=st), s, args.steps, flush)
+    b_fill = 12 * N + 8 * CO.nnz
+    b_full = 16 * N + 12 * CO.nnz + 4 * (m + 1)
+    out["coo_coalesce_50M"] = {
+        "workload": "COO -> CSR with duplicates summed, 50M triplets (35M distinct pairs + 15M "
+                    "repeats, shuffled) over 1M x 1M, FP64",
+        "triplets": N, "nnz_out": CO.nnz, "structure_ms": round(struct_ms, 3),
+        "fill_us": round(fill_ms * 1e3, 2), "fill_gbs": round(b_fill / (fill_ms * 1e-3) / 1e9, 1),
+        "fill_frac_of_hbm": round(b_fill / (fill_ms * 1e-3) / 1e9 / peak, 4),
+        "coalesce_gbs": round(b_full / ((struct_ms) * 1e-3) / 1e9, 1),
+        "algorithmic_bytes_fill": b_fill, "algorithmic_bytes_coalesce": b_full}
+    del CO, R, Cc, X, Cx
+    torch.cuda.empty_cache()
+    return out
+
+
+def reference_ba_spd_csr_times(m, blocks_rows, cperm, X, S, reps):
+    from oracle import oracle
+    L = C.CDLL(str(oracle.REF_DIR / "libsdl_reftime.so"))
+    ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+    L.ref_time_ba_spd_csr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, ip, ip, dp, C.c_int,
+                                      C.c_int, C.c_int, dp]
+    L.ref_time_ba_spd_csr.restype = None
+    nb, m0, n0 = X.shape
+    keep = [np.ascontiguousarray(a) for a in (blocks_rows, cperm, X, S[0], S[1], S[2])]
+    c = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    out = np.zeros(2)
+    L.ref_time_ba_spd_csr(m, nb, m0, n0, c(keep[0], C.c_int), c(keep[1], C.c_int), c(keep[2], C.c_double),
+                          c(keep[3], C.c_int), c(keep[4], C.c_int), c(keep[5], C.c_double), S[3], S[4], reps,
+                          out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def run_dense(args, dev, peak):
+    """stacked_pd x CSC: 64 permuted-dense blocks of 64 x 256 (N(0,1)) whose 4096
+    rows are a random permutation, col_perm 0..255, times S 256 x 100000 with 6
+    distinct uniform rows per column (upstream BA_spd_csr_*): 64 output blocks of
+    64 x 100000, 3.28 GB of FP64 -- bound by writing C. Algorithmic bytes:
+    8 sum(m0 n0) + 12 nnz(S) + 4 (n_S + 1) + 8 nnz(C) + 4 sum(n0_C)."""
+    import torch
+    from oracle import oracle
+    from sparsediff_linalg_b200 import workloads as wl
+    from sparsediff_linalg_b200.device import BlocksCsr
+    rng = np.random.default_rng(6)
+    nb, m0, n0, S_n = 64, 64, 256, 100_000
+    rows = rng.permutation(nb * m0).astype(np.int32)
+    blocks_rows = np.concatenate([np.sort(rows[k * m0:(k + 1) * m0]) for k in range(nb)]).astype(np.int32)
+    cperm = np.arange(n0, dtype=np.int32)
+    X = rng.standard_normal((nb, m0, n0))
+    St = wl.fixed_rowlen_csr(S_n, n0, 6, rng)  # S's columns as rows of S^T
+    Sp, Si, Sx = oracle.transpose(St[0], St[1], St[2], S_n, n0)
+    S = (Sp, Si, Sx, n0, S_n)
+    t0 = time.perf_counter()
+    P = BlocksCsr([m0] * nb, [n0] * nb, [cperm] * nb, Sp, Si, n0, S_n)
+    alloc_ms = (time.perf_counter() - t0) * 1e3
+    Bv = torch.as_tensor(X.ravel(), device=dev)
+    Sx_d = torch.as_tensor(Sx, device=dev)
+    Cv = torch.empty(P.c_values, dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        P.fill(Bv, Sx_d, Cv, stream=s)
+    steps = max(3, min(args.steps, 10))
+    ms = _event_ms(lambda st: P.fill(Bv, Sx_d, Cv, stream=st), s, steps, flush)
+    nnzC = P.c_values
+    sum_n0C = sum(b[2] for b in P.blocks)
+    B_alg = 8 * nb * m0 * n0 + 12 * len(Si) + 4 * (S_n + 1) + 8 * nnzC + 4 * sum_n0C
+    out = {"workload": "stacked_pd (64 blocks of 64 x 256, rows permuted) x CSC 256 x 100000 with 6 "
+                       "entries per column, FP64", "out_blocks": P.out_blocks, "nnz_C": int(nnzC),
+           "alloc_ms": round(alloc_ms, 2), "fill_ms": round(ms, 4),
+           "fill_gbs": round(B_alg / (ms * 1e-3) / 1e9, 1),
+           "fill_frac_of_hbm": round(B_alg / (ms * 1e-3) / 1e9 / peak, 4), "algorithmic_bytes": int(B_alg),
+           "l2": "flushed before each timed fill (256 MiB write); C (3.28 GB) exceeds L2"}
+    if not args.no_cpu_baseline:
+        try:
+            r = reference_ba_spd_csr_times(nb * m0, blocks_rows, cperm, X, S, 1)
+            out["upstream_cpu"] = {"alloc_ms": round(r[0] * 1e3, 1), "fill_ms": round(r[1] * 1e3, 1),
+                                   "cores": 1}
+        except Exception as e:  # noqa: BLE001
+            out["upstream_cpu"] = {"unavailable": str(e)[:200]}
+    del P, Bv, Sx_d, Cv
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_learned(args, dev):

@@ -219,6 +219,36 @@ sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, double *Cx,
                              void *stream);
 void sdl_coalesce_destroy(sdl_coalesce *C);
 
+/* ------------------------------------------------------------------------
+   Dense blocks times a sparse CSR, device-resident: C_k = B_k S[col_perm_k, :]
+   for source blocks B_k of shape m0[k] x n0[k] whose columns are the rows
+   col_perm[k] (strictly increasing) of S (S_m x S_n). Replaces upstream's
+   BA_spd_csr_alloc / BA_spd_csr_fill_values (src/stacked_pd/stacked_pd_linalg.c:
+   657-671) and, with one block, BA_pd_csr_alloc / BA_pd_csr_fill_values
+   (src/permuted_dense/permuted_dense_linalg.c:313-430). Output block k has
+   upstream's shape: B's rows times the columns of S that its rows reach
+   (ascending); with keep_empty = 0, blocks without such columns are dropped, as
+   upstream's stacked_pd product does. The structure (Sp, Si, col_perm) is read
+   from host memory at create; the fill reads device values: B_vals holds the
+   source blocks in order, each m0 x n0 row-major (a stacked_pd's value buffer),
+   C_vals receives the output blocks in order, each m0 x n0_C row-major. Every
+   output is summed in upstream's order, bit for bit.
+   ------------------------------------------------------------------------ */
+typedef struct sdl_blocks_csr sdl_blocks_csr;
+sdl_status sdl_blocks_csr_create(int n_blocks, const int *m0, const int *n0,
+                                 const int *const *col_perm, const int *Sp, const int *Si,
+                                 int S_m, int S_n, int keep_empty, void *stream,
+                                 sdl_blocks_csr **out);
+/* Number of output blocks, and the lengths of the C and B value arrays. */
+sdl_status sdl_blocks_csr_info(const sdl_blocks_csr *P, int *out_blocks, long long *c_values,
+                               long long *b_values);
+/* Output block k: its source block, rows, columns and (host) column indices. */
+sdl_status sdl_blocks_csr_block(const sdl_blocks_csr *P, int k, int *src_block, int *m0,
+                                int *n0_C, const int **col_perm);
+sdl_status sdl_blocks_csr_fill(const sdl_blocks_csr *P, const double *B_vals,
+                               const double *S_x, double *C_vals, void *stream);
+void sdl_blocks_csr_destroy(sdl_blocks_csr *P);
+
 /* Host-pointer form for COO_matrix users (no upstream counterpart): the
    coalesced CSR of A (m x n), and a refill of its values from A->x. */
 CSR_matrix *COO_coalesce_alloc(const COO_matrix *A);

@@ -103,6 +103,11 @@ def reference():
             "BA_matrices_fill_values": (None, [matrix_p, matrix_p, matrix_p]),
             "ATA_matrices_alloc": (matrix_p, [matrix_p]),
             "ATDA_matrices_fill_values": (None, [matrix_p, vp, matrix_p]),
+            "new_permuted_dense": (matrix_p, [C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+            "new_stacked_pd": (matrix_p, [C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+            # internal upstream entry points (src/internal/stacked_pd_linalg.h)
+            "BA_spd_csr_alloc": (matrix_p, [matrix_p, CSR_p]),
+            "BA_spd_csr_fill_values": (None, [matrix_p, CSR_p, matrix_p]),
         }
         bind(L, extra)
         _REF = L
@@ -211,3 +216,35 @@ def spgemm(A, B):
     Ap, Ai, Ax, mA, nA = A
     Bp, Bi, Bx, mB, nB = B
     return gustavson(Ap, Ai, Ax, mA, 1, None, Bp, Bi, Bx, mB, nB)
+
+
+def blocks_csr(blocks, Sp, Si, Sx, S_n):
+    """C_k = B_k S[col_perm_k, :] for dense blocks [(X_k (m0 x n0), col_perm_k)], as
+    upstream's BA_pd_csr_alloc / BA_pd_csr_fill_values
+    (src/permuted_dense/permuted_dense_linalg.c:313-430): output columns are the
+    union of the patterns of S's rows col_perm_k, ascending; every output is summed
+    over the compact CSC of S[col_perm_k, :] in its order (row r of the block
+    ascending), from +0.0, one rounding per product and per sum. Returns
+    [(col_perm_C, C_k)] per block (numpy, float64). Test infrastructure only."""
+    out = []
+    for X, cperm in blocks:
+        X = np.asarray(X, np.float64)
+        ents = []  # (column of S, local row r, value) in upstream's order
+        for r, row in enumerate(cperm):
+            for q in range(Sp[row], Sp[row + 1]):
+                ents.append((int(Si[q]), r, float(Sx[q])))
+        cols = sorted({c for c, _, _ in ents})
+        loc = {c: k for k, c in enumerate(cols)}
+        per = [[] for _ in cols]
+        for c, r, v in ents:  # r ascending, then q: upstream's compact order
+            per[loc[c]].append((r, v))
+        C = np.zeros((X.shape[0], len(cols)))
+        if cols:
+            depth = max(len(e) for e in per)
+            for t in range(depth):  # one term of every column at a time: sequential sums
+                idx = [k for k in range(len(cols)) if len(per[k]) > t]
+                rr = np.array([per[k][t][0] for k in idx])
+                vv = np.array([per[k][t][1] for k in idx])
+                C[:, idx] = C[:, idx] + X[:, rr] * vv[None, :]
+        out.append((np.array(cols, np.int32), C))
+    return out

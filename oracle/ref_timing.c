@@ -115,3 +115,56 @@ void ref_time_spgemm(const int *Ap, const int *Ai, const double *Ax, int mA, int
     free_matrix(Am);
     free_matrix(Bm);
 }
+
+/* CSR -> CSC conversion through upstream's raw kernels (the CSC mirror refresh of
+ * SparseDiffEngine). out[0] = alloc seconds (structure), out[1] = seconds per
+ * value refill, out[2] = nnz. */
+void ref_time_csr_to_csc(const int *Ap, const int *Ai, const double *Ax, int m, int n, int reps,
+                         double *out)
+{
+    mat_t *A = copy_csr(Ap, Ai, Ax, m, n);
+    int *iwork = (int *)malloc((size_t)(n > 0 ? n : 1) * sizeof(int));
+    double t0 = now();
+    mat_t *C = csr_to_csc_alloc(A, iwork);
+    out[0] = now() - t0;
+    t0 = now();
+    for (int r = 0; r < reps; ++r) csr_to_csc_fill_values(A, C, iwork);
+    out[1] = (now() - t0) / (reps > 0 ? reps : 1);
+    out[2] = Ap[m];
+    free(iwork);
+    free_CSC_matrix(C);
+    free_CSR_matrix(A);
+}
+
+/* stacked_pd x CSR through upstream's BA_spd_csr_alloc / BA_spd_csr_fill_values
+ * (src/stacked_pd/stacked_pd_linalg.c:657-671): n_blocks dense blocks of m0 x n0
+ * with row_perm rows[k * m0 ...] of an m-row stacked_pd and col_perm cperm (shared),
+ * values X (block-major). out[0] = alloc seconds, out[1] = seconds per fill. */
+extern matrix *new_permuted_dense(int m, int n, int m0, int n0, const int *row_perm,
+                                  const int *col_perm, const double *X);
+extern matrix *new_stacked_pd(int m, int n, int n_blocks, matrix **blocks,
+                              const int *src_block_idx_p, const int *src_block_idx);
+extern matrix *BA_spd_csr_alloc(const matrix *B, const mat_t *S);
+extern void BA_spd_csr_fill_values(const matrix *B, const mat_t *S, matrix *C);
+
+void ref_time_ba_spd_csr(int m, int n_blocks, int m0, int n0, const int *rows, const int *cperm,
+                         const double *X, const int *Sp, const int *Si, const double *Sx, int S_m,
+                         int S_n, int reps, double *out)
+{
+    matrix **blocks = (matrix **)malloc((size_t)n_blocks * sizeof(matrix *));
+    for (int k = 0; k < n_blocks; ++k)
+        blocks[k] = new_permuted_dense(m, S_m, m0, n0, rows + (size_t)k * m0, cperm,
+                                       X + (size_t)k * m0 * n0);
+    matrix *B = new_stacked_pd(m, S_m, n_blocks, blocks, NULL, NULL);
+    free(blocks);
+    mat_t *S = copy_csr(Sp, Si, Sx, S_m, S_n);
+    double t0 = now();
+    matrix *C = BA_spd_csr_alloc(B, S);
+    out[0] = now() - t0;
+    t0 = now();
+    for (int r = 0; r < reps; ++r) BA_spd_csr_fill_values(B, S, C);
+    out[1] = (now() - t0) / (reps > 0 ? reps : 1);
+    free_matrix(C);
+    free_matrix(B);
+    free_CSR_matrix(S);
+}

@@ -5,15 +5,21 @@
 #include <cstring>
 
 #include "capi_common.h"
+#include "dense_plan.h"
 #include "matrix_kinds.h"
 #include "sparsediff_linalg/matrix.h"
 #include "sparsediff_linalg/tracked_alloc.h"
 
 namespace sdl {
 
+// Device state bound to a permuted_dense produced by BA_matrices_alloc (B pd,
+// A sparse): the product plan and the device copies of B's and C's values.
 struct PdImpl
 {
+    std::unique_ptr<BlocksCsrPlan> ba;
+    DevBuf<double> bvals, cvals;
 };
+const double *sparse_dev_values(sdl_sparse *A, cudaStream_t s);
 struct SpdImpl
 {
 };
@@ -165,8 +171,50 @@ matrix *spd_copy_sparsity(const sdl_stacked *A)
 
 matrix *dense_BTA_alloc(matrix *, matrix *) { unsupported("BTA_matrices_alloc"); }
 void dense_BTDA_fill(matrix *, const double *, matrix *, matrix *) { unsupported("BTDA_matrices_fill_values"); }
-matrix *dense_BA_alloc(const matrix *, matrix *) { unsupported("BA_matrices_alloc"); }
-void dense_BA_fill(const matrix *, const matrix *, matrix *) { unsupported("BA_matrices_fill_values"); }
+// BA with B permuted_dense and A sparse (upstream matmul_dispatchers.c:197-223 ->
+// permuted_dense_linalg.c:313-430 BA_pd_csr_*): C is permuted_dense with B's
+// row_perm and the columns of S = A's CSR that B's col_perm rows reach.
+matrix *dense_BA_alloc(const matrix *Bm, matrix *Am)
+{
+    if (Bm->kind != MATRIX_PERMUTED_DENSE || Am->kind != MATRIX_SPARSE) unsupported("BA_matrices_alloc");
+    const permuted_dense *B = as_pd(Bm);
+    sdl_sparse *A = as_sparse(Am);
+    cudaStream_t s = runtime().stream;
+    const int *cperm = B->col_perm;
+    auto plan = blocks_csr_build(1, &B->m0, &B->n0, &cperm, A->csr->p, A->csr->i, A->csr->m, A->csr->n,
+                                 true, s);
+    const std::vector<int> &cpC = plan->col_perm[0];
+    matrix *Cm = new_permuted_dense(B->base.m, A->csr->n, B->m0, (int)cpC.size(), B->row_perm,
+                                    cpC.empty() ? nullptr : cpC.data(), nullptr);
+    if (!Cm) fail(SDL_ERR_INTERNAL, "BA_matrices_alloc: output allocation failed");
+    permuted_dense *C = as_pd(Cm);
+    C->impl->bvals.reset((size_t)std::max<long long>(1, plan->b_total));
+    C->impl->cvals.reset((size_t)std::max<long long>(1, plan->c_total));
+    C->impl->ba = std::move(plan);
+    sparse_dev_values(A, s); // the device mirror of A's values exists before any fill
+    SDL_CUDA(cudaStreamSynchronize(s));
+    return Cm;
+}
+
+void dense_BA_fill(const matrix *Bm, const matrix *Am, matrix *Cm)
+{
+    if (Bm->kind != MATRIX_PERMUTED_DENSE || Am->kind != MATRIX_SPARSE || Cm->kind != MATRIX_PERMUTED_DENSE)
+        unsupported("BA_matrices_fill_values");
+    const permuted_dense *B = as_pd(Bm);
+    permuted_dense *C = as_pd(Cm);
+    PdImpl *im = C->impl;
+    if (!im || !im->ba) fail(SDL_ERR_INVALID, "BA_matrices_fill_values: C was not produced by BA_matrices_alloc");
+    const BlocksCsrPlan &P = *im->ba;
+    if (P.b_total != (long long)B->m0 * B->n0 || P.S_nnz != as_sparse(Am)->csr->nnz)
+        fail(SDL_ERR_INVALID, "BA_matrices_fill_values: operands do not match the alloc");
+    cudaStream_t s = runtime().stream;
+    h2d(im->bvals.get(), B->X, (size_t)P.b_total, s);
+    const double *Sx = sparse_dev_values(as_sparse(Am), s);
+    blocks_csr_fill(P, im->bvals.get(), Sx, im->cvals.get(), s);
+    d2h(C->X, im->cvals.get(), (size_t)P.c_total, s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    matrix_values_changed(Cm);
+}
 matrix *dense_ATA_alloc(matrix *) { unsupported("ATA_matrices_alloc"); }
 void dense_ATDA_fill(const matrix *, const double *, matrix *) { unsupported("ATDA_matrices_fill_values"); }
 void dense_DA_fill(const double *, const matrix *, matrix *) { unsupported("DA_matrices_fill_values"); }
@@ -280,3 +328,60 @@ extern "C" matrix *new_stacked_pd(int m, int n, int n_blocks, permuted_dense **b
         return &spd->base;
     });
 }
+
+// ------------------------------------------------------------------ device API
+struct sdl_blocks_csr
+{
+    std::unique_ptr<sdl::BlocksCsrPlan> P;
+};
+
+extern "C" sdl_status sdl_blocks_csr_create(int n_blocks, const int *m0, const int *n0,
+                                            const int *const *col_perm, const int *Sp, const int *Si,
+                                            int S_m, int S_n, int keep_empty, void *stream,
+                                            sdl_blocks_csr **out)
+{
+    return guard_status("sdl_blocks_csr_create", [&]() {
+        if (!out || (n_blocks > 0 && (!m0 || !n0 || !col_perm)) || (S_m > 0 && (!Sp || !Si)))
+            fail(SDL_ERR_INVALID, "NULL argument");
+        *out = nullptr;
+        auto h = std::make_unique<sdl_blocks_csr>();
+        h->P = blocks_csr_build(n_blocks, m0, n0, col_perm, Sp, Si, S_m, S_n, keep_empty != 0,
+                                pick_stream(stream));
+        *out = h.release();
+    });
+}
+
+extern "C" sdl_status sdl_blocks_csr_info(const sdl_blocks_csr *P, int *out_blocks, long long *c_values,
+                                          long long *b_values)
+{
+    return guard_status("sdl_blocks_csr_info", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL plan");
+        if (out_blocks) *out_blocks = (int)P->P->src.size();
+        if (c_values) *c_values = P->P->c_total;
+        if (b_values) *b_values = P->P->b_total;
+    });
+}
+
+extern "C" sdl_status sdl_blocks_csr_block(const sdl_blocks_csr *P, int k, int *src_block, int *m0,
+                                           int *n0_C, const int **col_perm)
+{
+    return guard_status("sdl_blocks_csr_block", [&]() {
+        if (!P || k < 0 || k >= (int)P->P->src.size()) fail(SDL_ERR_INVALID, "bad output block");
+        if (src_block) *src_block = P->P->src[k];
+        if (m0) *m0 = P->P->m0[k];
+        if (n0_C) *n0_C = P->P->n0_C[k];
+        if (col_perm) *col_perm = P->P->col_perm[k].data();
+    });
+}
+
+extern "C" sdl_status sdl_blocks_csr_fill(const sdl_blocks_csr *P, const double *B_vals, const double *S_x,
+                                          double *C_vals, void *stream)
+{
+    return guard_status("sdl_blocks_csr_fill", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL plan");
+        if (P->P->c_total > 0 && (!B_vals || !S_x || !C_vals)) fail(SDL_ERR_INVALID, "NULL value pointer");
+        blocks_csr_fill(*P->P, B_vals, S_x, C_vals, pick_stream(stream));
+    });
+}
+
+extern "C" void sdl_blocks_csr_destroy(sdl_blocks_csr *P) { delete P; }

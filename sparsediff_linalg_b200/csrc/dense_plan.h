@@ -1,0 +1,63 @@
+// Products of dense blocks (permuted_dense / the blocks of a stacked_pd) with a
+// sparse CSR: C_k = B_k S[col_perm_k, :] for every block k (upstream
+// src/permuted_dense/permuted_dense_linalg.c:313-430 BA_pd_csr_*,
+// src/stacked_pd/stacked_pd_linalg.c:657-671 BA_spd_csr_*).
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "sdl_internal.h"
+
+namespace sdl {
+
+// Device descriptor of one output block.
+struct BlkDesc
+{
+    long long b_off; // first value of the source block in the B value array
+    long long c_off; // first value of the output block in the C value array
+    long long cp_off; // column offsets of its compact CSC (n0_C + 1)
+    long long d_off;  // its compact CSC entries (rows, vals)
+    int m0, n0_B, n0_C, pad;
+};
+
+// One CTA's share: columns [c0, c0 + 32) of output block `blk`.
+struct BlkTile
+{
+    int blk, c0;
+};
+
+struct BlocksCsrPlan
+{
+    int S_m = 0, S_n = 0, S_nnz = 0;
+    int n_src = 0;
+    // output blocks: the source blocks whose product has at least one column
+    // (upstream spd_map_filter_blocks drops the empty ones)
+    std::vector<int> src;                   // source block of each output block
+    std::vector<std::vector<int>> col_perm; // col_perm of each output block (host)
+    std::vector<int> m0, n0_C;
+    long long c_total = 0, b_total = 0, d_total = 0;
+    // compact CSC of S restricted to a block's col_perm rows, shared by blocks whose
+    // col_perms are equal: column offsets, local row in the block, position in S.x
+    DevBuf<int> cp, rows, pos;
+    DevBuf<double> vals; // S.x gathered in compact order (refill scratch)
+    DevBuf<double> BT;   // the source blocks transposed (refill scratch)
+    int tr_x = 0, tr_y = 0; // transpose grid: 32 x 32 tiles of the largest block
+    DevBuf<BlkDesc> desc;
+    DevBuf<BlkTile> tiles;
+    int ntiles = 0;
+};
+
+// Builds the plan of C_k = B_k S[col_perm_k, :] for n_src source blocks of shape
+// m0[k] x n0[k] (col_perm[k] strictly increasing rows of S); S given by its host CSR
+// structure (S_m x S_n). When keep_empty, every source block gets an output block
+// (a single permuted_dense), else blocks without columns are dropped.
+std::unique_ptr<BlocksCsrPlan> blocks_csr_build(int n_src, const int *m0, const int *n0,
+                                                const int *const *col_perm, const int *Sp, const int *Si,
+                                                int S_m, int S_n, bool keep_empty, cudaStream_t s);
+// C values (output blocks in order, each m0 x n0_C row-major) from the B values
+// (source blocks in order, each m0 x n0 row-major) and S.x; all device pointers.
+void blocks_csr_fill(const BlocksCsrPlan &P, const double *B_vals, const double *S_x, double *C_vals,
+                     cudaStream_t s);
+
+} // namespace sdl

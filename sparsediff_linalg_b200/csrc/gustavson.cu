@@ -792,6 +792,7 @@ __global__ void __launch_bounds__(256) k_entry_values_batched(const EntChunk *__
     const EntChunk c = chunks[blockIdx.x];
     const ProdSched S = scheds[c.prod];
     const ProdPtrs P = ptrs[c.prod];
+    if (!P.Lx && !P.d) return; // unit product: the refill reads no V
     entry_values_run(S, P, c.begin + threadIdx.x, c.begin + c.count, blockDim.x);
 }
 
@@ -830,7 +831,8 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
         r.C = ptrs[prod].Cx;
         r.W = scheds[prod].W;
         r.X = scheds[prod].X;
-        r.V = scheds[prod].V;
+        // a unit product (no L values, no d) has every entry value 1.0: V is not read
+        r.V = (ptrs[prod].Lx || ptrs[prod].d) ? scheds[prod].V : nullptr;
         r.ES = scheds[prod].ES;
         r.nV = (unsigned)scheds[prod].nV;
         r.nA = (unsigned)scheds[prod].nA;
@@ -841,7 +843,7 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
         r.C = P1.Cx;
         r.W = S1.W;
         r.X = S1.X;
-        r.V = S1.V;
+        r.V = (P1.Lx || P1.d) ? S1.V : nullptr;
         r.ES = S1.ES;
         r.nV = (unsigned)S1.nV;
         r.nA = (unsigned)S1.nA;
@@ -869,7 +871,7 @@ __device__ __forceinline__ bool term_value(const ProdBase &pb, int vbase, unsign
     const int2 es = pb.ES[vi];
     const unsigned a = (unsigned)(es.x + u);
     if (a >= pb.nA || (unsigned)es.y >= pb.nV) return false;
-    prod = __dmul_rn(pb.V[es.y], pb.Ax[a]);
+    prod = pb.V ? __dmul_rn(pb.V[es.y], pb.Ax[a]) : __dmul_rn(1.0, pb.Ax[a]);
     return true;
 }
 
@@ -967,7 +969,7 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
             {
                 const unsigned a = (unsigned)(es[j].x + base + tid + j * REFILL_THREADS);
                 ok[j] = ok[j] && a < pb.nA && (unsigned)es[j].y < pb.nV;
-                v[j] = ok[j] ? pb.V[es[j].y] : 0.0;
+                v[j] = ok[j] ? (pb.V ? pb.V[es[j].y] : 1.0) : 0.0;
                 x[j] = ok[j] ? pb.Ax[a] : 0.0;
             }
             unsigned wn[RUNROLL];
@@ -1626,7 +1628,7 @@ ProdSched sched_of(const Product &P)
 
 void entry_values(const ProdSched &S, const ProdPtrs &vals, cudaStream_t s)
 {
-    if (S.nV <= 0) return;
+    if (S.nV <= 0 || (!vals.Lx && !vals.d)) return; // unit product: every value is 1.0
     SDL_LAUNCH(k_entry_values, grid_for(S.nV, 256 * EV_ILP, runtime().num_sms * 8), 256, 0, s, S, vals);
 }
 

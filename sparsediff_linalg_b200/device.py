@@ -142,6 +142,53 @@ class Coalesce:
             pass
 
 
+class BlocksCsr:
+    """C_k = B_k S[col_perm_k, :] for dense blocks B_k (m0[k] x n0[k], a stacked_pd's
+    blocks) and a sparse CSR S (sdl_blocks_csr_*). The structure is taken from host
+    arrays; fill() works on device tensors: B_vals (source blocks in order, each
+    row-major), S_x, and C_vals (output blocks in order, each m0 x n0_C row-major)."""
+
+    def __init__(self, m0, n0, col_perms, Sp, Si, S_m, S_n, keep_empty=False, stream=None):
+        import numpy as np
+        L = lib()
+        nb = len(m0)
+        self._m0 = np.ascontiguousarray(m0, np.int32)
+        self._n0 = np.ascontiguousarray(n0, np.int32)
+        self._perms = [np.ascontiguousarray(c, np.int32) for c in col_perms]
+        arr = (C.c_void_p * max(1, nb))(*[c.ctypes.data for c in self._perms])
+        self._Sp = np.ascontiguousarray(Sp, np.int32)
+        self._Si = np.ascontiguousarray(Si, np.int32)
+        h = C.c_void_p()
+        check(L.sdl_blocks_csr_create(nb, self._m0.ctypes.data, self._n0.ctypes.data, arr,
+                                      self._Sp.ctypes.data, self._Si.ctypes.data, S_m, S_n,
+                                      1 if keep_empty else 0, _stream(stream), C.byref(h)))
+        self.handle = h
+        ob, cv, bv = C.c_int(), C.c_longlong(), C.c_longlong()
+        check(L.sdl_blocks_csr_info(h, C.byref(ob), C.byref(cv), C.byref(bv)))
+        self.out_blocks, self.c_values, self.b_values = ob.value, cv.value, bv.value
+        self.blocks = []
+        for k in range(self.out_blocks):
+            src, m, n0c, cp = C.c_int(), C.c_int(), C.c_int(), C.c_void_p()
+            check(L.sdl_blocks_csr_block(h, k, C.byref(src), C.byref(m), C.byref(n0c), C.byref(cp)))
+            if n0c.value > 0:
+                perm = np.ctypeslib.as_array(C.cast(cp, C.POINTER(C.c_int)), shape=(n0c.value,)).copy()
+            else:
+                perm = np.zeros(0, np.int32)
+            self.blocks.append((src.value, m.value, n0c.value, perm))
+
+    def fill(self, B_vals, S_x, C_vals, stream=None):
+        check(lib().sdl_blocks_csr_fill(self.handle, _ptr(B_vals), _ptr(S_x), _ptr(C_vals),
+                                        _stream(stream)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().sdl_blocks_csr_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 class Batch:
     """Batched refill of many products: one persistent launch over all their tiles,
     replayed from a CUDA graph (sdl_batch_*)."""

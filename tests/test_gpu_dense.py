@@ -1,0 +1,144 @@
+"""Dense blocks times a sparse CSR on the GPU (permuted_dense / stacked_pd x sparse),
+against the CPU oracle and the upstream library itself. Tolerance: none -- the
+blocks' column sets and every value must be bit-identical (each output is summed
+in upstream's order)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from sparsediff_linalg_b200 import workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.int64)
+
+
+def _blocks(rng, S_m, specs):
+    """specs: [(m0, n0)]; col_perm = n0 sorted distinct rows of S."""
+    out = []
+    for m0, n0 in specs:
+        perm = np.sort(rng.choice(S_m, size=n0, replace=False)).astype(np.int32)
+        X = rng.standard_normal((m0, n0)) * 10.0 ** rng.integers(-6, 7, (m0, n0))
+        out.append((X, perm))
+    return out
+
+
+def _run_device(blocks, S, keep_empty):
+    import torch
+    from sparsediff_linalg_b200.device import BlocksCsr
+    Sp, Si, Sx, S_m, S_n = S
+    P = BlocksCsr([X.shape[0] for X, _ in blocks], [X.shape[1] for X, _ in blocks],
+                  [c for _, c in blocks], Sp, Si, S_m, S_n, keep_empty=keep_empty)
+    Bv = torch.as_tensor(np.concatenate([X.ravel() for X, _ in blocks] + [np.zeros(1)]), device="cuda")
+    Sx_d = torch.as_tensor(np.asarray(Sx, np.float64), device="cuda")
+    Cv = torch.full((max(1, P.c_values),), np.nan, dtype=torch.float64, device="cuda")
+    P.fill(Bv, Sx_d, Cv)
+    torch.cuda.synchronize()
+    Cv = Cv.cpu().numpy()
+    res, off = [], 0
+    for src, m0, n0c, perm in P.blocks:
+        res.append((src, perm, Cv[off:off + m0 * n0c].reshape(m0, n0c)))
+        off += m0 * n0c
+    return P, res
+
+
+@pytest.mark.parametrize("keep_empty", [False, True])
+def test_blocks_csr_bit_exact(sdl, orc, keep_empty):
+    """Blocks of many shapes (incl. 1 x 1, empty-result blocks, columns with more
+    than 8 terms) against the oracle; empty blocks dropped unless keep_empty."""
+    rng = np.random.default_rng(91)
+    S_m, S_n = 300, 5000
+    lens = rng.integers(0, 40, S_m)
+    lens[:20] = 0                       # rows of S without entries
+    lens[20:25] = 3000                  # dense-ish rows: columns with many terms
+    S = wl.variable_rowlen_csr(S_m, S_n, lens, rng)
+    specs = [(1, 1), (7, 13), (64, 256), (33, 5), (5, 40), (16, 300)]
+    blocks = _blocks(rng, S_m, specs)
+    blocks.append((rng.standard_normal((4, 10)), np.arange(10, dtype=np.int32)))  # only empty rows
+    want = orc.blocks_csr(blocks, S[0], S[1], S[2], S_n)
+    P, got = _run_device(blocks, S, keep_empty)
+    kept = [k for k, (cols, C_k) in enumerate(want) if keep_empty or C_k.size]
+    assert [g[0] for g in got] == kept
+    for (src, perm, Cg) in got:
+        cols, Cw = want[src]
+        assert np.array_equal(perm, cols)
+        assert np.array_equal(bits(Cg), bits(Cw)), f"block {src}"
+
+
+def test_blocks_csr_config_shape(sdl, orc):
+    """The 64 x 256 block shape of the benchmark (S 256 x 20000, 6 entries per
+    column), four blocks."""
+    rng = np.random.default_rng(92)
+    S_m, S_n = 256, 20000
+    St = wl.fixed_rowlen_csr(S_n, S_m, 6, rng)          # CSC of S as a CSR of S^T
+    from oracle import oracle
+    Sp, Si, Sx = oracle.transpose(St[0], St[1], St[2], S_n, S_m)
+    S = (Sp, Si, Sx, S_m, S_n)
+    blocks = [(rng.standard_normal((64, 256)), np.arange(256, dtype=np.int32)) for _ in range(4)]
+    want = orc.blocks_csr(blocks, Sp, Si, Sx, S_n)
+    P, got = _run_device(blocks, S, False)
+    assert len(got) == 4
+    for (src, perm, Cg) in got:
+        cols, Cw = want[src]
+        assert np.array_equal(perm, cols)
+        assert np.array_equal(bits(Cg), bits(Cw))
+
+
+def test_BA_pd_sparse_matches_upstream_library(sdl, orc):
+    """BA_matrices_alloc / BA_matrices_fill_values with B permuted_dense and A
+    sparse, through the drop-in C ABI, against the same calls on the upstream
+    library compiled from its sources; then a refill with new values of both."""
+    if not orc.reference_available():
+        pytest.skip("upstream library not built")
+    from sparsediff_linalg_b200 import matrices as M
+    from sparsediff_linalg_b200._lib import CSR_p, matrix_p
+    from sparsediff_linalg_b200.host import csr_from_ptr
+    ref = orc.reference()
+    rng = np.random.default_rng(93)
+    A = wl.small_random_csr(120, 900, 0.03, rng)       # S: 120 x 900
+    rp = np.sort(rng.choice(200, size=37, replace=False)).astype(np.int32)
+    cp = np.sort(rng.choice(120, size=50, replace=False)).astype(np.int32)
+    X = rng.standard_normal((37, 50))
+    to_csr = C.CFUNCTYPE(CSR_p, matrix_p)
+
+    def ref_sparse(csr):
+        p, i, x, m, n = csr
+        c = ref.new_CSR_matrix(m, n, len(i))
+        s = c.contents
+        np.ctypeslib.as_array(s.p, shape=(m + 1,))[:] = p
+        np.ctypeslib.as_array(s.i, shape=(max(1, len(i)),))[:len(i)] = i
+        np.ctypeslib.as_array(s.x, shape=(max(1, len(i)),))[:len(i)] = x
+        return ref.new_sparse_matrix(c)
+
+    Ar = ref_sparse(A)
+    Br = ref.new_permuted_dense(200, 120, 37, 50, rp.ctypes.data, cp.ctypes.data, X.ctypes.data)
+    Cr = ref.BA_matrices_alloc(Br, Ar)
+    ref.BA_matrices_fill_values(Br, Ar, Cr)
+    want = csr_from_ptr(to_csr(Cr.contents.to_csr)(Cr))
+
+    Am = M.SparseMatrix.from_csr(*A)
+    Bm = M.permuted_dense(200, 120, rp, cp, X)
+    Cm = M.BA(Bm, Am)
+    M.BA_fill(Bm, Am, Cm)
+    got = Cm.csr()
+    for g, w in zip(got, want[:3]):
+        assert np.array_equal(bits(g) if g.dtype == np.float64 else g, bits(w) if w.dtype == np.float64 else w)
+    # refill: new values of A and B in both libraries
+    ax = rng.standard_normal(len(A[1]))
+    X2 = rng.standard_normal((37, 50))
+    Am.set_values(ax)
+    Bm.set_values(X2.ravel())
+    M.BA_fill(Bm, Am, Cm)
+    np.ctypeslib.as_array(Ar.contents.x, shape=(len(ax),))[:] = ax
+    Ar.contents.values_version += 1
+    np.ctypeslib.as_array(Br.contents.x, shape=(X2.size,))[:] = X2.ravel()
+    Br.contents.values_version += 1
+    ref.BA_matrices_fill_values(Br, Ar, Cr)
+    want2 = csr_from_ptr(to_csr(Cr.contents.to_csr)(Cr))
+    assert np.array_equal(bits(Cm.csr()[2]), bits(want2[2]))
+    ref.free_matrix(Cr)
+    ref.free_matrix(Br)
+    ref.free_matrix(Ar)
