@@ -656,6 +656,55 @@ def run_dense(args, dev, peak):
             out["upstream_cpu"] = {"unavailable": str(e)[:200]}
     del P, Bv, Sx_d, Cv
     torch.cuda.empty_cache()
+    out["ata_dmma"] = run_dense_ata(args, dev, X, blocks_rows, cperm)
+    return out
+
+
+def reference_atda_spd_times(m, n, blocks_rows, cperm, X, d, reps):
+    from oracle import oracle
+    L = C.CDLL(str(oracle.REF_DIR / "libsdl_reftime.so"))
+    ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+    L.ref_time_atda_spd.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, dp, dp, C.c_int, dp]
+    L.ref_time_atda_spd.restype = None
+    nb, m0, n0 = X.shape
+    keep = [np.ascontiguousarray(a) for a in (blocks_rows, cperm, X, d)]
+    c = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+    out = np.zeros(2)
+    L.ref_time_atda_spd(m, n, nb, m0, n0, c(keep[0], C.c_int), c(keep[1], C.c_int), c(keep[2], C.c_double),
+                        c(keep[3], C.c_double), reps, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def run_dense_ata(args, dev, X, blocks_rows, cperm):
+    """A^T diag(d) A of the same stacked_pd (64 blocks of 64 x 256, col_perm 0..255):
+    64 partials of 256 x 256 on the FP64 tensor cores (mma.sync m8n8k4), summed in
+    block order into one 256 x 256 block. 2 * 64 * 64 * 256 * 256 flops."""
+    import torch
+    from sparsediff_linalg_b200.device import BlocksAta
+    nb, m0, n0 = X.shape
+    m = nb * m0
+    rng = np.random.default_rng(7)
+    d = rng.uniform(0.1, 10.0, m)
+    P = BlocksAta([m0] * nb, [n0] * nb, [blocks_rows[k * m0:(k + 1) * m0] for k in range(nb)], [cperm] * nb,
+                  m, n0)
+    Xv = torch.as_tensor(X.ravel(), device=dev)
+    dd = torch.as_tensor(d, device=dev)
+    Cv = torch.empty(P.c_values, dtype=torch.float64, device=dev)
+    s = torch.cuda.current_stream()
+    for _ in range(3):
+        P.fill(Xv, dd, Cv, stream=s)
+    ms = _event_ms(lambda st: P.fill(Xv, dd, Cv, stream=st), s, max(3, min(args.steps, 10)))
+    flops = 2.0 * nb * m0 * n0 * n0
+    out = {"workload": "A^T diag(d) A, A the stacked_pd above (64 blocks of 64 x 256), FP64 tensor cores",
+           "out_blocks": P.out_blocks, "fill_us": round(ms * 1e3, 2),
+           "fp64_tflops": round(flops / (ms * 1e-3) / 1e12, 2), "flops": int(flops)}
+    if not args.no_cpu_baseline:
+        try:
+            r = reference_atda_spd_times(m, n0, blocks_rows, cperm, X, d, 3)
+            out["upstream_cpu"] = {"alloc_ms": round(r[0] * 1e3, 2), "fill_ms": round(r[1] * 1e3, 2),
+                                   "blas": "OpenBLAS 0.3.15 (its own threading)"}
+        except Exception as e:  # noqa: BLE001
+            out["upstream_cpu"] = {"unavailable": str(e)[:200]}
     return out
 
 

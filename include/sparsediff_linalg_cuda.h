@@ -249,6 +249,32 @@ sdl_status sdl_blocks_csr_fill(const sdl_blocks_csr *P, const double *B_vals,
                                const double *S_x, double *C_vals, void *stream);
 void sdl_blocks_csr_destroy(sdl_blocks_csr *P);
 
+/* ------------------------------------------------------------------------
+   A^T diag(d) A of dense blocks, device-resident (upstream ATA_spd_alloc /
+   ATDA_spd_fill_values, src/stacked_pd/stacked_pd_linalg.c:197-237; with one
+   block ATA_pd_alloc / ATDA_pd_fill_values, src/permuted_dense/
+   permuted_dense_linalg.c:87-112). Block k is m0[k] x n0[k] at rows row_perm[k]
+   of m and columns col_perm[k] (strictly increasing) of n. Each block's
+   X^T diag(d) X runs on the FP64 tensor cores; the partials are coalesced as
+   upstream does (output blocks grouped by the set of blocks that hold a row;
+   each cell summed from +0.0 in block order). The dgemm inside upstream has no
+   specified summation order, so results agree within rounding (about 1e-15 of
+   the sum of |terms|), not bit for bit. X_vals: the blocks' values in order,
+   row-major; d: m values or NULL (identity); C_vals: the output blocks in order,
+   row-major.
+   ------------------------------------------------------------------------ */
+typedef struct sdl_blocks_ata sdl_blocks_ata;
+sdl_status sdl_blocks_ata_create(int n_blocks, const int *m0, const int *n0,
+                                 const int *const *row_perm, const int *const *col_perm, int m,
+                                 int n, void *stream, sdl_blocks_ata **out);
+sdl_status sdl_blocks_ata_info(const sdl_blocks_ata *P, int *out_blocks, long long *c_values,
+                               long long *x_values);
+sdl_status sdl_blocks_ata_block(const sdl_blocks_ata *P, int k, int *m0, int *n0,
+                                const int **rows, const int **cols);
+sdl_status sdl_blocks_ata_fill(const sdl_blocks_ata *P, const double *X_vals, const double *d,
+                               double *C_vals, void *stream);
+void sdl_blocks_ata_destroy(sdl_blocks_ata *P);
+
 /* Host-pointer form for COO_matrix users (no upstream counterpart): the
    coalesced CSR of A (m x n), and a refill of its values from A->x. */
 CSR_matrix *COO_coalesce_alloc(const COO_matrix *A);

@@ -248,3 +248,45 @@ def blocks_csr(blocks, Sp, Si, Sx, S_n):
                 C[:, idx] = C[:, idx] + X[:, rr] * vv[None, :]
         out.append((np.array(cols, np.int32), C))
     return out
+
+
+def blocks_ata(blocks, d, n):
+    """A^T diag(d) A of dense blocks [(X_k, row_perm_k, col_perm_k)], as upstream's
+    ATA_spd_alloc / ATDA_spd_fill_values (src/stacked_pd/stacked_pd_linalg.c:197-237
+    with the coalescing of src/stacked_pd/stacked_pd_coalesce.c:150-381): per block
+    P_k = X_k^T diag(d[row_perm_k]) X_k; output blocks grouped by the set of blocks
+    whose col_perm holds a row (in order of first appearance, rows ascending), columns
+    the union of their col_perms; each cell the partials summed from 0 in block
+    order. Returns [(rows, cols, C_o, Cabs_o)] where Cabs is the same sum of |terms|
+    (the scale of the rounding bound). Test infrastructure only."""
+    parts = []
+    for X, rp, cp in blocks:
+        X = np.asarray(X, np.float64)
+        dp = np.ones(X.shape[0]) if d is None else np.asarray(d, np.float64)[np.asarray(rp)]
+        W = X * dp[:, None]
+        parts.append((np.asarray(cp), X.T @ W, np.abs(X).T @ np.abs(W)))
+    sig_of, order = {}, []
+    for r in range(n):
+        sig = tuple(k for k, (cp, _, _) in enumerate(parts) if r in set(cp.tolist()))
+        if not sig:
+            continue
+        if sig not in sig_of:
+            sig_of[sig] = []
+            order.append(sig)
+        sig_of[sig].append(r)
+    out = []
+    for sig in order:
+        rows = np.array(sig_of[sig], np.int32)
+        cols = np.unique(np.concatenate([parts[k][0] for k in sig])).astype(np.int32)
+        Cv = np.zeros((len(rows), len(cols)))
+        Ca = np.zeros_like(Cv)
+        for k in sig:
+            cp, Pk, Ak = parts[k]
+            pos = {c: j for j, c in enumerate(cp.tolist())}
+            ri = [pos[r] for r in rows.tolist()]
+            cj = [j for j, c in enumerate(cols.tolist()) if c in pos]
+            ck = [pos[c] for c in cols.tolist() if c in pos]
+            Cv[:, cj] = Cv[:, cj] + Pk[np.ix_(ri, ck)]
+            Ca[:, cj] = Ca[:, cj] + Ak[np.ix_(ri, ck)]
+        out.append((rows, cols, Cv, Ca))
+    return out

@@ -168,3 +168,27 @@ void ref_time_ba_spd_csr(int m, int n_blocks, int m0, int n0, const int *rows, c
     free_matrix(B);
     free_CSR_matrix(S);
 }
+
+/* A^T diag(d) A of the same stacked_pd through upstream's ATA_matrices_alloc /
+ * ATDA_matrices_fill_values (per-block cblas_dgemm, then coalescing).
+ * out[0] = alloc seconds, out[1] = seconds per fill. */
+extern matrix *ATA_matrices_alloc(matrix *A);
+extern void ATDA_matrices_fill_values(const matrix *A, const double *d, matrix *C);
+
+void ref_time_atda_spd(int m, int n, int n_blocks, int m0, int n0, const int *rows, const int *cperm,
+                       const double *X, const double *d, int reps, double *out)
+{
+    matrix **blocks = (matrix **)malloc((size_t)n_blocks * sizeof(matrix *));
+    for (int k = 0; k < n_blocks; ++k)
+        blocks[k] = new_permuted_dense(m, n, m0, n0, rows + (size_t)k * m0, cperm, X + (size_t)k * m0 * n0);
+    matrix *A = new_stacked_pd(m, n, n_blocks, blocks, NULL, NULL);
+    free(blocks);
+    double t0 = now();
+    matrix *C = ATA_matrices_alloc(A);
+    out[0] = now() - t0;
+    t0 = now();
+    for (int r = 0; r < reps; ++r) ATDA_matrices_fill_values(A, d, C);
+    out[1] = (now() - t0) / (reps > 0 ? reps : 1);
+    free_matrix(C);
+    free_matrix(A);
+}

@@ -133,6 +133,12 @@ EXTENSION_SIGNATURES = {
     "sdl_blocks_csr_block": (C.c_int, [vp, C.c_int, c_int_p, c_int_p, c_int_p, C.POINTER(vp)]),
     "sdl_blocks_csr_fill": (C.c_int, [vp, vp, vp, vp, vp]),
     "sdl_blocks_csr_destroy": (None, [vp]),
+    "sdl_blocks_ata_create": (C.c_int, [C.c_int, vp, vp, C.POINTER(vp), C.POINTER(vp), C.c_int, C.c_int, vp,
+                                        C.POINTER(vp)]),
+    "sdl_blocks_ata_info": (C.c_int, [vp, c_int_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "sdl_blocks_ata_block": (C.c_int, [vp, C.c_int, c_int_p, c_int_p, C.POINTER(vp), C.POINTER(vp)]),
+    "sdl_blocks_ata_fill": (C.c_int, [vp, vp, vp, vp, vp]),
+    "sdl_blocks_ata_destroy": (None, [vp]),
     "COO_coalesce_alloc": (CSR_p, [COO_p]),
     "COO_coalesce_fill_values": (None, [COO_p, CSR_p]),
 }

@@ -16,12 +16,16 @@ namespace sdl {
 // A sparse): the product plan and the device copies of B's and C's values.
 struct PdImpl
 {
-    std::unique_ptr<BlocksCsrPlan> ba;
-    DevBuf<double> bvals, cvals;
+    std::unique_ptr<BlocksCsrPlan> ba;  // bound by BA_matrices_alloc (B pd, A sparse)
+    std::unique_ptr<BlocksAtaPlan> ata; // bound by ATA_matrices_alloc (A pd)
+    DevBuf<double> bvals, cvals, dvec;
 };
 const double *sparse_dev_values(sdl_sparse *A, cudaStream_t s);
+// Device state bound to a stacked_pd produced by ATA_matrices_alloc (A spd).
 struct SpdImpl
 {
+    std::unique_ptr<BlocksAtaPlan> ata;
+    DevBuf<double> xvals, cvals, dvec;
 };
 
 namespace {
@@ -215,8 +219,100 @@ void dense_BA_fill(const matrix *Bm, const matrix *Am, matrix *Cm)
     SDL_CUDA(cudaStreamSynchronize(s));
     matrix_values_changed(Cm);
 }
-matrix *dense_ATA_alloc(matrix *) { unsupported("ATA_matrices_alloc"); }
-void dense_ATDA_fill(const matrix *, const double *, matrix *) { unsupported("ATDA_matrices_fill_values"); }
+// ATA with A permuted_dense or stacked_pd (upstream matmul_dispatchers.c:490-527 ->
+// ATA_pd_* / ATA_spd_*): the partials on the FP64 tensor cores, coalesced as upstream.
+matrix *dense_ATA_alloc(matrix *Am)
+{
+    cudaStream_t s = runtime().stream;
+    if (Am->kind == MATRIX_PERMUTED_DENSE)
+    {
+        const permuted_dense *A = as_pd(Am);
+        const int *rp = A->row_perm, *cp = A->col_perm;
+        auto plan = blocks_ata_build(1, &A->m0, &A->n0, &rp, &cp, A->base.m, A->base.n, s);
+        // one block: C = n0 x n0 at col_perm x col_perm (upstream permuted_dense_linalg.c:87-99)
+        matrix *Cm = new_permuted_dense(A->base.n, A->base.n, A->n0, A->n0, A->col_perm, A->col_perm, nullptr);
+        if (!Cm) fail(SDL_ERR_INTERNAL, "ATA_matrices_alloc: output allocation failed");
+        permuted_dense *C = as_pd(Cm);
+        C->impl->bvals.reset((size_t)std::max<long long>(1, plan->x_total));
+        C->impl->cvals.reset((size_t)std::max<long long>(1, plan->c_total));
+        C->impl->dvec.reset((size_t)std::max(1, A->base.m));
+        C->impl->ata = std::move(plan);
+        return Cm;
+    }
+    if (Am->kind != MATRIX_STACKED_PD) unsupported("ATA_matrices_alloc");
+    const sdl_stacked *A = as_spd(Am);
+    std::vector<int> m0(std::max(1, A->n_blocks)), n0(std::max(1, A->n_blocks));
+    std::vector<const int *> rp(std::max(1, A->n_blocks)), cp(std::max(1, A->n_blocks));
+    for (int k = 0; k < A->n_blocks; ++k)
+    {
+        m0[k] = A->blocks[k]->m0;
+        n0[k] = A->blocks[k]->n0;
+        rp[k] = A->blocks[k]->row_perm;
+        cp[k] = A->blocks[k]->col_perm;
+    }
+    auto plan = blocks_ata_build(A->n_blocks, m0.data(), n0.data(), rp.data(), cp.data(), A->base.m, A->base.n, s);
+    const int nb = plan->n_out;
+    permuted_dense **blocks = (permuted_dense **)sp_malloc(sizeof(permuted_dense *) * std::max(1, nb));
+    std::vector<int> sp_p(1, 0), sp_i;
+    for (int o = 0; o < nb; ++o)
+    {
+        const std::vector<int> &r = plan->out_rows[o], &c = plan->out_cols[o];
+        blocks[o] = as_pd(new_permuted_dense(A->base.n, A->base.n, (int)r.size(), (int)c.size(), r.data(),
+                                             c.data(), nullptr));
+        if (!blocks[o]) fail(SDL_ERR_INTERNAL, "ATA_matrices_alloc: output allocation failed");
+        sp_i.insert(sp_i.end(), plan->out_srcs[o].begin(), plan->out_srcs[o].end());
+        sp_p.push_back((int)sp_i.size());
+    }
+    if (sp_i.empty()) sp_i.push_back(0);
+    matrix *Cm = new_stacked_pd(A->base.n, A->base.n, nb, blocks, sp_p.data(), sp_i.data());
+    sp_free(blocks);
+    if (!Cm) fail(SDL_ERR_INTERNAL, "ATA_matrices_alloc: output allocation failed");
+    sdl_stacked *C = as_spd(Cm);
+    C->impl->xvals.reset((size_t)std::max<long long>(1, plan->x_total));
+    C->impl->cvals.reset((size_t)std::max<long long>(1, plan->c_total));
+    C->impl->dvec.reset((size_t)std::max(1, A->base.m));
+    C->impl->ata = std::move(plan);
+    return Cm;
+}
+
+void dense_ATDA_fill(const matrix *Am, const double *d, matrix *Cm)
+{
+    cudaStream_t s = runtime().stream;
+    const BlocksAtaPlan *P = nullptr;
+    DevBuf<double> *xv = nullptr, *cv = nullptr, *dv = nullptr;
+    const double *hx = nullptr;
+    double *hc = nullptr;
+    if (Am->kind == MATRIX_PERMUTED_DENSE && Cm->kind == MATRIX_PERMUTED_DENSE)
+    {
+        permuted_dense *C = as_pd(Cm);
+        if (!C->impl || !C->impl->ata) fail(SDL_ERR_INVALID, "ATDA_matrices_fill_values: C was not produced by ATA_matrices_alloc");
+        P = C->impl->ata.get();
+        xv = &C->impl->bvals;
+        cv = &C->impl->cvals;
+        dv = &C->impl->dvec;
+        hx = as_pd(Am)->X;
+        hc = C->X;
+    }
+    else if (Am->kind == MATRIX_STACKED_PD && Cm->kind == MATRIX_STACKED_PD)
+    {
+        sdl_stacked *C = as_spd(Cm);
+        if (!C->impl || !C->impl->ata) fail(SDL_ERR_INVALID, "ATDA_matrices_fill_values: C was not produced by ATA_matrices_alloc");
+        P = C->impl->ata.get();
+        xv = &C->impl->xvals;
+        cv = &C->impl->cvals;
+        dv = &C->impl->dvec;
+        hx = as_spd(Am)->values;
+        hc = C->values;
+    }
+    else
+        unsupported("ATDA_matrices_fill_values");
+    h2d(xv->get(), hx, (size_t)P->x_total, s);
+    if (d) h2d(dv->get(), d, (size_t)P->m, s);
+    blocks_ata_fill(*P, xv->get(), d ? dv->get() : nullptr, cv->get(), s);
+    d2h(hc, cv->get(), (size_t)P->c_total, s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    matrix_values_changed(Cm);
+}
 void dense_DA_fill(const double *, const matrix *, matrix *) { unsupported("DA_matrices_fill_values"); }
 matrix *dense_transpose_alloc(const matrix *) { unsupported("transpose_matrices_alloc"); }
 void dense_transpose_fill(const matrix *, matrix *) { unsupported("transpose_matrices_fill_values"); }
@@ -385,3 +481,56 @@ extern "C" sdl_status sdl_blocks_csr_fill(const sdl_blocks_csr *P, const double 
 }
 
 extern "C" void sdl_blocks_csr_destroy(sdl_blocks_csr *P) { delete P; }
+
+struct sdl_blocks_ata
+{
+    std::unique_ptr<sdl::BlocksAtaPlan> P;
+};
+
+extern "C" sdl_status sdl_blocks_ata_create(int n_blocks, const int *m0, const int *n0,
+                                            const int *const *row_perm, const int *const *col_perm, int m,
+                                            int n, void *stream, sdl_blocks_ata **out)
+{
+    return guard_status("sdl_blocks_ata_create", [&]() {
+        if (!out || (n_blocks > 0 && (!m0 || !n0 || !row_perm || !col_perm))) fail(SDL_ERR_INVALID, "NULL argument");
+        *out = nullptr;
+        auto h = std::make_unique<sdl_blocks_ata>();
+        h->P = blocks_ata_build(n_blocks, m0, n0, row_perm, col_perm, m, n, pick_stream(stream));
+        *out = h.release();
+    });
+}
+
+extern "C" sdl_status sdl_blocks_ata_info(const sdl_blocks_ata *P, int *out_blocks, long long *c_values,
+                                          long long *x_values)
+{
+    return guard_status("sdl_blocks_ata_info", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL plan");
+        if (out_blocks) *out_blocks = P->P->n_out;
+        if (c_values) *c_values = P->P->c_total;
+        if (x_values) *x_values = P->P->x_total;
+    });
+}
+
+extern "C" sdl_status sdl_blocks_ata_block(const sdl_blocks_ata *P, int k, int *m0, int *n0, const int **rows,
+                                           const int **cols)
+{
+    return guard_status("sdl_blocks_ata_block", [&]() {
+        if (!P || k < 0 || k >= P->P->n_out) fail(SDL_ERR_INVALID, "bad output block");
+        if (m0) *m0 = (int)P->P->out_rows[k].size();
+        if (n0) *n0 = (int)P->P->out_cols[k].size();
+        if (rows) *rows = P->P->out_rows[k].data();
+        if (cols) *cols = P->P->out_cols[k].data();
+    });
+}
+
+extern "C" sdl_status sdl_blocks_ata_fill(const sdl_blocks_ata *P, const double *X_vals, const double *d,
+                                          double *C_vals, void *stream)
+{
+    return guard_status("sdl_blocks_ata_fill", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL plan");
+        if (P->P->c_total > 0 && (!X_vals || !C_vals)) fail(SDL_ERR_INVALID, "NULL value pointer");
+        blocks_ata_fill(*P->P, X_vals, d, C_vals, pick_stream(stream));
+    });
+}
+
+extern "C" void sdl_blocks_ata_destroy(sdl_blocks_ata *P) { delete P; }

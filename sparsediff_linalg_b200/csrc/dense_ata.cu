@@ -1,0 +1,239 @@
+// A^T diag(d) A of dense blocks on the FP64 tensor cores (upstream
+// src/permuted_dense/permuted_dense_linalg.c:87-112 ATA_pd_* / ATDA_pd_*, and
+// src/stacked_pd/stacked_pd_linalg.c:197-237 ATA_spd_* / ATDA_spd_* with the
+// coalescing of src/stacked_pd/stacked_pd_coalesce.c:150-381).
+//
+// Upstream forms dwork = diag(d_perm) X (one rounding per product) and calls
+// cblas_dgemm for X^T dwork, whose summation order BLAS leaves unspecified; here
+// the same dwork products feed mma.sync.m8n8k4 f64 tiles (the K loop in ascending
+// row order). Partials are then summed cell by cell in upstream's block order,
+// from +0.0. The dgemm part is therefore equal to upstream's within rounding
+// (tests compare at 1e-12 of the sum of |terms|), everything around it exactly.
+#include <algorithm>
+#include <climits>
+#include <map>
+
+#include "capi_common.h"
+#include "dense_plan.h"
+
+namespace sdl {
+namespace {
+
+int grid_cap2(long long work_items, int per_block, int cap)
+{
+    long long g = (work_items + per_block - 1) / per_block;
+    return (int)std::max<long long>(1, std::min<long long>(g, cap));
+}
+
+__device__ __forceinline__ void mma_f64(double &c0, double &c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+// One warp per 16 x 16 tile (a0, b0) of partial P_k = X^T diag(d_perm) X: four
+// m8n8k4 accumulators, K = the block's rows in steps of 4.
+//   A fragment (8 x 4, row-major): lane holds A[lane / 4][lane % 4] = X[k + lane % 4][a + lane / 4]
+//   B fragment (4 x 8, col-major): lane holds B[lane % 4][lane / 4] = d * X[k + lane % 4][b + lane / 4]
+//   C (8 x 8): lane holds C[lane / 4][2 (lane % 4) + {0, 1}]
+__global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ mtiles, int nmt,
+                                                      const long long *__restrict__ x_off,
+                                                      const long long *__restrict__ p_off,
+                                                      const int *__restrict__ m0d, const int *__restrict__ n0d,
+                                                      const int *__restrict__ rowperm_all,
+                                                      const long long *__restrict__ rowperm_off,
+                                                      const double *__restrict__ X_vals,
+                                                      const double *__restrict__ d, double *__restrict__ P)
+{
+    const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (w >= nmt) return;
+    const int lane = threadIdx.x & 31;
+    const int4 t = mtiles[w];
+    const int k = t.x, a0 = t.y, b0 = t.z;
+    const int m0 = m0d[k], n0 = n0d[k];
+    const double *X = X_vals + x_off[k];
+    const int *rp = rowperm_all + rowperm_off[k];
+    const int g = lane >> 2, q = lane & 3;
+    double c[2][2][2] = {};
+    for (int kk = 0; kk < m0; kk += 4)
+    {
+        const int i = kk + q;
+        const bool ok = i < m0;
+        const double di = (ok && d) ? d[rp[i]] : 1.0;
+        double a[2], b[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const int ca = a0 + 8 * h + g, cb = b0 + 8 * h + g;
+            a[h] = (ok && ca < n0) ? X[(long long)i * n0 + ca] : 0.0;
+            const double xb = (ok && cb < n0) ? X[(long long)i * n0 + cb] : 0.0;
+            b[h] = d ? __dmul_rn(xb, di) : xb; // dwork = diag(d_perm) X, as upstream
+        }
+#pragma unroll
+        for (int ha = 0; ha < 2; ++ha)
+#pragma unroll
+            for (int hb = 0; hb < 2; ++hb) mma_f64(c[ha][hb][0], c[ha][hb][1], a[ha], b[hb]);
+    }
+    double *Pk = P + p_off[k];
+#pragma unroll
+    for (int ha = 0; ha < 2; ++ha)
+#pragma unroll
+        for (int hb = 0; hb < 2; ++hb)
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+            {
+                const int r = a0 + 8 * ha + g, cc = b0 + 8 * hb + 2 * q + e;
+                if (r < n0 && cc < n0) Pk[(long long)r * n0 + cc] = c[ha][hb][e];
+            }
+}
+
+// Output cells: the partials that hold the cell, summed from +0.0 in block order.
+__global__ void k_ata_gather(const BlocksAtaPlan::OutDesc *__restrict__ outd, int o_base,
+                             const int *__restrict__ srcs, const int *__restrict__ maps,
+                             const long long *__restrict__ p_off, const int *__restrict__ n0d,
+                             const double *__restrict__ P, double *__restrict__ C)
+{
+    const BlocksAtaPlan::OutDesc D = outd[o_base + blockIdx.y];
+    const long long cells = (long long)D.m0 * D.n0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cells;
+         e += (long long)gridDim.x * blockDim.x)
+    {
+        const int i = (int)(e / D.n0), j = (int)(e - (long long)i * D.n0);
+        double acc = 0.0;
+        const int *mp = maps + D.map_off;
+        for (int t = D.s_begin; t < D.s_end; ++t, mp += D.m0 + D.n0)
+        {
+            const int si = mp[i], sj = mp[D.m0 + j];
+            if (si < 0 || sj < 0) continue;
+            const int k = srcs[t];
+            acc = __dadd_rn(acc, P[p_off[k] + (long long)si * n0d[k] + sj]);
+        }
+        C[D.c_off + e] = acc;
+    }
+}
+
+} // namespace
+
+std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const int *n0,
+                                                const int *const *row_perm, const int *const *col_perm,
+                                                int m, int n, cudaStream_t s)
+{
+    if (n_src < 0 || m < 0 || n < 0) fail(SDL_ERR_INVALID, "blocks A^T D A: negative size");
+    auto P = std::make_unique<BlocksAtaPlan>();
+    P->m = m;
+    P->n = n;
+    P->n_src = n_src;
+    std::vector<long long> x_off(std::max(1, n_src)), p_off(std::max(1, n_src)), rp_off(std::max(1, n_src));
+    std::vector<int> h_m0(std::max(1, n_src)), h_n0(std::max(1, n_src)), h_rp;
+    std::vector<int4> mt;
+    for (int k = 0; k < n_src; ++k)
+    {
+        if (m0[k] < 0 || n0[k] < 0) fail(SDL_ERR_INVALID, "blocks A^T D A: negative block shape");
+        for (int r = 0; r < m0[k]; ++r)
+            if (row_perm[k][r] < 0 || row_perm[k][r] >= m) fail(SDL_ERR_INVALID, "blocks A^T D A: row_perm out of range");
+        for (int c = 0; c < n0[k]; ++c)
+            if (col_perm[k][c] < 0 || col_perm[k][c] >= n || (c && col_perm[k][c] <= col_perm[k][c - 1]))
+                fail(SDL_ERR_INVALID, "blocks A^T D A: col_perm is not strictly increasing columns");
+        x_off[k] = P->x_total;
+        p_off[k] = P->p_total;
+        rp_off[k] = (long long)h_rp.size();
+        h_m0[k] = m0[k];
+        h_n0[k] = n0[k];
+        h_rp.insert(h_rp.end(), row_perm[k], row_perm[k] + m0[k]);
+        P->x_total += (long long)m0[k] * n0[k];
+        P->p_total += (long long)n0[k] * n0[k];
+        for (int a = 0; a < n0[k]; a += 16)
+            for (int b = 0; b < n0[k]; b += 16) mt.push_back(make_int4(k, a, b, 0));
+    }
+    // upstream's coalescing of the partials (row_perm = col_perm = col_perm_k):
+    // signature of column r = the blocks whose col_perm holds r, in block order;
+    // output blocks in order of first appearance scanning r ascending
+    std::vector<std::vector<int>> row_blocks(std::max(1, n));
+    for (int k = 0; k < n_src; ++k)
+        for (int c = 0; c < n0[k]; ++c) row_blocks[col_perm[k][c]].push_back(k);
+    std::map<std::vector<int>, int> sig_id;
+    for (int r = 0; r < n; ++r)
+    {
+        if (row_blocks[r].empty()) continue;
+        auto it = sig_id.find(row_blocks[r]);
+        int sid;
+        if (it == sig_id.end())
+        {
+            sid = (int)P->out_rows.size();
+            sig_id.emplace(row_blocks[r], sid);
+            P->out_rows.emplace_back();
+            P->out_srcs.push_back(row_blocks[r]);
+        }
+        else
+            sid = it->second;
+        P->out_rows[sid].push_back(r);
+    }
+    P->n_out = (int)P->out_rows.size();
+    std::vector<BlocksAtaPlan::OutDesc> od;
+    std::vector<int> h_srcs, h_maps;
+    std::vector<int> pos(std::max(1, n), -1);
+    for (int o = 0; o < P->n_out; ++o)
+    {
+        std::vector<int> cols;
+        for (int k : P->out_srcs[o]) cols.insert(cols.end(), col_perm[k], col_perm[k] + n0[k]);
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        P->out_cols.push_back(cols);
+        BlocksAtaPlan::OutDesc D{};
+        D.c_off = P->c_total;
+        D.m0 = (int)P->out_rows[o].size();
+        D.n0 = (int)cols.size();
+        if ((long long)D.m0 * D.n0 > INT_MAX) fail(SDL_ERR_OVERFLOW, "blocks A^T D A: output block exceeds INT_MAX values");
+        D.s_begin = (int)h_srcs.size();
+        D.map_off = (long long)h_maps.size();
+        for (int k : P->out_srcs[o])
+        {
+            h_srcs.push_back(k);
+            for (int c = 0; c < n0[k]; ++c) pos[col_perm[k][c]] = c;
+            for (int r : P->out_rows[o]) h_maps.push_back(pos[r]);
+            for (int c : cols) h_maps.push_back(pos[c]);
+            for (int c = 0; c < n0[k]; ++c) pos[col_perm[k][c]] = -1;
+        }
+        D.s_end = (int)h_srcs.size();
+        od.push_back(D);
+        P->c_total += (long long)D.m0 * D.n0;
+    }
+    P->x_off = upload(x_off.data(), x_off.size(), s);
+    P->p_off = upload(p_off.data(), p_off.size(), s);
+    P->m0d = upload(h_m0.data(), h_m0.size(), s);
+    P->n0d = upload(h_n0.data(), h_n0.size(), s);
+    P->rowperm_all = upload(h_rp.data(), std::max<size_t>(1, h_rp.size()), s);
+    P->rowperm_off = upload(rp_off.data(), rp_off.size(), s);
+    P->P.reset((size_t)std::max<long long>(1, P->p_total));
+    P->nmtiles = (int)mt.size();
+    P->mtiles = upload(mt.data(), std::max<size_t>(1, mt.size()), s);
+    P->outd = upload(od.data(), std::max<size_t>(1, od.size()), s);
+    P->srcs = upload(h_srcs.data(), std::max<size_t>(1, h_srcs.size()), s);
+    P->maps = upload(h_maps.data(), std::max<size_t>(1, h_maps.size()), s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    return P;
+}
+
+void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double *d, double *C_vals,
+                     cudaStream_t s)
+{
+    if (P.c_total == 0) return;
+    if (P.nmtiles > 0)
+        SDL_LAUNCH(k_ata_partials, (P.nmtiles + 3) / 4, 128, 0, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
+                   P.p_off.get(), P.m0d.get(), P.n0d.get(), P.rowperm_all.get(), P.rowperm_off.get(), X_vals, d,
+                   P.P.get());
+    long long maxcells = 0;
+    // grid.x covers the largest output block; grid.y = output blocks
+    // (cells of block o: P.out_rows[o].size() * P.out_cols[o].size())
+    for (int o = 0; o < P.n_out; ++o)
+        maxcells = std::max(maxcells, (long long)P.out_rows[o].size() * (long long)P.out_cols[o].size());
+    for (int o = 0; o < P.n_out; o += 65535)
+    {
+        const dim3 grid(grid_cap2(maxcells, 256, 4096), (unsigned)std::min(65535, P.n_out - o));
+        SDL_LAUNCH(k_ata_gather, grid, 256, 0, s, P.outd.get(), o, P.srcs.get(), P.maps.get(), P.p_off.get(),
+                   P.n0d.get(), P.P.get(), C_vals);
+    }
+}
+
+} // namespace sdl

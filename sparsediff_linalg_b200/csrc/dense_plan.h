@@ -61,3 +61,52 @@ void blocks_csr_fill(const BlocksCsrPlan &P, const double *B_vals, const double 
                      cudaStream_t s);
 
 } // namespace sdl
+
+namespace sdl {
+
+// A^T diag(d) A for dense blocks A_k (m0[k] x n0[k], rows row_perm[k] of an m-row
+// matrix, columns col_perm[k] of n): the partial of every block,
+// P_k = X_k^T diag(d[row_perm_k]) X_k (n0 x n0, rows and columns col_perm_k), on the
+// FP64 tensor cores, then upstream's coalescing (src/stacked_pd/
+// stacked_pd_coalesce.c:150-381): output blocks grouped by the set of blocks that
+// contain a row (its signature), each cell the sum of the partials that hold it,
+// from +0.0 in block order (upstream ATA_spd_* in src/stacked_pd/
+// stacked_pd_linalg.c:197-237; ATA_pd_* in permuted_dense_linalg.c:87-112 is the
+// one-block case).
+struct BlocksAtaPlan
+{
+    int n = 0, m = 0, n_src = 0;
+    // output blocks (signatures): rows, columns, contributing source blocks
+    std::vector<std::vector<int>> out_rows, out_cols, out_srcs;
+    std::vector<int> src_p; // out k's sources: out_srcs flattened, src_p offsets
+    long long c_total = 0, p_total = 0, x_total = 0;
+    DevBuf<long long> x_off, p_off;       // per source block: its values / its partial
+    DevBuf<int> m0d, n0d;                 // per source block
+    DevBuf<int> rowperm_all;              // per source block, concatenated
+    DevBuf<long long> rowperm_off;
+    DevBuf<double> P;                     // partials (refill scratch)
+    DevBuf<int4> mtiles;                  // 16 x 16 tiles of the partials: (block, a0, b0, -)
+    int nmtiles = 0;
+    // gather of the output cells: per output block, per source: row / column maps
+    struct OutDesc
+    {
+        long long c_off; // first value of the output block
+        int m0, n0;
+        int s_begin, s_end; // its sources in srcs
+        long long map_off;  // row maps then column maps of its sources
+    };
+    DevBuf<OutDesc> outd;
+    DevBuf<int> srcs;   // source block ids
+    DevBuf<int> maps;   // per (output block, source): m0 row positions, n0 column positions (-1: absent)
+    int n_out = 0;
+};
+
+std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const int *n0,
+                                                const int *const *row_perm, const int *const *col_perm,
+                                                int m, int n, cudaStream_t s);
+// C values (output blocks in order, row-major) from the source values X_vals
+// (blocks in order, row-major) and d (m values, or null for the identity).
+void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double *d, double *C_vals,
+                     cudaStream_t s);
+
+} // namespace sdl

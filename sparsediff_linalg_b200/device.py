@@ -189,6 +189,51 @@ class BlocksCsr:
             pass
 
 
+class BlocksAta:
+    """A^T diag(d) A of dense blocks (m0[k] x n0[k] at rows row_perms[k] of m and
+    columns col_perms[k] of n) on the FP64 tensor cores, coalesced as upstream's
+    stacked_pd (sdl_blocks_ata_*). fill() works on device tensors: X_vals (blocks in
+    order, row-major), d (m values or None), C_vals (output blocks in order)."""
+
+    def __init__(self, m0, n0, row_perms, col_perms, m, n, stream=None):
+        import numpy as np
+        L = lib()
+        nb = len(m0)
+        self._m0 = np.ascontiguousarray(m0, np.int32)
+        self._n0 = np.ascontiguousarray(n0, np.int32)
+        self._rp = [np.ascontiguousarray(r, np.int32) for r in row_perms]
+        self._cp = [np.ascontiguousarray(c, np.int32) for c in col_perms]
+        ra = (C.c_void_p * max(1, nb))(*[r.ctypes.data for r in self._rp])
+        ca = (C.c_void_p * max(1, nb))(*[c.ctypes.data for c in self._cp])
+        h = C.c_void_p()
+        check(L.sdl_blocks_ata_create(nb, self._m0.ctypes.data, self._n0.ctypes.data, ra, ca, m, n,
+                                      _stream(stream), C.byref(h)))
+        self.handle = h
+        ob, cv, xv = C.c_int(), C.c_longlong(), C.c_longlong()
+        check(L.sdl_blocks_ata_info(h, C.byref(ob), C.byref(cv), C.byref(xv)))
+        self.out_blocks, self.c_values, self.x_values = ob.value, cv.value, xv.value
+        self.blocks = []
+        for k in range(self.out_blocks):
+            mm, nn, rr, cc = C.c_int(), C.c_int(), C.c_void_p(), C.c_void_p()
+            check(L.sdl_blocks_ata_block(h, k, C.byref(mm), C.byref(nn), C.byref(rr), C.byref(cc)))
+            rows = np.ctypeslib.as_array(C.cast(rr, C.POINTER(C.c_int)), shape=(mm.value,)).copy() \
+                if mm.value else np.zeros(0, np.int32)
+            cols = np.ctypeslib.as_array(C.cast(cc, C.POINTER(C.c_int)), shape=(nn.value,)).copy() \
+                if nn.value else np.zeros(0, np.int32)
+            self.blocks.append((rows, cols))
+
+    def fill(self, X_vals, d, C_vals, stream=None):
+        check(lib().sdl_blocks_ata_fill(self.handle, _ptr(X_vals), _ptr(d), _ptr(C_vals), _stream(stream)))
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None):
+                lib().sdl_blocks_ata_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
 class Batch:
     """Batched refill of many products: one persistent launch over all their tiles,
     replayed from a CUDA graph (sdl_batch_*)."""

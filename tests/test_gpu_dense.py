@@ -142,3 +142,139 @@ def test_BA_pd_sparse_matches_upstream_library(sdl, orc):
     ref.free_matrix(Cr)
     ref.free_matrix(Br)
     ref.free_matrix(Ar)
+
+
+# ---------------------------------------------------------------- A^T D A (FP64 tensor cores)
+def _spd_blocks(rng, m, n, specs):
+    """Row-disjoint blocks (a stacked_pd): specs [(m0, n0)]; col_perms overlap."""
+    rows = rng.permutation(m)
+    out, at = [], 0
+    for m0, n0 in specs:
+        rp = np.sort(rows[at:at + m0]).astype(np.int32)
+        at += m0
+        cp = np.sort(rng.choice(n, size=n0, replace=False)).astype(np.int32)
+        out.append((rng.standard_normal((m0, n0)), rp, cp))
+    return out
+
+
+def _close(got, want, scale, what):
+    err = np.abs(got - want)
+    bound = 1e-12 * scale + 1e-300
+    assert np.all(err <= bound), f"{what}: max err/bound {np.max(err / bound)}"
+
+
+def test_blocks_ata_matches_oracle(sdl, orc):
+    """Overlapping col_perms (several signatures), uneven shapes (K not a multiple of
+    4, n0 not a multiple of 16), with and without d: structure exact, values within
+    1e-12 of the sum of |terms| (upstream's dgemm order is unspecified)."""
+    import torch
+    from sparsediff_linalg_b200.device import BlocksAta
+    rng = np.random.default_rng(94)
+    m, n = 400, 70
+    blocks = _spd_blocks(rng, m, n, [(13, 20), (64, 45), (7, 3), (30, 70), (1, 1), (50, 33)])
+    for use_d in (True, False):
+        d = rng.uniform(0.1, 10, m) if use_d else None
+        want = orc.blocks_ata(blocks, d, n)
+        P = BlocksAta([X.shape[0] for X, _, _ in blocks], [X.shape[1] for X, _, _ in blocks],
+                      [r for _, r, _ in blocks], [c for _, _, c in blocks], m, n)
+        assert P.out_blocks == len(want)
+        Xv = torch.as_tensor(np.concatenate([X.ravel() for X, _, _ in blocks]), device="cuda")
+        dd = None if d is None else torch.as_tensor(d, device="cuda")
+        Cv = torch.full((P.c_values,), np.nan, dtype=torch.float64, device="cuda")
+        P.fill(Xv, dd, Cv)
+        torch.cuda.synchronize()
+        Cv = Cv.cpu().numpy()
+        off = 0
+        for (rows, cols), (wr, wc, Cw, Ca) in zip(P.blocks, want):
+            assert np.array_equal(rows, wr) and np.array_equal(cols, wc)
+            Cg = Cv[off:off + len(rows) * len(cols)].reshape(len(rows), len(cols))
+            off += Cg.size
+            _close(Cg, Cw, Ca, "A^T D A block")
+
+
+def _ref_csr(ref, M):
+    from sparsediff_linalg_b200._lib import CSR_p, matrix_p
+    from sparsediff_linalg_b200.host import csr_from_ptr
+    to_csr = C.CFUNCTYPE(CSR_p, matrix_p)
+    return csr_from_ptr(to_csr(M.contents.to_csr)(M))
+
+
+def test_ATDA_stacked_pd_matches_upstream_library(sdl, orc):
+    """ATA_matrices_alloc / ATDA_matrices_fill_values with A stacked_pd through the
+    drop-in C ABI vs the upstream library: identical structure, values within
+    1e-12 of the sum of |terms|; a refill with new values and d."""
+    if not orc.reference_available():
+        pytest.skip("upstream library not built")
+    from sparsediff_linalg_b200 import matrices as M
+    ref = orc.reference()
+    rng = np.random.default_rng(95)
+    m, n = 300, 60
+    blocks = _spd_blocks(rng, m, n, [(20, 30), (64, 25), (9, 60), (40, 12)])
+    d = rng.uniform(0.1, 10, m)
+
+    def build_ref(blks):
+        arr = (C.c_void_p * len(blks))()
+        for k, (X, rp, cp) in enumerate(blks):
+            Xc = np.ascontiguousarray(X)
+            pm = ref.new_permuted_dense(m, n, len(rp), len(cp), rp.ctypes.data, cp.ctypes.data, Xc.ctypes.data)
+            arr[k] = C.cast(pm, C.c_void_p)
+        return ref.new_stacked_pd(m, n, len(blks), arr, None, None)
+
+    Ar = build_ref(blocks)
+    Cr = ref.ATA_matrices_alloc(Ar)
+    ref.ATDA_matrices_fill_values(Ar, d.ctypes.data, Cr)
+    wp, wi, wx = _ref_csr(ref, Cr)[:3]
+
+    Am = M.stacked_pd(m, n, [M.permuted_dense(m, n, rp, cp, X) for X, rp, cp in blocks])
+    Cm = M.ATA(Am)
+    M.ATDA_fill(Am, d, Cm)
+    gp, gi, gx = Cm.csr()
+    assert np.array_equal(gp, wp) and np.array_equal(gi, wi)
+    dense_abs = np.zeros((n, n))
+    for rows, cols, _, Ca in orc.blocks_ata(blocks, d, n):
+        dense_abs[np.ix_(rows, cols)] = Ca
+    rr = np.repeat(np.arange(n), np.diff(wp))
+    _close(gx, wx, dense_abs[rr, wi], "ATDA stacked_pd")
+    # refill: new block values and d
+    X2 = [rng.standard_normal(X.shape) for X, _, _ in blocks]
+    d2 = rng.uniform(0.1, 10, m)
+    Am.set_values(np.concatenate([x.ravel() for x in X2]))
+    M.ATDA_fill(Am, d2, Cm)
+    blocks2 = [(x, rp, cp) for x, (_, rp, cp) in zip(X2, blocks)]
+    Ar2 = build_ref(blocks2)
+    Cr2 = ref.ATA_matrices_alloc(Ar2)
+    ref.ATDA_matrices_fill_values(Ar2, d2.ctypes.data, Cr2)
+    wx2 = _ref_csr(ref, Cr2)[2]
+    dense_abs[:] = 0
+    for rows, cols, _, Ca in orc.blocks_ata(blocks2, d2, n):
+        dense_abs[np.ix_(rows, cols)] = Ca
+    _close(Cm.csr()[2], wx2, dense_abs[rr, wi], "ATDA stacked_pd refill")
+    for h in (Cr, Ar, Cr2, Ar2):
+        ref.free_matrix(h)
+
+
+def test_ATDA_permuted_dense_matches_upstream_library(sdl, orc):
+    if not orc.reference_available():
+        pytest.skip("upstream library not built")
+    from sparsediff_linalg_b200 import matrices as M
+    ref = orc.reference()
+    rng = np.random.default_rng(96)
+    m, n = 90, 50
+    rp = np.sort(rng.choice(m, 37, replace=False)).astype(np.int32)
+    cp = np.sort(rng.choice(n, 29, replace=False)).astype(np.int32)
+    X = rng.standard_normal((37, 29))
+    d = rng.uniform(0.1, 10, m)
+    Ar = ref.new_permuted_dense(m, n, 37, 29, rp.ctypes.data, cp.ctypes.data, X.ctypes.data)
+    Cr = ref.ATA_matrices_alloc(Ar)
+    ref.ATDA_matrices_fill_values(Ar, d.ctypes.data, Cr)
+    wp, wi, wx = _ref_csr(ref, Cr)[:3]
+    Am = M.permuted_dense(m, n, rp, cp, X)
+    Cm = M.ATA(Am)
+    M.ATDA_fill(Am, d, Cm)
+    gp, gi, gx = Cm.csr()
+    assert np.array_equal(gp, wp) and np.array_equal(gi, wi)
+    W = X * d[rp][:, None]
+    scale = (np.abs(X).T @ np.abs(W)).ravel()
+    _close(gx, wx, scale, "ATDA permuted_dense")
+    ref.free_matrix(Cr)
+    ref.free_matrix(Ar)
