@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-conversions", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
+    ap.add_argument("--dense-blocks", type=int, default=64,
+                    help="blocks of the stacked_pd x CSC case (64 is the configuration; fewer for profiling)")
     ap.add_argument("--learned-matrices", type=int, default=200)
     return ap.parse_args()
 
@@ -618,7 +620,7 @@ def run_dense(args, dev, peak):
     from sparsediff_linalg_b200 import workloads as wl
     from sparsediff_linalg_b200.device import BlocksCsr
     rng = np.random.default_rng(6)
-    nb, m0, n0, S_n = 64, 64, 256, 100_000
+    nb, m0, n0, S_n = args.dense_blocks, 64, 256, 100_000
     rows = rng.permutation(nb * m0).astype(np.int32)
     blocks_rows = np.concatenate([np.sort(rows[k * m0:(k + 1) * m0]) for k in range(nb)]).astype(np.int32)
     cperm = np.arange(n0, dtype=np.int32)
@@ -641,7 +643,7 @@ def run_dense(args, dev, peak):
     nnzC = P.c_values
     sum_n0C = sum(b[2] for b in P.blocks)
     B_alg = 8 * nb * m0 * n0 + 12 * len(Si) + 4 * (S_n + 1) + 8 * nnzC + 4 * sum_n0C
-    out = {"workload": "stacked_pd (64 blocks of 64 x 256, rows permuted) x CSC 256 x 100000 with 6 "
+    out = {"workload": f"stacked_pd ({nb} blocks of 64 x 256, rows permuted) x CSC 256 x 100000 with 6 "
                        "entries per column, FP64", "out_blocks": P.out_blocks, "nnz_C": int(nnzC),
            "alloc_ms": round(alloc_ms, 2), "fill_ms": round(ms, 4),
            "fill_gbs": round(B_alg / (ms * 1e-3) / 1e9, 1),
