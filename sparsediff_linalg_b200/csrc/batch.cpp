@@ -76,8 +76,8 @@ extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, 
             {
                 rebase_tiles(P->tiles.get(), P->ntiles, i, B->tiles.get() + t_off, s);
                 t_off += P->ntiles;
-                append_entry_chunks(hs[i].nV, i, 2048, chunks);
             }
+            if ((P->num_count[NUM_TILE] && P->ntiles) || P->big_lists) append_entry_chunks(hs[i].nV, i, 2048, chunks);
         }
         if (count)
             SDL_CUDA(cudaMemcpyAsync(B->scheds.get(), hs.data(), count * sizeof(ProdSched),
@@ -120,7 +120,10 @@ extern "C" sdl_status sdl_batch_refill(sdl_batch *B, void *stream)
             for (int i : B->with_big)
             {
                 const ProdPtrs &pp = B->host_ptrs[i];
-                big_rows_refill(*B->prods[i], pp.Lx, pp.d, pp.Ax, pp.Cx, s, B->ptrs.get() + i);
+                if (B->prods[i]->big_lists)
+                    big_lists_refill(*B->prods[i], B->ptrs.get() + i, s);
+                else
+                    big_rows_refill(*B->prods[i], pp.Lx, pp.d, pp.Ax, pp.Cx, s, B->ptrs.get() + i);
             }
         };
         if (!B->exec)

@@ -33,6 +33,8 @@ namespace sdl {
 
 void segment_sort_u64(unsigned long long *d_keys, const int *d_off, int nseg, int nkeys,
                       cudaStream_t s);
+void radix_sort_pairs(unsigned *keys, uint2 *vals, unsigned *keys_tmp, uint2 *vals_tmp, int n, int key_bits,
+                      cudaStream_t s);
 
 namespace {
 
@@ -1299,6 +1301,216 @@ void validate_product(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     if (d.L_map) validate_compressed(nullptr, d.L_map, 0, INT_MAX, d.L_nnz, "product L_map", s);
 }
 
+// ------------------------------------------------------------ rows beyond the tile budget
+// Term counts and output counts of the big rows.
+__global__ void k_big_sizes(const int *__restrict__ rows, int nbig, const long long *__restrict__ ub,
+                            const int *__restrict__ Cp, long long *__restrict__ terms, long long *__restrict__ outs)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nbig;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        const int r = rows[i];
+        terms[i] = ub[r];
+        outs[i] = Cp[r + 1] - Cp[r];
+    }
+}
+
+// One CTA per big row at a time (grid-stride over the rows): every term of the row,
+// in upstream's visiting order t (stored at the row's term offset + t), gets the key
+// = its output's index among all big-row outputs and its {A position, entry-value
+// slot}. Output positions come from a per-CTA global map column -> position; only
+// the row's own columns are ever read, so it needs no clearing.
+__global__ void k_big_terms(const int *__restrict__ rows, int nbig, const int *__restrict__ tterm_off,
+                            const int *__restrict__ bout_off, NumArgs a, int *__restrict__ posmap_all, int n,
+                            unsigned *__restrict__ keys, uint2 *__restrict__ data)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    CtaChunk ch;
+    ch.v = nullptr;
+    ch.incl = reinterpret_cast<int *>(smraw);
+    ch.s = ch.incl + blockDim.x;
+    ch.len = ch.s + blockDim.x;
+    ch.scr = ch.len + blockDim.x;
+    int *posmap = posmap_all + (long long)blockIdx.x * n;
+    for (int it = blockIdx.x; it < nbig; it += gridDim.x)
+    {
+        const int row = rows[it];
+        const int b = row / a.L_m, r = row - b * a.L_m;
+        const int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
+        for (int q = threadIdx.x; q < nr; q += blockDim.x) posmap[a.Ci[cs + q]] = q;
+        __syncthreads();
+        const long long base = tterm_off[it];
+        long long cursor = 0;
+        const int ls = a.Lp[r], le = a.Lp[r + 1];
+        for (int c = ls; c < le; c += blockDim.x)
+        {
+            const int total = cta_load_chunk(a.Li, a.Ap, b, a.n_L, c, le, ch, nullptr, nullptr, nullptr, false);
+            const int nent = min((int)blockDim.x, le - c);
+            for (int u = threadIdx.x; u < total; u += blockDim.x)
+            {
+                const int e = cta_entry_of(ch.incl, nent, u);
+                const int jj = ch.s[e] + u - (ch.incl[e] - ch.len[e]);
+                const int ii = c + e;
+                const int pos = posmap[a.Ai[jj]];
+                const long long t = cursor + u;
+                const unsigned slot = (unsigned)(b * a.L_nnz + (a.value_order ? a.L_map[ii] : ii));
+                if (pos < 0 || pos >= nr)
+                {
+                    atomicOr(a.err, 1);
+                    continue;
+                }
+                keys[base + t] = (unsigned)(bout_off[it] + pos);
+                data[base + t] = make_uint2((unsigned)jj, slot);
+            }
+            cursor += total;
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+}
+
+// After the stable sort by output: the first pair of every output (every output
+// has a term, so each output index starts exactly one run).
+__global__ void k_big_starts(const unsigned *__restrict__ keys, int T, int O, int *__restrict__ ostart,
+                             int *__restrict__ err)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < T;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        const unsigned k = keys[i];
+        if (k >= (unsigned)O)
+        {
+            atomicOr(err, 1);
+            continue;
+        }
+        if (i == 0 || keys[i - 1] != k) ostart[k] = (int)i;
+    }
+}
+
+// Output-major refill of the big rows: a thread per output sums its pairs from +0.0
+// in upstream's visiting order (loads of four pairs in flight together). A CTA takes
+// 256 consecutive big outputs; its first row is found by a search, then each thread
+// steps forward over the rows its output is past.
+template <bool BATCHED>
+__global__ void __launch_bounds__(256) k_big_refill(const int *__restrict__ brows, int nbig,
+                                                    const int *__restrict__ bout_off, int nout,
+                                                    const int *__restrict__ bostart, const uint2 *__restrict__ pairs,
+                                                    const int *__restrict__ Cp, const ProdPtrs *__restrict__ vals_dev,
+                                                    ProdPtrs vals, const double *__restrict__ V, long long nV,
+                                                    long long nA, int *__restrict__ err)
+{
+    __shared__ int r_first;
+    ProdPtrs P = vals;
+    if (BATCHED) P = *vals_dev;
+    const double *Vp = (P.Lx || P.d) ? V : nullptr;
+    const int o_first = blockIdx.x * blockDim.x;
+    if (o_first >= nout) return;
+    if (threadIdx.x == 0)
+    {
+        int lo = 0, hi = nbig; // last row with bout_off <= o_first
+        while (hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (bout_off[mid] <= o_first)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        r_first = lo;
+    }
+    __syncthreads();
+    const int o = o_first + threadIdx.x;
+    if (o >= nout) return;
+    int r = r_first;
+    while (r + 1 < nbig && bout_off[r + 1] <= o) ++r;
+    const int cpos = Cp[brows[r]] + (o - bout_off[r]);
+    const int i0 = bostart[o], i1 = bostart[o + 1];
+    double acc = 0.0;
+    for (int i = i0; i < i1; i += 4)
+    {
+        double pr[4];
+        bool ok[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            ok[j] = false;
+            pr[j] = 0.0;
+            if (i + j < i1)
+            {
+                const uint2 q = pairs[i + j];
+                if ((long long)q.x < nA && (long long)q.y < nV)
+                {
+                    ok[j] = true;
+                    pr[j] = __dmul_rn(Vp ? Vp[q.y] : 1.0, P.Ax[q.x]);
+                }
+                else
+                    atomicOr(err, 1);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (ok[j]) acc = __dadd_rn(acc, pr[j]);
+    }
+    P.Cx[cpos] = acc;
+}
+
+// Output-major term lists of the rows beyond the tile budget (k_big_terms, a stable
+// radix sort by output, k_big_starts). Kept within 31-bit offsets; larger products
+// keep the CTA kernels.
+void build_big_lists(const ProductDesc &d, Product &P, const long long *ub, const NumArgs &na, cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    P.big_lists = false;
+    const int nbig = P.num_count[NUM_C2K] + P.num_count[NUM_C8K] + P.num_count[NUM_GMEM];
+    if (nbig == 0) return;
+    const int *rows = P.num_rows.get() + P.num_offset[NUM_C2K]; // classes C2K, C8K, GMEM are adjacent
+    DevBuf<long long> terms(nbig), outs(nbig), toff((size_t)nbig + 1), ooff((size_t)nbig + 1);
+    SDL_LAUNCH(k_big_sizes, grid_for(nbig, 256, rt.num_sms * 8), 256, 0, s, rows, nbig, ub, P.Cp.get(),
+               terms.get(), outs.get());
+    const long long T = exclusive_scan_i64(terms.get(), toff.get(), nbig, s);
+    const long long O = exclusive_scan_i64(outs.get(), ooff.get(), nbig, s);
+    if (T >= INT_MAX || O >= INT_MAX || T < O) return; // the CTA kernels handle them
+    // 32-bit copies of the offsets (the sort and the refill take int offsets)
+    std::vector<long long> ht((size_t)nbig + 1), ho((size_t)nbig + 1);
+    SDL_CUDA(cudaMemcpyAsync(ht.data(), toff.get(), ht.size() * sizeof(long long), cudaMemcpyDeviceToHost, s));
+    SDL_CUDA(cudaMemcpyAsync(ho.data(), ooff.get(), ho.size() * sizeof(long long), cudaMemcpyDeviceToHost, s));
+    SDL_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> hti(ht.begin(), ht.end()), hoi(ho.begin(), ho.end());
+    DevBuf<int> toff32 = DevBuf<int>((size_t)nbig + 1);
+    P.bout_off.reset((size_t)nbig + 1);
+    SDL_CUDA(cudaMemcpyAsync(toff32.get(), hti.data(), hti.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    SDL_CUDA(cudaMemcpyAsync(P.bout_off.get(), hoi.data(), hoi.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    // terms -> (output, pair), then a stable sort by output
+    const long long per_slot = std::max(1, P.n);
+    const int slots = (int)std::min<long long>({(long long)rt.num_sms, std::max<long long>(1, (2LL << 30) / (per_slot * 4)),
+                                                (long long)nbig});
+    {
+        DevBuf<int> posmap((size_t)slots * per_slot);
+        DevBuf<unsigned> keys(std::max<long long>(1, T)), keys2(std::max<long long>(1, T));
+        DevBuf<uint2> tmp(std::max<long long>(1, T));
+        P.bpairs.reset(std::max<long long>(1, T));
+        const int th = 512;
+        const size_t sm = (3 * (size_t)th + 32) * 4;
+        SDL_LAUNCH(k_big_terms, slots, th, sm, s, rows, nbig, toff32.get(), P.bout_off.get(), na, posmap.get(), P.n,
+                   keys.get(), P.bpairs.get());
+        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
+        int bits = 1;
+        while (bits < 32 && (1LL << bits) < O) ++bits;
+        radix_sort_pairs(keys.get(), P.bpairs.get(), keys2.get(), tmp.get(), (int)T, bits, s);
+        P.bostart.reset((size_t)O + 1);
+        SDL_CUDA(cudaMemcpyAsync(P.bostart.get() + O, &hti[nbig], sizeof(int), cudaMemcpyHostToDevice, s));
+        SDL_LAUNCH(k_big_starts, grid_for(T, 256, rt.num_sms * 8), 256, 0, s, keys.get(), (int)T, (int)O,
+                   P.bostart.get(), rt.d_error);
+        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: heavy-row term lists are inconsistent");
+    }
+    P.brows.reset(nbig);
+    SDL_CUDA(cudaMemcpyAsync(P.brows.get(), rows, (size_t)nbig * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    SDL_CUDA(cudaStreamSynchronize(s));
+    P.nbig = nbig;
+    P.big_outputs = (int)O;
+    P.big_lists = true;
+}
+
 // Everything the refill needs once C's structure is known: row classes, the
 // compiled tile schedule and the larger rows' scratch.
 void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
@@ -1364,7 +1576,8 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
                tile_start.get(), nullptr, nullptr, word_begin.get(), x_begin.get(), P.tiles.get(),
                P.W.get(), P.X.get(), P.ES.get());
     if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
-    if (P.num_count[NUM_GMEM])
+    build_big_lists(d, P, ub, na, s);
+    if (P.num_count[NUM_GMEM] && !P.big_lists)
     {
         long long per_slot = std::max(1, P.n);
         long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
@@ -1768,7 +1981,28 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
         entry_values(S, vals, s);
         tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S);
     }
-    big_rows_refill(P, Lx, dvec, Ax, Cx, s);
+    if (P.big_lists)
+    {
+        if (!P.num_count[NUM_TILE]) entry_values(sched_of(P), ProdPtrs{Lx, dvec, Ax, Cx}, s);
+        big_lists_refill(P, nullptr, s, ProdPtrs{Lx, dvec, Ax, Cx});
+    }
+    else
+        big_rows_refill(P, Lx, dvec, Ax, Cx, s);
+}
+
+void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs vals)
+{
+    if (!P.big_lists || P.big_outputs == 0) return;
+    const int grid = (P.big_outputs + 255) / 256;
+    const long long nV = (long long)P.desc.L_nnz * P.desc.blocks;
+    if (ptrs)
+        SDL_LAUNCH(k_big_refill<true>, grid, 256, 0, s, P.brows.get(), P.nbig, P.bout_off.get(), P.big_outputs,
+                   P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, P.V.get(), nV, (long long)P.desc.A_nnz,
+                   runtime().d_error);
+    else
+        SDL_LAUNCH(k_big_refill<false>, grid, 256, 0, s, P.brows.get(), P.nbig, P.bout_off.get(), P.big_outputs,
+                   P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, P.V.get(), nV, (long long)P.desc.A_nnz,
+                   runtime().d_error);
 }
 
 } // namespace sdl

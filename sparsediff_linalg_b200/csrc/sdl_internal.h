@@ -272,6 +272,14 @@ struct Product
     DevBuf<double> V;      // entry values of the current refill (L_nnz * blocks)
     DevBuf<int> gmem_scratch; // posmap scratch for NUM_GMEM rows (slots x n ints)
     int gmem_slots = 0;
+    // Rows beyond the tile budget, output-major: every output's terms as {A
+    // position, entry-value slot} pairs in upstream's visiting order (big_lists).
+    bool big_lists = false;
+    int nbig = 0, big_outputs = 0;
+    DevBuf<int> brows;          // the rows (big row i = brows[i])
+    DevBuf<int> bout_off;       // outputs of big rows before big row i (nbig + 1)
+    DevBuf<int> bostart;        // first pair of every big-row output (big_outputs + 1)
+    DevBuf<uint2> bpairs;       // the pairs
     TuneConfig cfg;
     // per-row statistics kept for the learned scheduler (optional)
     DevBuf<long long> row_terms; // ub per row
@@ -314,6 +322,9 @@ void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const 
                  cudaStream_t s, ProdPtrs vals = ProdPtrs{}, ProdSched sched = ProdSched{});
 // Copies `n` descriptors, setting `prod`.
 void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s);
+// The larger rows of one product from their output-major term lists (needs
+// P.big_lists), values as in tile_refill.
+void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs vals = ProdPtrs{});
 // The larger rows of one product (CTA kernels), for the given values; with `vals`
 // (a device ProdPtrs) the kernels read the value pointers from there instead.
 void big_rows_refill(const Product &P, const double *Lx, const double *d, const double *Ax,
