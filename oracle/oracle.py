@@ -99,6 +99,7 @@ def reference():
             "free_matrix": (None, [matrix_p]),
             "BTA_matrices_alloc": (matrix_p, [matrix_p, matrix_p]),
             "BTDA_matrices_fill_values": (None, [matrix_p, vp, matrix_p, matrix_p]),
+            "BTA_matrices_fill_values": (None, [matrix_p, matrix_p, matrix_p]),
             "BA_matrices_alloc": (matrix_p, [matrix_p, matrix_p]),
             "BA_matrices_fill_values": (None, [matrix_p, matrix_p, matrix_p]),
             "ATA_matrices_alloc": (matrix_p, [matrix_p]),

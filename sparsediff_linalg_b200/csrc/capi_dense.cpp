@@ -173,8 +173,145 @@ matrix *spd_copy_sparsity(const sdl_stacked *A)
     return C;
 }
 
-matrix *dense_BTA_alloc(matrix *, matrix *) { unsupported("BTA_matrices_alloc"); }
-void dense_BTDA_fill(matrix *, const double *, matrix *, matrix *) { unsupported("BTDA_matrices_fill_values"); }
+// BTA with B sparse and A permuted_dense / stacked_pd (upstream matmul_dispatchers.c:
+// 335-375 -> BTA_csc_pd_* / BTA_csc_spd_*): C = B^T diag(d) A, each block's partial
+// bit-identical to upstream's, coalesced as upstream's stacked_pd.
+namespace {
+struct BlockView
+{
+    std::vector<int> m0, n0;
+    std::vector<const int *> rp, cp;
+    int m = 0, n = 0;
+    const double *host_x = nullptr; // the blocks' values, block-major
+};
+BlockView blocks_of(const matrix *Am)
+{
+    BlockView v;
+    if (Am->kind == MATRIX_PERMUTED_DENSE)
+    {
+        const permuted_dense *A = as_pd(Am);
+        v.m0 = {A->m0};
+        v.n0 = {A->n0};
+        v.rp = {A->row_perm};
+        v.cp = {A->col_perm};
+        v.host_x = A->X;
+    }
+    else
+    {
+        const sdl_stacked *A = as_spd(Am);
+        for (int k = 0; k < A->n_blocks; ++k)
+        {
+            v.m0.push_back(A->blocks[k]->m0);
+            v.n0.push_back(A->blocks[k]->n0);
+            v.rp.push_back(A->blocks[k]->row_perm);
+            v.cp.push_back(A->blocks[k]->col_perm);
+        }
+        v.host_x = A->values;
+    }
+    v.m = Am->m;
+    v.n = Am->n;
+    return v;
+}
+} // namespace
+
+matrix *dense_BTA_alloc(matrix *Am, matrix *Bm)
+{
+    if (Bm->kind != MATRIX_SPARSE || (Am->kind != MATRIX_PERMUTED_DENSE && Am->kind != MATRIX_STACKED_PD))
+        unsupported("BTA_matrices_alloc");
+    sdl_sparse *B = as_sparse(Bm);
+    if (B->csr->m != Am->m) fail(SDL_ERR_INVALID, "BTA_matrices_alloc: B and A have different row counts");
+    cudaStream_t s = runtime().stream;
+    BlockView v = blocks_of(Am);
+    const int nb = (int)v.m0.size();
+    auto plan = blocks_btda_build(nb, v.m0.data(), v.n0.data(), v.rp.data(), v.cp.data(), v.m, v.n, B->csr->p,
+                                  B->csr->i, B->csr->n, s);
+    sparse_dev_values(B, s); // the device mirror of B's values exists before any fill
+    matrix *Cm = nullptr;
+    if (Am->kind == MATRIX_PERMUTED_DENSE)
+    {
+        // one block: rows = the columns of B that reach A's rows (upstream permuted_dense_linalg.c:646-672)
+        const std::vector<int> &act = plan->act[0];
+        const permuted_dense *A = as_pd(Am);
+        Cm = new_permuted_dense(B->csr->n, A->base.n, (int)act.size(), A->n0, act.empty() ? nullptr : act.data(),
+                                A->col_perm, nullptr);
+        if (!Cm) fail(SDL_ERR_INTERNAL, "BTA_matrices_alloc: output allocation failed");
+        permuted_dense *C = as_pd(Cm);
+        C->impl->bvals.reset((size_t)std::max<long long>(1, plan->x_total));
+        C->impl->cvals.reset((size_t)std::max<long long>(1, plan->c_total));
+        C->impl->dvec.reset((size_t)std::max(1, v.m));
+        C->impl->ata = std::move(plan);
+        SDL_CUDA(cudaStreamSynchronize(s));
+        return Cm;
+    }
+    const int no = plan->n_out;
+    permuted_dense **blocks = (permuted_dense **)sp_malloc(sizeof(permuted_dense *) * std::max(1, no));
+    std::vector<int> sp_p(1, 0), sp_i;
+    for (int o = 0; o < no; ++o)
+    {
+        const std::vector<int> &r = plan->out_rows[o], &c = plan->out_cols[o];
+        blocks[o] = as_pd(new_permuted_dense(B->csr->n, v.n, (int)r.size(), (int)c.size(), r.data(), c.data(), nullptr));
+        if (!blocks[o]) fail(SDL_ERR_INTERNAL, "BTA_matrices_alloc: output allocation failed");
+        sp_i.insert(sp_i.end(), plan->out_srcs[o].begin(), plan->out_srcs[o].end());
+        sp_p.push_back((int)sp_i.size());
+    }
+    if (sp_i.empty()) sp_i.push_back(0);
+    Cm = new_stacked_pd(B->csr->n, v.n, no, blocks, sp_p.data(), sp_i.data());
+    sp_free(blocks);
+    if (!Cm) fail(SDL_ERR_INTERNAL, "BTA_matrices_alloc: output allocation failed");
+    sdl_stacked *C = as_spd(Cm);
+    C->impl->xvals.reset((size_t)std::max<long long>(1, plan->x_total));
+    C->impl->cvals.reset((size_t)std::max<long long>(1, plan->c_total));
+    C->impl->dvec.reset((size_t)std::max(1, v.m));
+    C->impl->ata = std::move(plan);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    return Cm;
+}
+
+void dense_BTDA_fill(matrix *Am, const double *d, matrix *Bm, matrix *Cm)
+{
+    if (Bm->kind != MATRIX_SPARSE || Am->kind != Cm->kind ||
+        (Am->kind != MATRIX_PERMUTED_DENSE && Am->kind != MATRIX_STACKED_PD))
+        unsupported("BTDA_matrices_fill_values");
+    cudaStream_t s = runtime().stream;
+    const BlocksAtaPlan *P = nullptr;
+    DevBuf<double> *xv = nullptr, *cv = nullptr, *dv = nullptr;
+    double *hc = nullptr;
+    if (Cm->kind == MATRIX_PERMUTED_DENSE)
+    {
+        permuted_dense *C = as_pd(Cm);
+        P = C->impl ? C->impl->ata.get() : nullptr;
+        if (P)
+        {
+            xv = &C->impl->bvals;
+            cv = &C->impl->cvals;
+            dv = &C->impl->dvec;
+            hc = C->X;
+        }
+    }
+    else
+    {
+        sdl_stacked *C = as_spd(Cm);
+        P = C->impl ? C->impl->ata.get() : nullptr;
+        if (P)
+        {
+            xv = &C->impl->xvals;
+            cv = &C->impl->cvals;
+            dv = &C->impl->dvec;
+            hc = C->values;
+        }
+    }
+    if (!P || !P->btda) fail(SDL_ERR_INVALID, "BTDA_matrices_fill_values: C was not produced by BTA_matrices_alloc");
+    BlockView v = blocks_of(Am);
+    if (P->x_total != (long long)[&]() { long long t = 0; for (size_t k = 0; k < v.m0.size(); ++k) t += (long long)v.m0[k] * v.n0[k]; return t; }())
+        fail(SDL_ERR_INVALID, "BTDA_matrices_fill_values: A does not match the alloc");
+    h2d(xv->get(), v.host_x, (size_t)P->x_total, s);
+    if (d) h2d(dv->get(), d, (size_t)P->m, s);
+    const double *Bx = sparse_dev_values(as_sparse(Bm), s);
+    blocks_btda_fill(*P, xv->get(), d ? dv->get() : nullptr, Bx, cv->get(), s);
+    d2h(hc, cv->get(), (size_t)P->c_total, s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    matrix_values_changed(Cm);
+}
 // BA with B permuted_dense and A sparse (upstream matmul_dispatchers.c:197-223 ->
 // permuted_dense_linalg.c:313-430 BA_pd_csr_*): C is permuted_dense with B's
 // row_perm and the columns of S = A's CSR that B's col_perm rows reach.
@@ -285,7 +422,8 @@ void dense_ATDA_fill(const matrix *Am, const double *d, matrix *Cm)
     if (Am->kind == MATRIX_PERMUTED_DENSE && Cm->kind == MATRIX_PERMUTED_DENSE)
     {
         permuted_dense *C = as_pd(Cm);
-        if (!C->impl || !C->impl->ata) fail(SDL_ERR_INVALID, "ATDA_matrices_fill_values: C was not produced by ATA_matrices_alloc");
+        if (!C->impl || !C->impl->ata || C->impl->ata->btda)
+            fail(SDL_ERR_INVALID, "ATDA_matrices_fill_values: C was not produced by ATA_matrices_alloc");
         P = C->impl->ata.get();
         xv = &C->impl->bvals;
         cv = &C->impl->cvals;
@@ -296,7 +434,8 @@ void dense_ATDA_fill(const matrix *Am, const double *d, matrix *Cm)
     else if (Am->kind == MATRIX_STACKED_PD && Cm->kind == MATRIX_STACKED_PD)
     {
         sdl_stacked *C = as_spd(Cm);
-        if (!C->impl || !C->impl->ata) fail(SDL_ERR_INVALID, "ATDA_matrices_fill_values: C was not produced by ATA_matrices_alloc");
+        if (!C->impl || !C->impl->ata || C->impl->ata->btda)
+            fail(SDL_ERR_INVALID, "ATDA_matrices_fill_values: C was not produced by ATA_matrices_alloc");
         P = C->impl->ata.get();
         xv = &C->impl->xvals;
         cv = &C->impl->cvals;

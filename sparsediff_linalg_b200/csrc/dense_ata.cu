@@ -88,6 +88,51 @@ __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ m
             }
 }
 
+// One warp per (block k, active column c of B): row c of the partial,
+// P_k[c, j] = sum over B's column c (CSC order, rows of block k only) of
+// B.x * (d[row] * X_k[kk, j]) -- upstream's two roundings -- or B.x * X_k[kk, j]
+// without d, from +0.0. Lanes take the columns j of the block.
+__global__ void __launch_bounds__(256) k_btda_partials(const int2 *__restrict__ wtask, int nwt,
+                                                       const int *__restrict__ ent_off, const int *__restrict__ ent_kk,
+                                                       const int *__restrict__ ent_pos,
+                                                       const long long *__restrict__ x_off,
+                                                       const long long *__restrict__ p_off,
+                                                       const int *__restrict__ m0d, const int *__restrict__ n0d,
+                                                       const int *__restrict__ rowperm_all,
+                                                       const long long *__restrict__ rowperm_off,
+                                                       const double *__restrict__ X_vals, const double *__restrict__ d,
+                                                       const double *__restrict__ Bx, int B_nnz,
+                                                       double *__restrict__ P, int *__restrict__ err)
+{
+    const int t = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (t >= nwt) return;
+    const int lane = threadIdx.x & 31;
+    const int2 wt = wtask[t];
+    const int k = wt.x, a = wt.y;
+    const int m0 = m0d[k], n0 = n0d[k];
+    const double *X = X_vals + x_off[k];
+    const int *rp = rowperm_all + rowperm_off[k];
+    const int e0 = ent_off[t], e1 = ent_off[t + 1];
+    double *Pk = P + p_off[k] + (long long)a * n0;
+    for (int j = lane; j < n0; j += 32)
+    {
+        double acc = 0.0;
+        for (int e = e0; e < e1; ++e)
+        {
+            const int kk = ent_kk[e], pos = ent_pos[e];
+            if (kk < 0 || kk >= m0 || pos < 0 || pos >= B_nnz)
+            {
+                atomicOr(err, 1);
+                continue;
+            }
+            const double x = X[(long long)kk * n0 + j];
+            const double w = d ? __dmul_rn(d[rp[kk]], x) : x;
+            acc = __dadd_rn(acc, __dmul_rn(Bx[pos], w));
+        }
+        Pk[j] = acc;
+    }
+}
+
 // Output cells: the partials that hold the cell, summed from +0.0 in block order.
 __global__ void k_ata_gather(const BlocksAtaPlan::OutDesc *__restrict__ outd, int o_base,
                              const int *__restrict__ srcs, const int *__restrict__ maps,
@@ -114,6 +159,74 @@ __global__ void k_ata_gather(const BlocksAtaPlan::OutDesc *__restrict__ outd, in
 }
 
 } // namespace
+
+// Upstream's coalescing of per-block partials (src/stacked_pd/stacked_pd_coalesce.c:
+// 150-381): partial k covers rows prow[k] x columns pcol[k] (both ascending) of a
+// nrows x ncols result. The signature of a row is the list of partials holding it,
+// in partial order; rows with the same signature form one output block (blocks in
+// order of first appearance scanning rows ascending), whose columns are the union
+// of those partials' columns. Fills the output blocks of P and, per output block
+// and contributing partial, its row and column maps (-1: absent).
+void coalesce_partials(const std::vector<std::vector<int>> &prow, const std::vector<std::vector<int>> &pcol,
+                       int nrows, int ncols, BlocksAtaPlan &P, std::vector<BlocksAtaPlan::OutDesc> &od,
+                       std::vector<int> &h_srcs, std::vector<int> &h_maps)
+{
+    const int n_src = (int)prow.size();
+    std::vector<std::vector<int>> row_blocks(std::max(1, nrows));
+    for (int k = 0; k < n_src; ++k)
+        for (int r : prow[k]) row_blocks[r].push_back(k);
+    std::map<std::vector<int>, int> sig_id;
+    P.out_rows.clear();
+    P.out_cols.clear();
+    P.out_srcs.clear();
+    for (int r = 0; r < nrows; ++r)
+    {
+        if (row_blocks[r].empty()) continue;
+        auto it = sig_id.find(row_blocks[r]);
+        int sid;
+        if (it == sig_id.end())
+        {
+            sid = (int)P.out_rows.size();
+            sig_id.emplace(row_blocks[r], sid);
+            P.out_rows.emplace_back();
+            P.out_srcs.push_back(row_blocks[r]);
+        }
+        else
+            sid = it->second;
+        P.out_rows[sid].push_back(r);
+    }
+    P.n_out = (int)P.out_rows.size();
+    P.c_total = 0;
+    std::vector<int> rpos(std::max(1, nrows), -1), cpos(std::max(1, ncols), -1);
+    for (int o = 0; o < P.n_out; ++o)
+    {
+        std::vector<int> cols;
+        for (int k : P.out_srcs[o]) cols.insert(cols.end(), pcol[k].begin(), pcol[k].end());
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        P.out_cols.push_back(cols);
+        BlocksAtaPlan::OutDesc D{};
+        D.c_off = P.c_total;
+        D.m0 = (int)P.out_rows[o].size();
+        D.n0 = (int)cols.size();
+        if ((long long)D.m0 * D.n0 > INT_MAX) fail(SDL_ERR_OVERFLOW, "dense blocks: output block exceeds INT_MAX values");
+        D.s_begin = (int)h_srcs.size();
+        D.map_off = (long long)h_maps.size();
+        for (int k : P.out_srcs[o])
+        {
+            h_srcs.push_back(k);
+            for (size_t q = 0; q < prow[k].size(); ++q) rpos[prow[k][q]] = (int)q;
+            for (size_t q = 0; q < pcol[k].size(); ++q) cpos[pcol[k][q]] = (int)q;
+            for (int r : P.out_rows[o]) h_maps.push_back(rpos[r]);
+            for (int c : cols) h_maps.push_back(cpos[c]);
+            for (int r : prow[k]) rpos[r] = -1;
+            for (int c : pcol[k]) cpos[c] = -1;
+        }
+        D.s_end = (int)h_srcs.size();
+        od.push_back(D);
+        P.c_total += (long long)D.m0 * D.n0;
+    }
+}
 
 std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const int *n0,
                                                 const int *const *row_perm, const int *const *col_perm,
@@ -146,59 +259,16 @@ std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const 
         for (int a = 0; a < n0[k]; a += 16)
             for (int b = 0; b < n0[k]; b += 16) mt.push_back(make_int4(k, a, b, 0));
     }
-    // upstream's coalescing of the partials (row_perm = col_perm = col_perm_k):
-    // signature of column r = the blocks whose col_perm holds r, in block order;
-    // output blocks in order of first appearance scanning r ascending
-    std::vector<std::vector<int>> row_blocks(std::max(1, n));
+    // upstream's coalescing of the partials (row_perm = col_perm = col_perm_k)
+    std::vector<std::vector<int>> prow(n_src), pcol(n_src);
     for (int k = 0; k < n_src; ++k)
-        for (int c = 0; c < n0[k]; ++c) row_blocks[col_perm[k][c]].push_back(k);
-    std::map<std::vector<int>, int> sig_id;
-    for (int r = 0; r < n; ++r)
     {
-        if (row_blocks[r].empty()) continue;
-        auto it = sig_id.find(row_blocks[r]);
-        int sid;
-        if (it == sig_id.end())
-        {
-            sid = (int)P->out_rows.size();
-            sig_id.emplace(row_blocks[r], sid);
-            P->out_rows.emplace_back();
-            P->out_srcs.push_back(row_blocks[r]);
-        }
-        else
-            sid = it->second;
-        P->out_rows[sid].push_back(r);
+        prow[k].assign(col_perm[k], col_perm[k] + n0[k]);
+        pcol[k] = prow[k];
     }
-    P->n_out = (int)P->out_rows.size();
     std::vector<BlocksAtaPlan::OutDesc> od;
     std::vector<int> h_srcs, h_maps;
-    std::vector<int> pos(std::max(1, n), -1);
-    for (int o = 0; o < P->n_out; ++o)
-    {
-        std::vector<int> cols;
-        for (int k : P->out_srcs[o]) cols.insert(cols.end(), col_perm[k], col_perm[k] + n0[k]);
-        std::sort(cols.begin(), cols.end());
-        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-        P->out_cols.push_back(cols);
-        BlocksAtaPlan::OutDesc D{};
-        D.c_off = P->c_total;
-        D.m0 = (int)P->out_rows[o].size();
-        D.n0 = (int)cols.size();
-        if ((long long)D.m0 * D.n0 > INT_MAX) fail(SDL_ERR_OVERFLOW, "blocks A^T D A: output block exceeds INT_MAX values");
-        D.s_begin = (int)h_srcs.size();
-        D.map_off = (long long)h_maps.size();
-        for (int k : P->out_srcs[o])
-        {
-            h_srcs.push_back(k);
-            for (int c = 0; c < n0[k]; ++c) pos[col_perm[k][c]] = c;
-            for (int r : P->out_rows[o]) h_maps.push_back(pos[r]);
-            for (int c : cols) h_maps.push_back(pos[c]);
-            for (int c = 0; c < n0[k]; ++c) pos[col_perm[k][c]] = -1;
-        }
-        D.s_end = (int)h_srcs.size();
-        od.push_back(D);
-        P->c_total += (long long)D.m0 * D.n0;
-    }
+    coalesce_partials(prow, pcol, n, n, *P, od, h_srcs, h_maps);
     P->x_off = upload(x_off.data(), x_off.size(), s);
     P->p_off = upload(p_off.data(), p_off.size(), s);
     P->m0d = upload(h_m0.data(), h_m0.size(), s);
@@ -226,6 +296,138 @@ void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double 
     long long maxcells = 0;
     // grid.x covers the largest output block; grid.y = output blocks
     // (cells of block o: P.out_rows[o].size() * P.out_cols[o].size())
+    for (int o = 0; o < P.n_out; ++o)
+        maxcells = std::max(maxcells, (long long)P.out_rows[o].size() * (long long)P.out_cols[o].size());
+    for (int o = 0; o < P.n_out; o += 65535)
+    {
+        const dim3 grid(grid_cap2(maxcells, 256, 4096), (unsigned)std::min(65535, P.n_out - o));
+        SDL_LAUNCH(k_ata_gather, grid, 256, 0, s, P.outd.get(), o, P.srcs.get(), P.maps.get(), P.p_off.get(),
+                   P.n0d.get(), P.P.get(), C_vals);
+    }
+}
+
+std::unique_ptr<BlocksAtaPlan> blocks_btda_build(int n_src, const int *m0, const int *n0,
+                                                 const int *const *row_perm, const int *const *col_perm, int m,
+                                                 int n, const int *Bp, const int *Bi, int nB, cudaStream_t s)
+{
+    if (n_src < 0 || m < 0 || n < 0 || nB < 0) fail(SDL_ERR_INVALID, "B^T D A (dense blocks): negative size");
+    auto P = std::make_unique<BlocksAtaPlan>();
+    P->btda = true;
+    P->m = m;
+    P->n = n;
+    P->nB = nB;
+    P->n_src = n_src;
+    P->B_nnz = m ? Bp[m] : 0;
+    // row -> (block, local row); a stacked_pd's blocks own disjoint rows
+    std::vector<int> rb(std::max(1, m), -1), rl(std::max(1, m), -1);
+    std::vector<long long> x_off(std::max(1, n_src)), p_off(std::max(1, n_src)), rp_off(std::max(1, n_src));
+    std::vector<int> h_m0(std::max(1, n_src)), h_n0(std::max(1, n_src)), h_rp;
+    for (int k = 0; k < n_src; ++k)
+    {
+        if (m0[k] < 0 || n0[k] < 0) fail(SDL_ERR_INVALID, "B^T D A (dense blocks): negative block shape");
+        for (int r = 0; r < m0[k]; ++r)
+        {
+            const int row = row_perm[k][r];
+            if (row < 0 || row >= m) fail(SDL_ERR_INVALID, "B^T D A (dense blocks): row_perm out of range");
+            if (rb[row] >= 0) fail(SDL_ERR_INVALID, "B^T D A (dense blocks): two blocks share a row");
+            rb[row] = k;
+            rl[row] = r;
+        }
+        for (int c = 0; c < n0[k]; ++c)
+            if (col_perm[k][c] < 0 || col_perm[k][c] >= n || (c && col_perm[k][c] <= col_perm[k][c - 1]))
+                fail(SDL_ERR_INVALID, "B^T D A (dense blocks): col_perm is not strictly increasing columns");
+        x_off[k] = P->x_total;
+        rp_off[k] = (long long)h_rp.size();
+        h_m0[k] = m0[k];
+        h_n0[k] = n0[k];
+        h_rp.insert(h_rp.end(), row_perm[k], row_perm[k] + m0[k]);
+        P->x_total += (long long)m0[k] * n0[k];
+    }
+    // B's entries column by column, rows ascending (its CSC order), with CSR positions
+    std::vector<int> ccnt((size_t)nB + 1, 0);
+    for (int i = 0; i < m; ++i)
+        for (int q = Bp[i]; q < Bp[i + 1]; ++q)
+        {
+            if (Bi[q] < 0 || Bi[q] >= nB) fail(SDL_ERR_INVALID, "B^T D A (dense blocks): column index of B out of range");
+            ccnt[Bi[q] + 1]++;
+        }
+    for (int c = 0; c < nB; ++c) ccnt[c + 1] += ccnt[c];
+    std::vector<int> crow((size_t)std::max(1, P->B_nnz)), cpos((size_t)std::max(1, P->B_nnz));
+    {
+        std::vector<int> nx(ccnt.begin(), ccnt.end() - 1);
+        for (int i = 0; i < m; ++i)
+            for (int q = Bp[i]; q < Bp[i + 1]; ++q)
+            {
+                const int e = nx[Bi[q]]++;
+                crow[e] = i;
+                cpos[e] = q;
+            }
+    }
+    // per block: the active columns of B and their entries
+    P->act.assign(n_src, {});
+    std::vector<std::vector<int>> ekk(n_src), epos(n_src), eoff(n_src);
+    for (int c = 0; c < nB; ++c)
+        for (int e = ccnt[c]; e < ccnt[c + 1]; ++e)
+        {
+            const int k = rb[crow[e]];
+            if (k < 0) continue;
+            if (P->act[k].empty() || P->act[k].back() != c)
+            {
+                P->act[k].push_back(c);
+                eoff[k].push_back((int)ekk[k].size());
+            }
+            ekk[k].push_back(rl[crow[e]]);
+            epos[k].push_back(cpos[e]);
+        }
+    std::vector<int2> wt;
+    std::vector<int> h_off(1, 0), h_kk, h_pos;
+    for (int k = 0; k < n_src; ++k)
+    {
+        p_off[k] = P->p_total;
+        P->p_total += (long long)P->act[k].size() * n0[k];
+        eoff[k].push_back((int)ekk[k].size());
+        for (size_t a = 0; a < P->act[k].size(); ++a)
+        {
+            wt.push_back(make_int2(k, (int)a));
+            h_kk.insert(h_kk.end(), ekk[k].begin() + eoff[k][a], ekk[k].begin() + eoff[k][a + 1]);
+            h_pos.insert(h_pos.end(), epos[k].begin() + eoff[k][a], epos[k].begin() + eoff[k][a + 1]);
+            h_off.push_back((int)h_kk.size());
+        }
+    }
+    // upstream's coalescing of the partials (rows = active columns of B, columns = col_perm_k)
+    std::vector<std::vector<int>> pcol(n_src);
+    for (int k = 0; k < n_src; ++k) pcol[k].assign(col_perm[k], col_perm[k] + n0[k]);
+    std::vector<BlocksAtaPlan::OutDesc> od;
+    std::vector<int> h_srcs, h_maps;
+    coalesce_partials(P->act, pcol, nB, n, *P, od, h_srcs, h_maps);
+    P->x_off = upload(x_off.data(), x_off.size(), s);
+    P->p_off = upload(p_off.data(), p_off.size(), s);
+    P->m0d = upload(h_m0.data(), h_m0.size(), s);
+    P->n0d = upload(h_n0.data(), h_n0.size(), s);
+    P->rowperm_all = upload(h_rp.data(), std::max<size_t>(1, h_rp.size()), s);
+    P->rowperm_off = upload(rp_off.data(), rp_off.size(), s);
+    P->P.reset((size_t)std::max<long long>(1, P->p_total));
+    P->nwtask = (int)wt.size();
+    P->wtask = upload(wt.data(), std::max<size_t>(1, wt.size()), s);
+    P->ent_off = upload(h_off.data(), h_off.size(), s);
+    P->ent_kk = upload(h_kk.data(), std::max<size_t>(1, h_kk.size()), s);
+    P->ent_pos = upload(h_pos.data(), std::max<size_t>(1, h_pos.size()), s);
+    P->outd = upload(od.data(), std::max<size_t>(1, od.size()), s);
+    P->srcs = upload(h_srcs.data(), std::max<size_t>(1, h_srcs.size()), s);
+    P->maps = upload(h_maps.data(), std::max<size_t>(1, h_maps.size()), s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    return P;
+}
+
+void blocks_btda_fill(const BlocksAtaPlan &P, const double *X_vals, const double *d, const double *B_x,
+                      double *C_vals, cudaStream_t s)
+{
+    if (P.c_total == 0) return;
+    if (P.nwtask > 0)
+        SDL_LAUNCH(k_btda_partials, (P.nwtask + 7) / 8, 256, 0, s, P.wtask.get(), P.nwtask, P.ent_off.get(),
+                   P.ent_kk.get(), P.ent_pos.get(), P.x_off.get(), P.p_off.get(), P.m0d.get(), P.n0d.get(),
+                   P.rowperm_all.get(), P.rowperm_off.get(), X_vals, d, B_x, P.B_nnz, P.P.get(), runtime().d_error);
+    long long maxcells = 0;
     for (int o = 0; o < P.n_out; ++o)
         maxcells = std::max(maxcells, (long long)P.out_rows[o].size() * (long long)P.out_cols[o].size());
     for (int o = 0; o < P.n_out; o += 65535)

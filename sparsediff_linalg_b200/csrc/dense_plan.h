@@ -99,6 +99,13 @@ struct BlocksAtaPlan
     DevBuf<int> srcs;   // source block ids
     DevBuf<int> maps;   // per (output block, source): m0 row positions, n0 column positions (-1: absent)
     int n_out = 0;
+    // B^T diag(d) A_k partials (blocks_btda_build): one warp task per (block, active
+    // column of B); its entries (block row, position in B's CSR values) in B's CSC order
+    bool btda = false;
+    int nB = 0, B_nnz = 0, nwtask = 0;
+    std::vector<std::vector<int>> act; // per block: the columns of B that reach its rows (host)
+    DevBuf<int2> wtask;                // (block, index of the active column)
+    DevBuf<int> ent_off, ent_kk, ent_pos;
 };
 
 std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const int *n0,
@@ -108,5 +115,19 @@ std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const 
 // (blocks in order, row-major) and d (m values, or null for the identity).
 void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double *d, double *C_vals,
                      cudaStream_t s);
+
+// B^T diag(d) A for B sparse (m x nB, host CSR structure) and A dense blocks (rows
+// row_perm[k] of m, pairwise disjoint; columns col_perm[k] of n): per block the
+// partial B^T diag(d) A_k over the columns of B that reach its rows (upstream
+// BTA_csc_pd_* / BTDA_csc_pd_*, src/permuted_dense/permuted_dense_linalg.c:646-741,
+// each output a sum over B's column in CSC order from +0.0: bit-identical), then
+// upstream's coalescing (BTA_csc_spd_* / BTDA_csc_spd_*, src/stacked_pd/
+// stacked_pd_linalg.c:594-608).
+std::unique_ptr<BlocksAtaPlan> blocks_btda_build(int n_src, const int *m0, const int *n0,
+                                                 const int *const *row_perm, const int *const *col_perm, int m,
+                                                 int n, const int *Bp, const int *Bi, int nB, cudaStream_t s);
+// C values from the blocks' values, d (or null: B^T A) and B's CSR values (device).
+void blocks_btda_fill(const BlocksAtaPlan &P, const double *X_vals, const double *d, const double *B_x,
+                      double *C_vals, cudaStream_t s);
 
 } // namespace sdl

@@ -278,3 +278,88 @@ def test_ATDA_permuted_dense_matches_upstream_library(sdl, orc):
     _close(gx, wx, scale, "ATDA permuted_dense")
     ref.free_matrix(Cr)
     ref.free_matrix(Ar)
+
+
+# ---------------------------------------------------------------- B^T diag(d) A, B sparse, A dense blocks
+@pytest.mark.parametrize("kind", ["pd", "spd"])
+@pytest.mark.parametrize("use_d", [True, False])
+def test_BTDA_sparse_dense_matches_upstream_library(sdl, orc, kind, use_d):
+    """BTA_matrices_alloc / BTDA_matrices_fill_values (BTA without d) with B sparse and
+    A permuted_dense or stacked_pd, through the drop-in C ABI, against the upstream
+    library: identical structure (the columns of B that reach each block, coalesced
+    as upstream's stacked_pd) and bit-identical values; then a refill."""
+    if not orc.reference_available():
+        pytest.skip("upstream library not built")
+    from sparsediff_linalg_b200 import matrices as M
+    ref = orc.reference()
+    rng = np.random.default_rng(97 + (kind == "spd") + 2 * use_d)
+    m, n, nB = 220, 40, 150
+    B = wl.small_random_csr(m, nB, 0.04, rng)
+    if kind == "pd":
+        blocks = [(rng.standard_normal((60, 25)), np.sort(rng.choice(m, 60, replace=False)).astype(np.int32),
+                   np.sort(rng.choice(n, 25, replace=False)).astype(np.int32))]
+    else:
+        blocks = _spd_blocks(rng, m, n, [(30, 12), (50, 40), (7, 5), (45, 22)])
+    d = rng.uniform(0.1, 10, m)
+
+    def ref_sparse(csr):
+        p, i, x, mm, nn = csr
+        c = ref.new_CSR_matrix(mm, nn, len(i))
+        st = c.contents
+        np.ctypeslib.as_array(st.p, shape=(mm + 1,))[:] = p
+        np.ctypeslib.as_array(st.i, shape=(max(1, len(i)),))[:len(i)] = i
+        np.ctypeslib.as_array(st.x, shape=(max(1, len(i)),))[:len(i)] = x
+        return ref.new_sparse_matrix(c)
+
+    def ref_dense(blks):
+        hs = []
+        for X, rp, cp in blks:
+            Xc = np.ascontiguousarray(X)
+            hs.append(ref.new_permuted_dense(m, n, len(rp), len(cp), rp.ctypes.data, cp.ctypes.data, Xc.ctypes.data))
+        if kind == "pd":
+            return hs[0]
+        arr = (C.c_void_p * len(hs))(*[C.cast(h, C.c_void_p) for h in hs])
+        return ref.new_stacked_pd(m, n, len(hs), arr, None, None)
+
+    def mine(blks):
+        pds = [M.permuted_dense(m, n, rp, cp, X) for X, rp, cp in blks]
+        return pds[0] if kind == "pd" else M.stacked_pd(m, n, pds)
+
+    Br, Ar = ref_sparse(B), ref_dense(blocks)
+    Cr = ref.BTA_matrices_alloc(Ar, Br)
+    dd = np.ascontiguousarray(d)
+    def fill_ref(A_, dv, B_, C_):
+        if use_d:
+            ref.BTDA_matrices_fill_values(A_, dv.ctypes.data, B_, C_)
+        else:
+            ref.BTA_matrices_fill_values(A_, B_, C_)
+
+    def fill_mine(A_, dv, B_, C_):
+        if use_d:
+            M.BTDA_fill(A_, dv, B_, C_)
+        else:
+            M.mlib().BTA_matrices_fill_values(A_.ptr, B_.ptr, C_.ptr)
+
+    fill_ref(Ar, dd, Br, Cr)
+    want = _ref_csr(ref, Cr)[:3]
+    Bm, Am = M.SparseMatrix.from_csr(*B), mine(blocks)
+    Cm = M.BTA(Am, Bm)
+    fill_mine(Am, d, Bm, Cm)
+    got = Cm.csr()
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    assert np.array_equal(bits(got[2]), bits(want[2]))
+    # refill with new values of A, B and d
+    X2 = [rng.standard_normal(X.shape) for X, _, _ in blocks]
+    bx = rng.standard_normal(len(B[1]))
+    d2 = rng.uniform(0.1, 10, m)
+    Am.set_values(np.concatenate([x.ravel() for x in X2]))
+    Bm.set_values(bx)
+    fill_mine(Am, d2, Bm, Cm)
+    Br2 = ref_sparse((B[0], B[1], bx, B[3], B[4]))
+    Ar2 = ref_dense([(x, rp, cp) for x, (_, rp, cp) in zip(X2, blocks)])
+    Cr2 = ref.BTA_matrices_alloc(Ar2, Br2)
+    fill_ref(Ar2, np.ascontiguousarray(d2), Br2, Cr2)
+    want2 = _ref_csr(ref, Cr2)[:3]
+    assert np.array_equal(bits(Cm.csr()[2]), bits(want2[2]))
+    for h in (Cr, Ar, Br, Cr2, Ar2, Br2):
+        ref.free_matrix(h)
