@@ -106,6 +106,10 @@ def reference():
             "ATDA_matrices_fill_values": (None, [matrix_p, vp, matrix_p]),
             "new_permuted_dense": (matrix_p, [C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
             "new_stacked_pd": (matrix_p, [C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+            "copy_sparsity_matrices_alloc": (matrix_p, [matrix_p]),
+            "transpose_matrices_alloc": (matrix_p, [matrix_p]),
+            "transpose_matrices_fill_values": (None, [matrix_p, matrix_p]),
+            "DA_matrices_fill_values": (None, [vp, matrix_p, matrix_p]),
             # internal upstream entry points (src/internal/stacked_pd_linalg.h)
             "BA_spd_csr_alloc": (matrix_p, [matrix_p, CSR_p]),
             "BA_spd_csr_fill_values": (None, [matrix_p, CSR_p, matrix_p]),

@@ -5,28 +5,13 @@
 #include <cstring>
 
 #include "capi_common.h"
-#include "dense_plan.h"
-#include "matrix_kinds.h"
+#include "dense_impl.h"
 #include "sparsediff_linalg/matrix.h"
 #include "sparsediff_linalg/tracked_alloc.h"
 
 namespace sdl {
 
-// Device state bound to a permuted_dense produced by BA_matrices_alloc (B pd,
-// A sparse): the product plan and the device copies of B's and C's values.
-struct PdImpl
-{
-    std::unique_ptr<BlocksCsrPlan> ba;  // bound by BA_matrices_alloc (B pd, A sparse)
-    std::unique_ptr<BlocksAtaPlan> ata; // bound by ATA_matrices_alloc (A pd)
-    DevBuf<double> bvals, cvals, dvec;
-};
 const double *sparse_dev_values(sdl_sparse *A, cudaStream_t s);
-// Device state bound to a stacked_pd produced by ATA_matrices_alloc (A spd).
-struct SpdImpl
-{
-    std::unique_ptr<BlocksAtaPlan> ata;
-    DevBuf<double> xvals, cvals, dvec;
-};
 
 namespace {
 
@@ -60,33 +45,14 @@ CSR_matrix *pd_to_csr(matrix *self)
     return pd->csr_cache;
 }
 
-matrix *unsupported_gather(const matrix *, const int *, int)
-{
-    return guard_upstream<matrix *>("row_gather_alloc", nullptr, []() -> matrix * {
-        fail(SDL_ERR_UNSUPPORTED, "row_gather of dense-block kinds is not provided by this build");
-    });
-}
-void unsupported_fill(const matrix *, matrix *)
-{
-    guard_upstream_void("fill", []() {
-        fail(SDL_ERR_UNSUPPORTED, "operation not provided by this build for dense-block kinds");
-    });
-}
-matrix *unsupported_reduce(const matrix *, const int *, int)
-{
-    return guard_upstream<matrix *>("row_reduce_alloc", nullptr, []() -> matrix * {
-        fail(SDL_ERR_UNSUPPORTED, "row_reduce of dense-block kinds is not provided by this build");
-    });
-}
-
 void wire_pd(permuted_dense *pd)
 {
     pd->base.kind = MATRIX_PERMUTED_DENSE;
     pd->base.to_csr = pd_to_csr;
-    pd->base.row_gather_alloc = unsupported_gather;
-    pd->base.row_gather_fill_values = unsupported_fill;
-    pd->base.row_reduce_alloc = unsupported_reduce;
-    pd->base.row_reduce_fill_values = unsupported_fill;
+    pd->base.row_gather_alloc = pd_row_gather_alloc;
+    pd->base.row_gather_fill_values = dense_rows_fill;
+    pd->base.row_reduce_alloc = pd_row_reduce_alloc;
+    pd->base.row_reduce_fill_values = dense_rows_fill;
 }
 
 CSR_matrix *spd_to_csr(matrix *self)
@@ -116,10 +82,10 @@ void wire_spd(sdl_stacked *spd)
 {
     spd->base.kind = MATRIX_STACKED_PD;
     spd->base.to_csr = spd_to_csr;
-    spd->base.row_gather_alloc = unsupported_gather;
-    spd->base.row_gather_fill_values = unsupported_fill;
-    spd->base.row_reduce_alloc = unsupported_reduce;
-    spd->base.row_reduce_fill_values = unsupported_fill;
+    spd->base.row_gather_alloc = spd_row_gather_alloc;
+    spd->base.row_gather_fill_values = dense_rows_fill;
+    spd->base.row_reduce_alloc = spd_row_reduce_alloc;
+    spd->base.row_reduce_fill_values = dense_rows_fill;
 }
 
 [[noreturn]] void unsupported(const char *what)
@@ -167,8 +133,8 @@ matrix *spd_copy_sparsity(const sdl_stacked *A)
 {
     permuted_dense **blocks = (permuted_dense **)sp_malloc(sizeof(permuted_dense *) * std::max(1, A->n_blocks));
     for (int k = 0; k < A->n_blocks; ++k) blocks[k] = as_pd(pd_copy_sparsity(A->blocks[k]));
-    matrix *C = new_stacked_pd(A->base.m, A->base.n, A->n_blocks, blocks, A->src_block_idx_p,
-                               A->src_block_idx);
+    // identity source map (upstream stacked_pd_linalg.c:34-47 passes NULL)
+    matrix *C = new_stacked_pd(A->base.m, A->base.n, A->n_blocks, blocks, nullptr, nullptr);
     sp_free(blocks);
     return C;
 }
@@ -216,8 +182,8 @@ BlockView blocks_of(const matrix *Am)
 
 matrix *dense_BTA_alloc(matrix *Am, matrix *Bm)
 {
-    if (Bm->kind != MATRIX_SPARSE || (Am->kind != MATRIX_PERMUTED_DENSE && Am->kind != MATRIX_STACKED_PD))
-        unsupported("BTA_matrices_alloc");
+    if (Bm->kind != MATRIX_SPARSE) return prog_BTA_alloc(Am, Bm);
+    if (Am->kind != MATRIX_PERMUTED_DENSE && Am->kind != MATRIX_STACKED_PD) unsupported("BTA_matrices_alloc");
     sdl_sparse *B = as_sparse(Bm);
     if (B->csr->m != Am->m) fail(SDL_ERR_INVALID, "BTA_matrices_alloc: B and A have different row counts");
     cudaStream_t s = runtime().stream;
@@ -269,6 +235,11 @@ matrix *dense_BTA_alloc(matrix *Am, matrix *Bm)
 
 void dense_BTDA_fill(matrix *Am, const double *d, matrix *Bm, matrix *Cm)
 {
+    if (ProgState *ps = prog_state(Cm); ps && ps->op == DP_OP_BTA)
+    {
+        prog_product_fill(Bm, d, Am, Cm, DP_OP_BTA);
+        return;
+    }
     if (Bm->kind != MATRIX_SPARSE || Am->kind != Cm->kind ||
         (Am->kind != MATRIX_PERMUTED_DENSE && Am->kind != MATRIX_STACKED_PD))
         unsupported("BTDA_matrices_fill_values");
@@ -317,7 +288,7 @@ void dense_BTDA_fill(matrix *Am, const double *d, matrix *Bm, matrix *Cm)
 // row_perm and the columns of S = A's CSR that B's col_perm rows reach.
 matrix *dense_BA_alloc(const matrix *Bm, matrix *Am)
 {
-    if (Bm->kind != MATRIX_PERMUTED_DENSE || Am->kind != MATRIX_SPARSE) unsupported("BA_matrices_alloc");
+    if (Bm->kind != MATRIX_PERMUTED_DENSE || Am->kind != MATRIX_SPARSE) return prog_BA_alloc(Bm, Am);
     const permuted_dense *B = as_pd(Bm);
     sdl_sparse *A = as_sparse(Am);
     cudaStream_t s = runtime().stream;
@@ -339,6 +310,11 @@ matrix *dense_BA_alloc(const matrix *Bm, matrix *Am)
 
 void dense_BA_fill(const matrix *Bm, const matrix *Am, matrix *Cm)
 {
+    if (ProgState *ps = prog_state(Cm); ps && ps->op == DP_OP_BA)
+    {
+        prog_product_fill(Bm, nullptr, Am, Cm, DP_OP_BA);
+        return;
+    }
     if (Bm->kind != MATRIX_PERMUTED_DENSE || Am->kind != MATRIX_SPARSE || Cm->kind != MATRIX_PERMUTED_DENSE)
         unsupported("BA_matrices_fill_values");
     const permuted_dense *B = as_pd(Bm);
@@ -452,9 +428,9 @@ void dense_ATDA_fill(const matrix *Am, const double *d, matrix *Cm)
     SDL_CUDA(cudaStreamSynchronize(s));
     matrix_values_changed(Cm);
 }
-void dense_DA_fill(const double *, const matrix *, matrix *) { unsupported("DA_matrices_fill_values"); }
-matrix *dense_transpose_alloc(const matrix *) { unsupported("transpose_matrices_alloc"); }
-void dense_transpose_fill(const matrix *, matrix *) { unsupported("transpose_matrices_fill_values"); }
+void dense_DA_fill(const double *d, const matrix *A, matrix *C) { prog_DA_fill(d, A, C); }
+matrix *dense_transpose_alloc(const matrix *A) { return prog_transpose_alloc(A); }
+void dense_transpose_fill(const matrix *A, matrix *AT) { prog_transpose_fill(A, AT); }
 
 } // namespace sdl
 
