@@ -806,3 +806,146 @@ void dense_rows_fill(const matrix *self, matrix *out)
 }
 
 } // namespace sdl
+
+namespace sdl {
+
+// ------------------------------------------------------------------ dense kron
+// C = kron(I_p, A) J or kron(A, I_p) J for a full permuted_dense A (m x n, identity
+// perms) and J of any kind with J->m = p n (upstream src/stacked_pd/
+// stacked_pd_kron_linalg.c:26-307, src/matmul_kron_dispatchers.c:28-123): diagonal
+// block k of the Kronecker factor is A at rows k m + i, columns k n + j (or
+// k + p i, k + p j); per block, upstream's BA_pd_pd (J pd), BA_pd_csr (J sparse)
+// or BTA_pd_spd of its transpose (J spd); blocks without values are dropped and C's
+// block q records its k.
+matrix *prog_dense_kron_alloc(const matrix *Am, int p, matrix *Jm, bool a_i)
+{
+    if (Am->kind != MATRIX_PERMUTED_DENSE) fail(SDL_ERR_INVALID, "dense kron: A must be a full permuted_dense");
+    const permuted_dense *A = as_pd(Am);
+    const int m = A->m0, n = A->n0;
+    if (m != Am->m || n != Am->n) fail(SDL_ERR_INVALID, "dense kron: A must be a full permuted_dense");
+    for (int i = 0; i < m; ++i)
+        if (A->row_perm[i] != i) fail(SDL_ERR_INVALID, "dense kron: A must be a full permuted_dense");
+    for (int j = 0; j < n; ++j)
+        if (A->col_perm[j] != j) fail(SDL_ERR_INVALID, "dense kron: A must be a full permuted_dense");
+    if (p < 0) fail(SDL_ERR_INVALID, "dense kron: negative p");
+    if ((long long)p * n != Jm->m) fail(SDL_ERR_INVALID, "dense kron: J must have p * A->n rows");
+    if ((long long)p * m > INT_MAX) fail(SDL_ERR_OVERFLOW, "dense kron: p * A->m exceeds INT_MAX");
+    cudaStream_t s = runtime().stream;
+    const int jkind = kind_of(Jm);
+    Blocks J;
+    if (jkind != A_SPARSE) J = view(Jm);
+    DpBuilder b;
+    std::vector<DpPart> parts;
+    std::vector<int> kept;
+    std::vector<int> rows(m), cols(n), ib, ij;
+    for (int k = 0; k < p; ++k)
+    {
+        for (int i = 0; i < m; ++i) rows[i] = a_i ? k + p * i : k * m + i;
+        for (int j = 0; j < n; ++j) cols[j] = a_i ? k + p * j : k * n + j;
+        DpPart part;
+        part.rows = rows;
+        if (jkind == A_PD)
+        {
+            const Blk &Jb = J.b[0];
+            if (!m || !Jb.n0 || !intersect(cols.data(), n, Jb.rp, Jb.m0, ib, ij)) continue;
+            part.cols.assign(Jb.cp, Jb.cp + Jb.n0);
+            const long long q = b.alloc((long long)m * Jb.n0);
+            b.gemm(q, m, Jb.n0, 0, n, false, ib, Jb.off, Jb.n0, ij, rows_at(Jb.rp, ij));
+            part.vals.push_back(DpPart::Val{part.cols, q, Jb.n0, 1});
+        }
+        else if (jkind == A_SPD)
+        {
+            std::vector<const Blk *> contrib;
+            for (const Blk &Jb : J.b)
+                if (intersect(cols.data(), n, Jb.rp, Jb.m0, ib, ij)) contrib.push_back(&Jb);
+            part.cols = sorted_union(contrib);
+            if (!m || part.cols.empty()) continue;
+            for (const Blk *Jb : contrib)
+            {
+                intersect(cols.data(), n, Jb->rp, Jb->m0, ib, ij);
+                const long long q = b.alloc((long long)m * Jb->n0);
+                b.gemm(q, m, Jb->n0, 0, n, false, ib, Jb->off, Jb->n0, ij, rows_at(Jb->rp, ij));
+                part.vals.push_back(DpPart::Val{std::vector<int>(Jb->cp, Jb->cp + Jb->n0), q, Jb->n0, 1});
+            }
+        }
+        else
+        {
+            // upstream BA_pd_csr: output columns = the union of J's rows cols[r];
+            // column c sums B[i, r] * J.x over those rows in ascending r
+            const CSR_matrix *S = as_sparse(Jm)->csr;
+            std::vector<int4> ent; // (column, r, position, 0)
+            for (int r = 0; r < n; ++r)
+                for (int q = S->p[cols[r]]; q < S->p[cols[r] + 1]; ++q) ent.push_back(make_int4(S->i[q], r, q, 0));
+            std::stable_sort(ent.begin(), ent.end(), [](const int4 &x, const int4 &y) { return x.x < y.x; });
+            const int n0C = distinct_outer(ent);
+            if (!m || !n0C) continue;
+            const long long q = b.alloc((long long)m * n0C);
+            Blk Ab{m, n, A->row_perm, A->col_perm, A->row_inv, 0};
+            std::vector<int> kk, pos, zr;
+            size_t e = 0;
+            while (e < ent.size())
+            {
+                const int c = ent[e].x;
+                kk.clear();
+                pos.clear();
+                zr.clear();
+                for (; e < ent.size() && ent[e].x == c; ++e)
+                {
+                    kk.push_back(ent[e].y);
+                    pos.push_back(ent[e].z);
+                    zr.push_back(0);
+                }
+                b.spvec(q + (long long)part.cols.size(), m, n0C, Ab.off, n, false, DP_SP_D_DENSE, kk, pos, zr, true);
+                part.cols.push_back(c);
+            }
+            part.vals.push_back(DpPart::Val{part.cols, q, n0C, 1});
+        }
+        parts.push_back(std::move(part));
+        kept.push_back(k);
+    }
+    std::unique_ptr<DenseProg> prog =
+        jkind == A_SPD ? dp_blocks(b, parts, s) : dp_direct(b, b.p_total, s);
+    std::vector<std::vector<int>> orows, ocols;
+    std::vector<int> sp(1, 0);
+    for (const DpPart &pt : parts)
+    {
+        orows.push_back(pt.rows);
+        ocols.push_back(pt.cols);
+        sp.push_back((int)sp.size());
+    }
+    matrix *C = make_spd(p * m, Jm->n, orows, ocols, sp, kept);
+    try
+    {
+        dp_finish(*prog, b, (long long)m * n, jkind == A_SPARSE ? 0 : J.nnz,
+                  jkind == A_SPARSE ? as_sparse(Jm)->csr->nnz : 0, 0, s);
+        bind(C, DP_OP_KRON, std::move(prog));
+    }
+    catch (...)
+    {
+        free_matrix(C);
+        throw;
+    }
+    return C;
+}
+
+void prog_dense_kron_fill(const matrix *Am, int p, const matrix *Jm, matrix *Cm)
+{
+    (void)p;
+    if (Am->kind != MATRIX_PERMUTED_DENSE) fail(SDL_ERR_INVALID, "dense kron: A must be a full permuted_dense");
+    const double *hr = nullptr, *Sx = nullptr;
+    long long nr = 0;
+    int ns = 0;
+    if (dense_kind(Jm))
+    {
+        hr = host_values(const_cast<matrix *>(Jm));
+        nr = value_count(Jm);
+    }
+    else
+    {
+        Sx = sparse_dev_values(as_sparse(Jm), runtime().stream);
+        ns = as_sparse(Jm)->csr->nnz;
+    }
+    run(Cm, DP_OP_KRON, as_pd(Am)->X, value_count(Am), hr, nr, Sx, ns, nullptr, "dense kron fill_values");
+}
+
+} // namespace sdl

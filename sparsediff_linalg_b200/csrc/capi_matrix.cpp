@@ -80,28 +80,6 @@ void sparse_free(sdl_sparse *sm)
     sp_free(sm);
 }
 
-// Copy the device values of an output into its host CSR and publish them.
-void publish_output(sdl_sparse *C, cudaStream_t s)
-{
-    d2h(C->csr->x, C->impl->vals.x.get(), C->csr->nnz, s);
-    check_device_errors(s, "fill");
-    matrix_values_changed(&C->base);
-    C->impl->vals.seen = C->base.values_version;
-    C->impl->vals.valid = true;
-}
-
-// New sparse output whose structure is (Cp, Ci) on the device; host copy made.
-sdl_sparse *new_output(int m, int n, int nnz, const int *d_Cp, const int *d_Ci, cudaStream_t s)
-{
-    CSR_matrix *csr = new_CSR_matrix(m, n, nnz);
-    d2h(csr->p, d_Cp, (size_t)m + 1, s);
-    d2h(csr->i, d_Ci, nnz, s);
-    SDL_CUDA(cudaStreamSynchronize(s));
-    sdl_sparse *C = as_sparse(sparse_wrap(csr));
-    C->impl->vals.x.reset(std::max(1, nnz));
-    return C;
-}
-
 void check_sparse(const matrix *M, const char *what)
 {
     if (!M) fail(SDL_ERR_INVALID, std::string(what) + " is NULL");
@@ -288,6 +266,29 @@ void wire_sparse(sdl_sparse *sm)
 }
 
 } // namespace
+
+// Copy the device values of an output into its host CSR and publish them.
+void publish_output(sdl_sparse *C, cudaStream_t s)
+{
+    d2h(C->csr->x, C->impl->vals.x.get(), C->csr->nnz, s);
+    check_device_errors(s, "fill");
+    matrix_values_changed(&C->base);
+    C->impl->vals.seen = C->base.values_version;
+    C->impl->vals.valid = true;
+}
+
+// New sparse output whose structure is (Cp, Ci) on the device; host copy made.
+sdl_sparse *new_output(int m, int n, int nnz, const int *d_Cp, const int *d_Ci, cudaStream_t s)
+{
+    CSR_matrix *csr = new_CSR_matrix(m, n, nnz);
+    d2h(csr->p, d_Cp, (size_t)m + 1, s);
+    d2h(csr->i, d_Ci, nnz, s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    sdl_sparse *C = as_sparse(sparse_wrap(csr));
+    C->impl->vals.x.reset(std::max(1, nnz));
+    return C;
+}
+
 
 // ------------------------------------------------------------------ sparse helpers
 matrix *sparse_wrap(CSR_matrix *csr)

@@ -21,6 +21,7 @@ enum DpOp : int
     DP_OP_REDUCE,    // row_reduce vtable slot
     DP_OP_BTA,       // BTA_matrices_alloc (B or A dense-block, the other any kind)
     DP_OP_BA,        // BA_matrices_alloc
+    DP_OP_KRON,      // BA_kron_matrices_alloc / BA_dense_kron_I_matrices_alloc (A a full permuted_dense)
 };
 
 struct ProgState
@@ -66,5 +67,9 @@ matrix *spd_row_gather_alloc(const matrix *self, const int *map, int m_out);
 matrix *pd_row_reduce_alloc(const matrix *self, const int *group, int m_out);
 matrix *spd_row_reduce_alloc(const matrix *self, const int *group, int m_out);
 void dense_rows_fill(const matrix *self, matrix *out); // row_gather / row_reduce fill slots
+// C = kron(I_p, A) J (a_i = false) or kron(A, I_p) J (a_i = true) for a full
+// permuted_dense A and J of any kind; C is a stacked_pd.
+matrix *prog_dense_kron_alloc(const matrix *A, int p, matrix *J, bool a_i);
+void prog_dense_kron_fill(const matrix *A, int p, const matrix *J, matrix *C);
 
 } // namespace sdl

@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) k_dp_spvec(const DpSpTask *__restrict__ t
         double acc = 0.0;
         for (int e = T.e_begin; e < T.e_end; ++e)
         {
-            const double x = X[(long long)e_kk[e] * T.ld + t];
+            const double x = T.dense_trans ? X[(long long)t * T.ld + e_kk[e]] : X[(long long)e_kk[e] * T.ld + t];
             const double sv = Sx[e_pos[e]];
             double term;
             if (d && T.mode == DP_SP_D_DENSE)
@@ -269,12 +269,13 @@ void DpBuilder::gemm(long long p, int ni, int nj, long long l_off, int l_ld, boo
 }
 
 void DpBuilder::spvec(long long p, int nvec, int stride, long long x_off, int ld, bool dense_right, int mode,
-                      const std::vector<int> &kk, const std::vector<int> &pos, const std::vector<int> &grow)
+                      const std::vector<int> &kk, const std::vector<int> &pos, const std::vector<int> &grow,
+                      bool dense_trans)
 {
     if (nvec <= 0) return;
     if ((long long)e_kk.size() + (long long)kk.size() > INT_MAX) fail(SDL_ERR_OVERFLOW, "dense-block program too large");
     sp.push_back(DpSpTask{x_off, p, ld, nvec, (int)e_kk.size(), (int)(e_kk.size() + kk.size()), stride, mode,
-                          dense_right ? 1 : 0, 0});
+                          dense_right ? 1 : 0, dense_trans ? 1 : 0});
     e_kk.insert(e_kk.end(), kk.begin(), kk.end());
     e_pos.insert(e_pos.end(), pos.begin(), pos.end());
     e_row.insert(e_row.end(), grow.begin(), grow.end());
@@ -315,8 +316,9 @@ static void dp_validate(const DpBuilder &b, long long nl, long long nr, int ns, 
         const long long nx = t.dense_right ? nr : nl;
         for (int e = t.e_begin; e < t.e_end; ++e)
         {
-            if (b.e_kk[e] < 0 || t.x_off + (long long)b.e_kk[e] * t.ld + (t.nvec - 1) >= nx)
-                bad_prog("vector reads outside the dense operand");
+            const long long last = t.dense_trans ? (long long)(t.nvec - 1) * t.ld + b.e_kk[e]
+                                                 : (long long)b.e_kk[e] * t.ld + (t.nvec - 1);
+            if (b.e_kk[e] < 0 || t.x_off < 0 || t.x_off + last >= nx) bad_prog("vector reads outside the dense operand");
             if (b.e_pos[e] < 0 || b.e_pos[e] >= ns) bad_prog("vector reads outside the sparse values");
             if (d_len > 0 && (b.e_row[e] < 0 || b.e_row[e] >= d_len)) bad_prog("vector row outside d");
         }
@@ -441,6 +443,20 @@ std::unique_ptr<DenseProg> dp_coalesced(DpBuilder &b, const std::vector<DpPart> 
         P->out_cols.push_back(std::move(cols));
     }
     dp_stage2(*P, b, parts, {}, accumulate, s);
+    return P;
+}
+
+std::unique_ptr<DenseProg> dp_blocks(DpBuilder &b, const std::vector<DpPart> &parts, cudaStream_t s)
+{
+    auto P = std::make_unique<DenseProg>();
+    P->n_out = (int)parts.size();
+    for (size_t k = 0; k < parts.size(); ++k)
+    {
+        P->out_rows.push_back(parts[k].rows);
+        P->out_cols.push_back(parts[k].cols);
+        P->out_srcs.push_back({(int)k});
+    }
+    dp_stage2(*P, b, parts, {}, true, s);
     return P;
 }
 

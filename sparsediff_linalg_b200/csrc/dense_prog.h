@@ -67,12 +67,12 @@ enum DpSpMode : int
 
 // One vector of `nvec` values: P[p + t * stride] = sum over the entries e in
 // [e_begin, e_end) of the term (mode) for S.x[e_pos[e]], the dense value
-// X[x_off + e_kk[e] * ld + t] and d[e_row[e]], from +0.0 in entry order. X is XL
-// (dense_right == 0) or XR.
+// X[x_off + e_kk[e] * ld + t] (or X[x_off + t * ld + e_kk[e]] when dense_trans)
+// and d[e_row[e]], from +0.0 in entry order. X is XL (dense_right == 0) or XR.
 struct DpSpTask
 {
     long long x_off, p;
-    int ld, nvec, e_begin, e_end, stride, mode, dense_right, pad;
+    int ld, nvec, e_begin, e_end, stride, mode, dense_right, dense_trans;
 };
 
 // Output block of stage 2: m0 x n0 values at C + c_off; its value sources
@@ -148,7 +148,8 @@ struct DpBuilder
               long long r_off, int r_ld, const std::vector<int> &ri, const std::vector<int> &dr);
     // one vector; entries (dense row, position of S.x, global row for d)
     void spvec(long long p, int nvec, int stride, long long x_off, int ld, bool dense_right, int mode,
-               const std::vector<int> &kk, const std::vector<int> &pos, const std::vector<int> &grow);
+               const std::vector<int> &kk, const std::vector<int> &pos, const std::vector<int> &grow,
+               bool dense_trans = false);
 };
 
 // A partial of a coalesced result: rows x cols of the result (both ascending),
@@ -181,6 +182,9 @@ std::unique_ptr<DenseProg> dp_direct(DpBuilder &b, long long c_total, cudaStream
 // from their single holder.
 std::unique_ptr<DenseProg> dp_coalesced(DpBuilder &b, const std::vector<DpPart> &parts, int nrows, int ncols,
                                         bool accumulate, cudaStream_t s);
+// Finish a program whose output blocks are the parts themselves, in order (rows
+// x cols of each part), each cell the sum of its part's value sources from +0.0.
+std::unique_ptr<DenseProg> dp_blocks(DpBuilder &b, const std::vector<DpPart> &parts, cudaStream_t s);
 // Finish a program whose one output block (rows x cols) is the sum of `parts`
 // (each part's rows a subset of `rows`) from +0.0 in part order.
 std::unique_ptr<DenseProg> dp_single(DpBuilder &b, const std::vector<int> &rows, const std::vector<int> &cols,

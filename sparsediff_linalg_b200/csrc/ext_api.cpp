@@ -223,3 +223,12 @@ extern "C" sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, 
 }
 
 extern "C" void sdl_coalesce_destroy(sdl_coalesce *C) { delete C; }
+
+namespace sdl {
+// Coalesce with a factor per input triplet: each output sums (1 * d[t]) * x[t]
+// over its duplicates in ascending t, from +0.0 (d null: x[t]).
+void coalesce_fill_scaled(const sdl_coalesce *C, const double *x, const double *d, double *Cx, cudaStream_t s)
+{
+    product_numeric(C->P, nullptr, d, x, Cx, s);
+}
+} // namespace sdl

@@ -89,6 +89,11 @@ const DevStruct &sparse_dev_struct(sdl_sparse *A, cudaStream_t s);
 const double *sparse_dev_values(sdl_sparse *A, cudaStream_t s);
 const TransposePlan &sparse_dev_csc(sdl_sparse *A, cudaStream_t s);
 matrix *sparse_wrap(CSR_matrix *csr);
+// Copy the device values of a sparse output into its host CSR and publish them
+// (version bumped, device copy marked fresh).
+void publish_output(sdl_sparse *C, cudaStream_t s);
+// New sparse output whose structure is (Cp, Ci) on the device; host copy made.
+sdl_sparse *new_output(int m, int n, int nnz, const int *d_Cp, const int *d_Ci, cudaStream_t s);
 
 // dense kinds (capi_dense.cpp)
 void pd_free(permuted_dense *pd);

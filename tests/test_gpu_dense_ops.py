@@ -135,8 +135,11 @@ def csr_of(h):
 
 
 def structure_of(h):
-    """Blocks (row perm, col perm) and the source map of a dense-block handle."""
+    """Blocks (row perm, col perm) and the source map of a dense-block handle
+    (nothing for a sparse one)."""
     kind = h.contents.kind
+    if kind == 0:
+        return [], None
     if kind == PD:
         p = C.cast(h, C.POINTER(_PD)).contents
         return [(np.ctypeslib.as_array(p.row_perm, shape=(p.m0,)).copy() if p.m0 else np.zeros(0, np.int32),
