@@ -782,6 +782,9 @@ __device__ __forceinline__ void entry_values_run(const ProdSched &S, const ProdP
 
 __global__ void __launch_bounds__(256) k_entry_values(ProdSched S, ProdPtrs P)
 {
+    // the refill launched after this grid may start its prologue now; it waits for
+    // this grid's completion before it reads V
+    asm volatile("griddepcontrol.launch_dependents;");
     const long long step = (long long)gridDim.x * blockDim.x;
     entry_values_run(S, P, blockIdx.x * (long long)blockDim.x + threadIdx.x, S.nV, step);
 }
@@ -945,6 +948,10 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
         const ProdBase pb = prod_base<BATCHED>(dsc[0].prod, ptrs, scheds, P1, S1);
         load_terms(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
     }
+    // launched as a programmatic dependent of the entry-value kernel: everything
+    // above overlaps its tail; V is read only after it has completed (a no-op for
+    // an ordinary launch)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     for (int k = 0;; ++k)
     {
         const TileDesc &D = dsc[k & 3];
@@ -1892,8 +1899,23 @@ void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const 
         SDL_LAUNCH(k_tile_refill<true>, grid, REFILL_THREADS, refill_smem_bytes(), s, tiles, ntiles, ptrs,
                    scheds, vals, sched, runtime().d_error);
     else
-        SDL_LAUNCH(k_tile_refill<false>, grid, REFILL_THREADS, refill_smem_bytes(), s, tiles, ntiles, ptrs,
-                   scheds, vals, sched, runtime().d_error);
+    {
+        // programmatic dependent launch: the CTAs start while the entry-value kernel
+        // ahead of it on the stream drains (the kernel waits before reading V)
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(REFILL_THREADS);
+        cfg.dynamicSmemBytes = refill_smem_bytes();
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill<false>, tiles, ntiles, ptrs, scheds, vals, sched,
+                                    runtime().d_error));
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
 }
 
 void big_rows_refill(const Product &P, const double *Lx, const double *dvec, const double *Ax,
