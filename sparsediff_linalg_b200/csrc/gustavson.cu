@@ -963,23 +963,22 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
         for (int base = 0;; base += RSTEP)
         {
             const bool last = base + RSTEP >= nterms;
+            // every index below was checked once for the whole schedule when it was
+            // built (k_validate_schedule); the padding words past nterms are list words
             int2 es[RUNROLL];
-            bool ok[RUNROLL];
+            bool term[RUNROLL];
 #pragma unroll
             for (int j = 0; j < RUNROLL; ++j)
             {
-                const unsigned vi = (unsigned)(vbase + (int)(w[j] >> 14));
-                ok[j] = !(w[j] & (TERM_LIST << 12)) && vi < pb.nV;
-                es[j] = ok[j] ? pb.ES[vi] : make_int2(0, 0);
+                term[j] = !(w[j] & (TERM_LIST << 12));
+                es[j] = term[j] ? pb.ES[vbase + (int)(w[j] >> 14)] : make_int2(0, 0);
             }
             double v[RUNROLL], x[RUNROLL];
 #pragma unroll
             for (int j = 0; j < RUNROLL; ++j)
             {
-                const unsigned a = (unsigned)(es[j].x + base + tid + j * REFILL_THREADS);
-                ok[j] = ok[j] && a < pb.nA && (unsigned)es[j].y < pb.nV;
-                v[j] = ok[j] ? (pb.V ? pb.V[es[j].y] : 1.0) : 0.0;
-                x[j] = ok[j] ? pb.Ax[a] : 0.0;
+                v[j] = term[j] ? (pb.V ? pb.V[es[j].y] : 1.0) : 0.0;
+                x[j] = term[j] ? pb.Ax[es[j].x + base + tid + j * REFILL_THREADS] : 0.0;
             }
             unsigned wn[RUNROLL];
             if (!last)
@@ -995,13 +994,8 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
 #pragma unroll
             for (int j = 0; j < RUNROLL; ++j)
             {
-                if (w[j] & (TERM_LIST << 12)) continue;
+                if (!term[j]) continue;
                 const int p = (int)(w[j] & 0xfffu);
-                if (!ok[j] || p >= nout)
-                {
-                    atomicOr(err, 1);
-                    continue;
-                }
                 const double prod = __dmul_rn(v[j], x[j]);
                 if (w[j] & (TERM_PAIR << 12))
                     atomicAdd(&win[p], prod);
@@ -1520,6 +1514,63 @@ void build_big_lists(const ProductDesc &d, Product &P, const long long *ub, cons
 
 // Everything the refill needs once C's structure is known: row classes, the
 // compiled tile schedule and the larger rows' scratch.
+// Checks every index the tile refill will use, once per schedule: per tile, its
+// window and output range, its words inside the word array, and for every term
+// word that is not a list word its entry, the entry's A position for that term and
+// its value slot, and its output inside the window; per list, its output and items.
+// The refill's term loop then reads without per-term checks.
+__global__ void k_validate_schedule(const TileDesc *__restrict__ tiles, int ntiles, const unsigned *__restrict__ W,
+                                    long long word_total, const unsigned *__restrict__ X, long long x_total,
+                                    const int2 *__restrict__ ES, long long nV, long long nA, long long nnzC,
+                                    int *__restrict__ err)
+{
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x)
+    {
+        const TileDesc D = tiles[t];
+        if (D.nterms < 0 || D.nout < 0 || D.nout > TILE_ACC || D.out_begin < 0 ||
+            (long long)D.out_begin + D.nout > nnzC || D.word_begin < 0 ||
+            (long long)D.word_begin + D.nterms > word_total || D.vbase < 0 || D.prod != 0)
+        {
+            if (threadIdx.x == 0) atomicOr(err, 4);
+            continue;
+        }
+        for (int u = threadIdx.x; u < D.nterms; u += blockDim.x)
+        {
+            const unsigned w = W[D.word_begin + u];
+            if (w & (TERM_LIST << 12)) continue;
+            const long long vi = (long long)D.vbase + (w >> 14);
+            if (vi >= nV)
+            {
+                atomicOr(err, 4);
+                continue;
+            }
+            const int2 es = ES[vi];
+            const long long a = (long long)es.x + u;
+            if (a < 0 || a >= nA || es.y < 0 || es.y >= nV || (int)(w & 0xfffu) >= D.nout) atomicOr(err, 4);
+        }
+        if (D.nlist > 0)
+        {
+            if (D.x_begin < 0 || (long long)D.x_begin + D.nlist + 1 > x_total)
+            {
+                if (threadIdx.x == 0) atomicOr(err, 4);
+                continue;
+            }
+            const unsigned *hdr = X + D.x_begin;
+            const long long items_end = (long long)(hdr[D.nlist] >> 12);
+            if ((long long)D.x_begin + D.nlist + 1 + items_end > x_total)
+            {
+                if (threadIdx.x == 0) atomicOr(err, 4);
+                continue;
+            }
+            for (int l = threadIdx.x; l < D.nlist; l += blockDim.x)
+                if ((int)(hdr[l] & 0xfffu) >= D.nout || (hdr[l] >> 12) > (hdr[l + 1] >> 12)) atomicOr(err, 4);
+            const unsigned *items = hdr + D.nlist + 1;
+            for (long long i = threadIdx.x; i < items_end; i += blockDim.x)
+                if (items[i] >= (unsigned)D.nterms) atomicOr(err, 4);
+        }
+    }
+}
+
 void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
 {
     Runtime &rt = runtime();
@@ -1583,6 +1634,13 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
                tile_start.get(), nullptr, nullptr, word_begin.get(), x_begin.get(), P.tiles.get(),
                P.W.get(), P.X.get(), P.ES.get());
     if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
+    if (P.ntiles > 0)
+    {
+        SDL_LAUNCH(k_validate_schedule, grid_for(P.ntiles, 1, rt.num_sms * 8), 256, 0, s, P.tiles.get(), P.ntiles,
+                   P.W.get(), word_total, P.X.get(), x_total, P.ES.get(), nV, (long long)d.A_nnz,
+                   (long long)P.nnz, rt.d_error);
+        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: the refill schedule failed its bounds check");
+    }
     build_big_lists(d, P, ub, na, s);
     if (P.num_count[NUM_GMEM] && !P.big_lists)
     {
