@@ -21,6 +21,7 @@
 //             accumulator (<= 8192 output entries), CTA + accumulator in C.x itself
 //             with a global column->position map (larger rows).
 #include <algorithm>
+#include <cstddef>
 #include <climits>
 #include <cstring>
 #include <string>
@@ -812,7 +813,6 @@ constexpr int RUNROLL = SDL_REFILL_UNROLL; // terms per thread whose loads are i
 constexpr int RSTEP = RUNROLL * REFILL_THREADS;
 constexpr int WIN = TILE_ACC; // outputs of a tile window
 
-__host__ __device__ constexpr size_t refill_smem_bytes() { return 2 * (size_t)WIN * 8 + 4 * sizeof(TileDesc); }
 
 // Base pointers of the product a tile belongs to: kernel parameters for a single
 // product, the batch's tables otherwise.
@@ -854,6 +854,13 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
         r.nA = (unsigned)S1.nA;
     }
     return r;
+}
+
+// Shared memory of a refill CTA: two windows, a ring of four tile descriptors and,
+// for batched refills, the resolved base pointers of each descriptor's product.
+__host__ __device__ constexpr size_t refill_smem_bytes()
+{
+    return 2 * (size_t)WIN * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase);
 }
 
 __device__ __forceinline__ void load_terms(const unsigned *__restrict__ W, int nterms, int base,
@@ -910,10 +917,29 @@ __device__ __forceinline__ double list_sum(const ProdBase &pb, const TileDesc &D
     return acc;
 }
 
-__device__ __forceinline__ void copy_desc(TileDesc *dst, const TileDesc *__restrict__ src)
+// Copies a tile descriptor into the ring; in a batched refill the thread that holds
+// the product index also resolves the product's base pointers into the ring (two
+// tiles ahead of their use, so the refill never waits on them).
+template <bool BATCHED>
+__device__ __forceinline__ void copy_desc(TileDesc *dst, ProdBase *bdst, const TileDesc *__restrict__ src,
+                                          const ProdPtrs *__restrict__ ptrs, const ProdSched *__restrict__ scheds,
+                                          const ProdPtrs &P1, const ProdSched &S1)
 {
     if (threadIdx.x < (int)(sizeof(TileDesc) / 4))
-        reinterpret_cast<int *>(dst)[threadIdx.x] = reinterpret_cast<const int *>(src)[threadIdx.x];
+    {
+        const int v = reinterpret_cast<const int *>(src)[threadIdx.x];
+        reinterpret_cast<int *>(dst)[threadIdx.x] = v;
+        if (BATCHED && threadIdx.x == (int)(offsetof(TileDesc, prod) / 4))
+            *bdst = prod_base<true>(v, ptrs, scheds, P1, S1);
+    }
+}
+
+// Base pointers of the tile in ring slot `slot`.
+template <bool BATCHED>
+__device__ __forceinline__ ProdBase base_of(const ProdBase *bse, int slot, const ProdPtrs &P1, const ProdSched &S1)
+{
+    if (BATCHED) return bse[slot];
+    return prod_base<false>(0, nullptr, nullptr, P1, S1);
 }
 
 // Refill of the tile rows from the entry-major schedule. Persistent CTAs walk their
@@ -935,17 +961,18 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
 {
     extern __shared__ __align__(16) double rsm[];
     TileDesc *dsc = reinterpret_cast<TileDesc *>(rsm + 2 * WIN);
+    ProdBase *bse = reinterpret_cast<ProdBase *>(dsc + 4);
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     int t = blockIdx.x;
     if (t >= ntiles) return;
     for (int i = tid; i < 2 * WIN; i += REFILL_THREADS) rsm[i] = 0.0;
-    copy_desc(dsc, tiles + t);
-    if (t + G < ntiles) copy_desc(dsc + 1, tiles + t + G);
+    copy_desc<BATCHED>(dsc, bse, tiles + t, ptrs, scheds, P1, S1);
+    if (t + G < ntiles) copy_desc<BATCHED>(dsc + 1, bse + 1, tiles + t + G, ptrs, scheds, P1, S1);
     __syncthreads();
     unsigned w[RUNROLL];
     {
-        const ProdBase pb = prod_base<BATCHED>(dsc[0].prod, ptrs, scheds, P1, S1);
+        const ProdBase pb = base_of<BATCHED>(bse, 0, P1, S1);
         load_terms(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
     }
     // launched as a programmatic dependent of the entry-value kernel: everything
@@ -956,9 +983,10 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
     {
         const TileDesc &D = dsc[k & 3];
         const bool has1 = t + G < ntiles;
-        if (t + 2 * G < ntiles) copy_desc(dsc + ((k + 2) & 3), tiles + t + 2 * G);
+        if (t + 2 * G < ntiles)
+            copy_desc<BATCHED>(dsc + ((k + 2) & 3), bse + ((k + 2) & 3), tiles + t + 2 * G, ptrs, scheds, P1, S1);
         double *win = rsm + (k & 1) * WIN;
-        const ProdBase pb = prod_base<BATCHED>(D.prod, ptrs, scheds, P1, S1);
+        const ProdBase pb = base_of<BATCHED>(bse, k & 3, P1, S1);
         const int nterms = D.nterms, nout = D.nout, vbase = D.vbase;
         for (int base = 0;; base += RSTEP)
         {
@@ -986,7 +1014,7 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
             else if (has1)
             {
                 const TileDesc &Dn = dsc[(k + 1) & 3];
-                const ProdBase pn = prod_base<BATCHED>(Dn.prod, ptrs, scheds, P1, S1);
+                const ProdBase pn = base_of<BATCHED>(bse, (k + 1) & 3, P1, S1);
                 load_terms(pn.W + Dn.word_begin, Dn.nterms, 0, wn);
             }
             else
