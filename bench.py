@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-conversions", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--dense-blocks", type=int, default=64,
                     help="blocks of the stacked_pd x CSC case (64 is the configuration; fewer for profiling)")
     ap.add_argument("--learned-matrices", type=int, default=200)
@@ -271,6 +272,12 @@ def run_b200(args, world, rank, local):
     P, Tr = btda_product(Ap, Ai, A[4], Bp, Bi, B[4])
     torch.cuda.synchronize()
     symbolic_ms = (time.perf_counter() - t0) * 1e3
+    # the product's plan picked by the autotuner on this pattern (timed refills
+    # below run with it); it reports the as-given plan's refill time beside its own
+    tune = None
+    if not args.no_autotune:
+        tune = P.autotune(reps=5, stream=stream)
+        torch.cuda.synchronize()
     Cx = torch.empty(P.nnz, dtype=torch.float64, device=dev)
     B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], P.nnz, B[4])
 
@@ -363,6 +370,7 @@ def run_b200(args, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "symbolic_ms": round(symbolic_ms, 3),
+        "autotune": tune,
         "spgemm_2000": {"symbolic_ms": round(sp_sym_ms, 3), "numeric_us": round(sp_num_us, 2),
                         "nnz_C": SP.nnz},
     }

@@ -99,6 +99,23 @@ sdl_status sdl_product_fill(const sdl_product *P, const double *Lx, const double
                             const double *Ax, double *Cx, void *stream);
 void sdl_product_destroy(sdl_product *P);
 
+/* No upstream counterpart: autotuner. Re-plans P for its own pattern (structure
+   and values are unchanged; only the schedule moves). Candidate symbolic bin
+   thresholds (warp-kernel row limit 128 / 512 terms, 4 / 8 / 16 warps per CTA)
+   are timed on the pattern; then candidate tile budgets (TILE_T, 3/4, 1/2 of it)
+   and resident refill CTAs per SM (all that fit, 4, 3) by `reps` refills each
+   with placeholder values, L2 flushed before each; P keeps the fastest plan
+   (the as-given plan unless a candidate beats it). The row offsets / column
+   indices sdl_product_info returned before are released: ask again. Allocates;
+   synchronises the stream. */
+sdl_status sdl_product_autotune(sdl_product *P, int reps, void *stream);
+/* The configuration P runs with and, after sdl_product_autotune, what the tuner
+   measured (microseconds of the chosen and of the as-given refill; candidates
+   timed; milliseconds the tuning took). Any pointer may be NULL. */
+sdl_status sdl_product_tuning(const sdl_product *P, int *warp_max_terms, int *rows_per_cta_warp,
+                              int *tile_budget, int *refill_ctas_per_sm, double *refill_us,
+                              double *default_refill_us, int *candidates, double *tune_ms);
+
 /* No upstream counterpart. Same result as sdl_product_fill, bit for bit, for
    callers that cannot call cudaMalloc while they refill: device memory wholly
    owned by another allocator, a fixed device-memory budget that may not grow, or

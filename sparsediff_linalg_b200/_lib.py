@@ -99,6 +99,9 @@ EXTENSION_SIGNATURES = {
     "sdl_product_info": (C.c_int, [vp, c_int_p, c_int_p, c_int_p, C.POINTER(C.c_longlong),
                                    C.POINTER(vp), C.POINTER(vp)]),
     "sdl_product_fill": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "sdl_product_autotune": (C.c_int, [vp, C.c_int, vp]),
+    "sdl_product_tuning": (C.c_int, [vp, c_int_p, c_int_p, c_int_p, c_int_p, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double), c_int_p, C.POINTER(C.c_double)]),
     "sdl_product_destroy": (None, [vp]),
     "sdl_product_fill_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "sdl_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, vp, C.POINTER(vp)]),

@@ -9,6 +9,7 @@ using namespace sdl;
 struct sdl_product
 {
     Product P;
+    TuneResult tuned;
 };
 
 struct sdl_transpose
@@ -86,6 +87,32 @@ extern "C" sdl_status sdl_product_create(const sdl_product_desc *desc, void *str
         auto p = std::make_unique<sdl_product>();
         product_symbolic(d, TuneConfig{}, p->P, pick_stream(stream));
         *out = p.release();
+    });
+}
+
+extern "C" sdl_status sdl_product_autotune(sdl_product *P, int reps, void *stream)
+{
+    return guard_status("sdl_product_autotune", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        P->tuned = product_autotune(P->P, reps, pick_stream(stream));
+    });
+}
+
+extern "C" sdl_status sdl_product_tuning(const sdl_product *P, int *warp_max_terms, int *rows_per_cta_warp,
+                                         int *tile_budget, int *refill_ctas_per_sm, double *refill_us,
+                                         double *default_refill_us, int *candidates, double *tune_ms)
+{
+    return guard_status("sdl_product_tuning", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        const TuneConfig &c = P->P.cfg;
+        if (warp_max_terms) *warp_max_terms = c.warp_max_terms;
+        if (rows_per_cta_warp) *rows_per_cta_warp = c.rows_per_cta_warp;
+        if (tile_budget) *tile_budget = c.tile_budget > 0 ? c.tile_budget : TILE_T;
+        if (refill_ctas_per_sm) *refill_ctas_per_sm = c.refill_ctas_per_sm;
+        if (refill_us) *refill_us = P->tuned.refill_us;
+        if (default_refill_us) *default_refill_us = P->tuned.default_refill_us;
+        if (candidates) *candidates = P->tuned.candidates;
+        if (tune_ms) *tune_ms = P->tuned.tune_ms;
     });
 }
 

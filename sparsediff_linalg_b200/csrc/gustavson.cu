@@ -21,6 +21,7 @@
 //             accumulator (<= 8192 output entries), CTA + accumulator in C.x itself
 //             with a global column->position map (larger rows).
 #include <algorithm>
+#include <chrono>
 #include <cstddef>
 #include <climits>
 #include <cstring>
@@ -120,7 +121,7 @@ __global__ void k_bin_scatter(const unsigned char *__restrict__ cls, int n, int 
     }
 }
 
-__global__ void k_sym_classify(const long long *__restrict__ ub, int m_out,
+__global__ void k_sym_classify(const long long *__restrict__ ub, int m_out, int warp_max,
                                unsigned char *__restrict__ cls)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
@@ -129,6 +130,7 @@ __global__ void k_sym_classify(const long long *__restrict__ ub, int m_out,
         long long u = ub[r];
         int c = u == 0 ? 255 : u <= 32 ? SYM_W32 : u <= 128 ? SYM_W128 : u <= 512 ? SYM_W512
                          : u <= 2048 ? SYM_C2K : u <= 8192 ? SYM_C8K : SYM_BITMAP;
+        if (u > warp_max && c <= SYM_W512) c = SYM_C2K; // rows above the warp threshold go to CTAs
         cls[r] = (unsigned char)c;
     }
 }
@@ -176,11 +178,11 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
 
 // tile index of every row = floor(exclusive weight prefix / TILE_T); flag rows that
 // start a tile
-__global__ void k_tile_flags(const long long *__restrict__ wpref, int m_out, int *__restrict__ flag)
+__global__ void k_tile_flags(const long long *__restrict__ wpref, int m_out, int budget, int *__restrict__ flag)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
          r += (long long)gridDim.x * blockDim.x)
-        flag[r] = (r == 0 || wpref[r] / TILE_T != wpref[r - 1] / TILE_T) ? 1 : 0;
+        flag[r] = (r == 0 || wpref[r] / budget != wpref[r - 1] / budget) ? 1 : 0;
 }
 
 __global__ void k_tile_starts(const int *__restrict__ flag, const int *__restrict__ tile_of, int m_out,
@@ -1268,11 +1270,11 @@ namespace {
 
 // Launches the symbolic kernel of every row class over the binned row lists.
 void sym_launch(const SymArgs &sa, const int *lists, const int *cnt, const int *off,
-                const ProductDesc &d, cudaStream_t s)
+                const ProductDesc &d, const TuneConfig &cfg, cudaStream_t s)
 {
     Runtime &rt = runtime();
     const int cap = rt.num_sms * 16;
-    const int wpb = 8;
+    const int wpb = std::max(1, std::min(16, cfg.rows_per_cta_warp));
     if (cnt[SYM_W32])
         SDL_LAUNCH(k_sym_warp<32>, grid_for(cnt[SYM_W32], wpb, cap), wpb * 32, wpb * 32 * 4, s,
                    lists + off[SYM_W32], cnt[SYM_W32], sa);
@@ -1284,7 +1286,7 @@ void sym_launch(const SymArgs &sa, const int *lists, const int *cnt, const int *
                    lists + off[SYM_W512], cnt[SYM_W512], sa);
     if (cnt[SYM_C2K])
     {
-        int th = 256;
+        const int th = cfg.cta_threads_2k == 128 || cfg.cta_threads_2k == 512 ? cfg.cta_threads_2k : 256;
         size_t sm = 2048 * 4 + (3 * th + 32) * 4;
         SDL_LAUNCH(k_sym_cta<2048>, grid_for(cnt[SYM_C2K], 1, cap), th, sm, s, lists + off[SYM_C2K],
                    cnt[SYM_C2K], sa);
@@ -1610,7 +1612,8 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
     exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
     DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
-    SDL_LAUNCH(k_tile_flags, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, wpref.get(), m_out,
+    const int budget = P.cfg.tile_budget > 0 ? std::max(TILE_T / 8, std::min(TILE_T, P.cfg.tile_budget)) : TILE_T;
+    SDL_LAUNCH(k_tile_flags, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, wpref.get(), m_out, budget,
                flag.get());
     P.ntiles = exclusive_scan_i32_checked(flag.get(), tile_of.get(), m_out, s);
     DevBuf<int> tile_start((size_t)P.ntiles + 1);
@@ -1801,13 +1804,13 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     DevBuf<int> tmp(std::max<long long>(1, P.terms));
     DevBuf<unsigned char> cls(m_out);
     SDL_LAUNCH(k_sym_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(), m_out,
-               cls.get());
+               cfg.warp_max_terms, cls.get());
     DevBuf<int> lists;
     int cnt[SYM_NBINS], off[SYM_NBINS + 1];
     bin_items(cls.get(), m_out, SYM_NBINS, lists, cnt, off, s);
     SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, ub_off.get(), tmp.get(), row_nnz.get(),
                nullptr, nullptr};
-    sym_launch(sa, lists.get(), cnt, off, d, s);
+    sym_launch(sa, lists.get(), cnt, off, d, cfg, s);
 
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
@@ -1849,13 +1852,14 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
     SDL_CUDA(cudaMemsetAsync(overflow.get(), 0, overflow.bytes(), s));
     DevBuf<int> tmp(std::max<long long>(1, st.cap_total));
     DevBuf<unsigned char> cls(m_out);
-    SDL_LAUNCH(k_sym_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(), m_out, cls.get());
+    SDL_LAUNCH(k_sym_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(), m_out,
+               cfg.warp_max_terms, cls.get());
     DevBuf<int> lists;
     int cnt[SYM_NBINS], off[SYM_NBINS + 1];
     bin_items(cls.get(), m_out, SYM_NBINS, lists, cnt, off, s);
     SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, cap_off.get(), tmp.get(), row_nnz.get(),
                cap.get(), overflow.get()};
-    sym_launch(sa, lists.get(), cnt, off, d, s);
+    sym_launch(sa, lists.get(), cnt, off, d, cfg, s);
 
     // rows whose columns did not fit: the exact pass again, into term-count space
     DevBuf<long long> fb_len(m_out), fb_off((size_t)m_out + 1);
@@ -1876,7 +1880,7 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
         for (int c = 0; c < SYM_NBINS; ++c) st.fallback_rows += fcnt[c];
         SymArgs fa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, fb_off.get(), fb.get(), row_nnz.get(),
                    nullptr, nullptr};
-        sym_launch(fa, flists.get(), fcnt, foff, d, s);
+        sym_launch(fa, flists.get(), fcnt, foff, d, cfg, s);
     }
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
@@ -1958,7 +1962,7 @@ void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStrea
 }
 
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
-                 cudaStream_t s, ProdPtrs vals, ProdSched sched)
+                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm)
 {
     if (ntiles <= 0) return;
     // kernel attributes and resident CTAs per SM, set once (outside any capture)
@@ -1980,7 +1984,8 @@ void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const 
         }
         per_sm[b] = std::max(1, per_sm[b]);
     }
-    const int grid = std::min(ntiles, runtime().num_sms * per_sm[b]);
+    const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm[b]) : per_sm[b];
+    const int grid = std::min(ntiles, runtime().num_sms * use);
     if (b)
         SDL_LAUNCH(k_tile_refill<true>, grid, REFILL_THREADS, refill_smem_bytes(), s, tiles, ntiles, ptrs,
                    scheds, vals, sched, runtime().d_error);
@@ -2087,7 +2092,7 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
         const ProdSched S = sched_of(P);
         const ProdPtrs vals{Lx, dvec, Ax, Cx};
         entry_values(S, vals, s);
-        tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S);
+        tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm);
     }
     if (P.big_lists)
     {
@@ -2111,6 +2116,145 @@ void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, Pr
         SDL_LAUNCH(k_big_refill<false>, grid, 256, 0, s, P.brows.get(), P.nbig, P.bout_off.get(), P.big_outputs,
                    P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, P.V.get(), nV, (long long)P.desc.A_nnz,
                    runtime().d_error);
+}
+
+} // namespace sdl
+
+// ------------------------------------------------------------------ autotuner
+namespace sdl {
+namespace {
+__global__ void k_tune_diff(const int *__restrict__ a, const int *__restrict__ b, long long n, int *__restrict__ err)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (a[i] != b[i]) atomicOr(err, 8);
+}
+
+__global__ void k_tune_fill(double *x, long long n, double v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = v;
+}
+} // namespace
+
+TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
+{
+    TuneResult R;
+    R.best = P.cfg;
+    if (P.m_out == 0 || P.nnz == 0) return R;
+    reps = std::max(1, std::min(reps, 50));
+    Runtime &rt = runtime();
+    const auto t_start = std::chrono::steady_clock::now();
+    const ProductDesc d = P.desc;
+    // placeholder values: d = A.x = 1 (the entry-value kernel runs as in a real refill)
+    DevBuf<double> dv((size_t)std::max(1, d.A_m)), ax((size_t)std::max(1, d.A_nnz)), cx((size_t)P.nnz);
+    SDL_LAUNCH(k_tune_fill, grid_for(std::max(1, d.A_m), 256, rt.num_sms * 8), 256, 0, s, dv.get(),
+               (long long)std::max(1, d.A_m), 1.0);
+    SDL_LAUNCH(k_tune_fill, grid_for(std::max(1, d.A_nnz), 256, rt.num_sms * 8), 256, 0, s, ax.get(),
+               (long long)std::max(1, d.A_nnz), 1.0);
+    DevBuf<unsigned char> flush((size_t)256 << 20); // larger than L2: each timed refill starts cold
+    cudaEvent_t e0, e1;
+    SDL_CUDA(cudaEventCreate(&e0));
+    SDL_CUDA(cudaEventCreate(&e1));
+    auto refill_us = [&](const Product &Q) -> double {
+        product_numeric(Q, nullptr, dv.get(), ax.get(), cx.get(), s);
+        double best = 1e30;
+        for (int r = 0; r < reps; ++r)
+        {
+            SDL_CUDA(cudaMemsetAsync(flush.get(), r & 0xff, flush.bytes(), s));
+            SDL_CUDA(cudaEventRecord(e0, s));
+            product_numeric(Q, nullptr, dv.get(), ax.get(), cx.get(), s);
+            SDL_CUDA(cudaEventRecord(e1, s));
+            SDL_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            SDL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, 1e3 * ms);
+        }
+        ++R.candidates;
+        return best;
+    };
+    auto build = [&](const TuneConfig &c, Product &out) -> double {
+        const auto t0 = std::chrono::steady_clock::now();
+        product_symbolic(d, c, out, s);
+        SDL_CUDA(cudaStreamSynchronize(s));
+        if (out.nnz != P.nnz || out.m_out != P.m_out)
+            fail(SDL_ERR_INTERNAL, "autotune: a candidate plan has another structure");
+        SDL_LAUNCH(k_tune_diff, grid_for(P.m_out + 1, 256, rt.num_sms * 8), 256, 0, s, out.Cp.get(), P.Cp.get(),
+                   (long long)P.m_out + 1, rt.d_error);
+        SDL_LAUNCH(k_tune_diff, grid_for(P.nnz, 256, rt.num_sms * 8), 256, 0, s, out.Ci.get(), P.Ci.get(),
+                   (long long)P.nnz, rt.d_error);
+        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "autotune: a candidate plan has another structure");
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    };
+    // the plan as given (default configuration) is the first candidate
+    R.default_refill_us = refill_us(P);
+    // stage 1: symbolic bin thresholds (warp-kernel threshold, warps per CTA)
+    const TuneConfig base = P.cfg;
+    const int sym_cand[][2] = {{512, 8}, {512, 4}, {512, 16}, {128, 8}};
+    TuneConfig sym_best = base;
+    double sym_best_ms = 1e30;
+    Product stage1;
+    for (const auto &sc : sym_cand)
+    {
+        TuneConfig c = base;
+        c.warp_max_terms = sc[0];
+        c.rows_per_cta_warp = sc[1];
+        Product Q;
+        const double ms = build(c, Q);
+        if (ms < sym_best_ms)
+        {
+            sym_best_ms = ms;
+            sym_best = c;
+            stage1 = std::move(Q);
+        }
+    }
+    R.sym_ms = sym_best_ms;
+    // stage 2: tile budget x refill CTAs per SM, on the chosen symbolic configuration
+    double best_us = R.default_refill_us;
+    TuneConfig best_cfg = base;
+    bool have_best = false;
+    Product best;
+    const int budgets[] = {TILE_T, 3 * TILE_T / 4, TILE_T / 2};
+    const int ctas[] = {0, 4, 3};
+    for (int b : budgets)
+    {
+        Product Q;
+        TuneConfig c = sym_best;
+        c.tile_budget = b == TILE_T ? 0 : b;
+        if (b == TILE_T && (c.tile_budget == stage1.cfg.tile_budget))
+            Q = std::move(stage1);
+        else
+            build(c, Q);
+        bool kept = false;
+        for (int k : ctas)
+        {
+            Q.cfg.refill_ctas_per_sm = k;
+            const double us = refill_us(Q);
+            if (us < best_us)
+            {
+                best_us = us;
+                best_cfg = Q.cfg;
+                kept = true;
+            }
+        }
+        if (kept)
+        {
+            Q.cfg = best_cfg;
+            best = std::move(Q);
+            have_best = true;
+        }
+    }
+    SDL_CUDA(cudaEventDestroy(e0));
+    SDL_CUDA(cudaEventDestroy(e1));
+    if (have_best)
+    {
+        P = std::move(best);
+        R.best = best_cfg;
+    }
+    else
+        R.best = P.cfg;
+    R.refill_us = best_us;
+    R.tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    return R;
 }
 
 } // namespace sdl

@@ -229,16 +229,27 @@ struct EntChunk
     int prod;
 };
 
+// Run-time parameters of a product's plan (the autotuner picks them per pattern).
 struct TuneConfig
 {
-    // rows whose term count (upper bound of their nnz) is <= warp_cap[k] go to the
-    // warp kernel of capacity class k (32, 128, 512); larger rows go to the CTA
-    // kernels; rows above cta_cap[1] terms are built with the bitmap kernel.
-    int warp_max_terms = 512; // rows above this go to CTA kernels
-    int rows_per_cta_warp = 8; // warps per CTA for the warp kernels
-    int cta_threads_2k = 256;
+    // symbolic pass: rows with at most 32 / 128 / 512 terms go to the warp kernel of
+    // that capacity, rows above warp_max_terms (128 or 512) to the CTA kernels
+    int warp_max_terms = 512;
+    int rows_per_cta_warp = 8;  // warps per CTA of the warp kernels
+    int cta_threads_2k = 256;   // threads of the CTA kernel for rows up to 2048 terms
     int cta_threads_8k = 512;
     int gmem_threads = 512;
+    // refill: weight (terms plus per-row costs) of a row tile, at most TILE_T, and
+    // resident refill CTAs per SM (0: as many as fit)
+    int tile_budget = 0; // 0: TILE_T
+    int refill_ctas_per_sm = 0;
+};
+// Autotuner results: the chosen configuration and what it measured.
+struct TuneResult
+{
+    TuneConfig best;
+    double sym_ms = 0, refill_us = 0, default_refill_us = 0, tune_ms = 0;
+    int candidates = 0;
 };
 
 // Operand description of C = kron(I_blocks, L) diag(d) A.
@@ -285,6 +296,11 @@ struct Product
     DevBuf<long long> row_terms; // ub per row
 };
 
+// Autotuner: re-plans P (built by product_symbolic) for its own pattern. Candidate
+// symbolic configurations are timed on the pattern, then candidate tile budgets and
+// refill CTAs per SM by refills with placeholder values (L2 flushed before each);
+// P ends up planned with the fastest, which is returned with its timings.
+TuneResult product_autotune(Product &P, int reps, cudaStream_t s);
 // Symbolic phase: fills P.Cp, P.Ci, P.nnz and the numeric schedule.
 void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P,
                       cudaStream_t s, bool keep_row_terms = false);
@@ -319,7 +335,8 @@ void append_entry_chunks(long long nV, int prod, int chunk, std::vector<EntChunk
 // tile t reads its pointers from ptrs[tiles[t].prod] / scheds[tiles[t].prod], or,
 // with null tables, from `vals` / `sched`.
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
-                 cudaStream_t s, ProdPtrs vals = ProdPtrs{}, ProdSched sched = ProdSched{});
+                 cudaStream_t s, ProdPtrs vals = ProdPtrs{}, ProdSched sched = ProdSched{},
+                 int ctas_per_sm = 0);
 // Copies `n` descriptors, setting `prod`.
 void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s);
 // The larger rows of one product from their output-major term lists (needs

@@ -76,6 +76,24 @@ class Product:
         check(lib().sdl_product_fill(self.handle, _ptr(Lx), _ptr(d), _ptr(Ax), _ptr(Cx),
                                      _stream(stream)))
 
+    def autotune(self, reps=5, stream=None):
+        """Re-plan for this pattern (sdl_product_autotune); returns tuning()."""
+        check(lib().sdl_product_autotune(self.handle, reps, _stream(stream)))
+        self._init_from_handle(self.handle)
+        return self.tuning()
+
+    def tuning(self):
+        """The plan's configuration and what the autotuner measured."""
+        i = [C.c_int() for _ in range(5)]
+        f = [C.c_double() for _ in range(3)]
+        check(lib().sdl_product_tuning(self.handle, C.byref(i[0]), C.byref(i[1]), C.byref(i[2]),
+                                       C.byref(i[3]), C.byref(f[0]), C.byref(f[1]), C.byref(i[4]),
+                                       C.byref(f[2])))
+        return {"warp_max_terms": i[0].value, "rows_per_cta_warp": i[1].value, "tile_budget": i[2].value,
+                "refill_ctas_per_sm": i[3].value, "refill_us": round(f[0].value, 2),
+                "default_refill_us": round(f[1].value, 2), "candidates": i[4].value,
+                "tune_ms": round(f[2].value, 1)}
+
     def __del__(self):
         try:
             if getattr(self, "handle", None):
@@ -276,4 +294,5 @@ def btda_product(A_p, A_i, A_n, B_p, B_i, B_n, stream=None):
     m = A_p.numel() - 1
     T = Transpose(B_p, B_i, m, B_n, stream=stream)
     P = Product(T.Tp, T.Ti, A_p, A_i, A_n, L_map=T.src, stream=stream)
+    P._owner = T  # the product's L arrays belong to the transpose plan: keep it alive with P
     return P, T
