@@ -20,14 +20,24 @@ struct sdl_transpose
 // Coalescing = group triplets by row (stable transpose of the one-entry-per-row
 // structure rows[]), then a unit-valued row-wise product with the triplet matrix
 // (row t = {(cols[t], x[t])}): each output entry sums its duplicates in ascending
-// triplet order, starting from +0.0, as upstream's row_reduce does.
+// triplet order, starting from +0.0, as upstream's row_reduce does. The product's
+// symbolic pass gives the output structure; value refills gather in output order
+// (coalesce.cu), which sums in the same order.
 struct sdl_coalesce
 {
     int m = 0, n = 0, nnz_in = 0;
     TransposePlan G;
     DevBuf<int> Ap, Ai;
     Product P;
+    DevBuf<int> perm, ostart; // triplets in output order; first slot of every output
 };
+
+namespace sdl {
+void coalesce_order_build(const int *rows, const int *cols, int n, const int *Cp, const int *Ci, int nout,
+                          DevBuf<int> &perm, DevBuf<int> &ostart, cudaStream_t s);
+void coalesce_order_fill(const int *ostart, const int *perm, const double *x, const double *f, int nout, double *C,
+                         cudaStream_t s);
+} // namespace sdl
 
 extern "C" int sdl_device_available(void)
 {
@@ -225,6 +235,7 @@ extern "C" sdl_status sdl_coalesce_create(const int *rows, const int *cols, int 
         d.A_n = n;
         d.A_nnz = nnz_in;
         product_symbolic(d, TuneConfig{}, c->P, s);
+        coalesce_order_build(rows, cols, nnz_in, c->P.Cp.get(), c->P.Ci.get(), c->P.nnz, c->perm, c->ostart, s);
         *out = c.release();
     });
 }
@@ -245,7 +256,7 @@ extern "C" sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, 
 {
     return guard_status("sdl_coalesce_fill", [&]() {
         if (!C) fail(SDL_ERR_INVALID, "NULL plan");
-        product_numeric(C->P, nullptr, nullptr, x, Cx, pick_stream(stream));
+        coalesce_order_fill(C->ostart.get(), C->perm.get(), x, nullptr, C->P.nnz, Cx, pick_stream(stream));
     });
 }
 
@@ -256,6 +267,6 @@ namespace sdl {
 // over its duplicates in ascending t, from +0.0 (d null: x[t]).
 void coalesce_fill_scaled(const sdl_coalesce *C, const double *x, const double *d, double *Cx, cudaStream_t s)
 {
-    product_numeric(C->P, nullptr, d, x, Cx, s);
+    coalesce_order_fill(C->ostart.get(), C->perm.get(), x, d, C->P.nnz, Cx, s);
 }
 } // namespace sdl
