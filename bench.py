@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-conversions", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--split-rows", action="store_true",
+                    help="N > 1: one headline product split by output rows across the ranks "
+                         "(strong scaling) instead of one product per rank (weak scaling)")
     ap.add_argument("--dense-blocks", type=int, default=64,
                     help="blocks of the stacked_pd x CSC case (64 is the configuration; fewer for profiling)")
     ap.add_argument("--learned-matrices", type=int, default=200)
@@ -267,9 +270,18 @@ def run_b200(args, world, rank, local):
     Ap, Ai, Bp, Bi = T(A[0]), T(A[1]), T(B[0]), T(B[1])
     sets = [(T(A[2]), T(B[2]), T(d)), (T(A2x), T(B2x), T(d2))]
 
+    split = args.split_rows and world > 1
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    P, Tr = btda_product(Ap, Ai, A[4], Bp, Bi, B[4])
+    if split:
+        # rows r0..r1 of C on this rank (balanced by terms, the same ranges on every
+        # rank); A, B and d are read whole, C stays row-partitioned
+        from sparsediff_linalg_b200.device import btda_product_rows
+        from sparsediff_linalg_b200.sharding import btda_row_weights, row_ranges
+        r0, r1 = row_ranges(btda_row_weights(A[0], B[0], B[1], B[4]), world)[rank]
+        P, Tr = btda_product_rows(Ap, Ai, A[4], Bp, Bi, B[4], r0, r1)
+    else:
+        P, Tr = btda_product(Ap, Ai, A[4], Bp, Bi, B[4])
     torch.cuda.synchronize()
     symbolic_ms = (time.perf_counter() - t0) * 1e3
     # the product's plan picked by the autotuner on this pattern (timed refills
@@ -278,8 +290,14 @@ def run_b200(args, world, rank, local):
     if not args.no_autotune:
         tune = P.autotune(reps=5, stream=stream)
         torch.cuda.synchronize()
-    Cx = torch.empty(P.nnz, dtype=torch.float64, device=dev)
-    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], P.nnz, B[4])
+    Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev)
+    nnz_C = P.nnz
+    if split:
+        import torch.distributed as dist
+        t = torch.tensor([P.nnz], dtype=torch.int64, device=dev)
+        dist.all_reduce(t)
+        nnz_C = int(t.item())
+    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], nnz_C, B[4])
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     for w in range(args.warmup):
@@ -307,10 +325,11 @@ def run_b200(args, world, rank, local):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     mean_ms = sum(step_ms) / len(step_ms)
     mean_ms_max = allmax(mean_ms)
-    value = world * B_alg / (mean_ms_max * 1e-3) / 1e9
+    # weak: every rank refills a whole product; split: the ranks share one product
+    value = (1 if split else world) * B_alg / (mean_ms_max * 1e-3) / 1e9
 
     peak, peak_kind = peaks()
-    achieved = B_alg / (mean_ms * 1e-3) / 1e9
+    achieved = (B_alg / world if split else B_alg) / (mean_ms * 1e-3) / 1e9
     traffic = None
     tj = ROOT / "profiles" / "btda_refill_traffic.json"
     if tj.exists():
@@ -351,17 +370,19 @@ def run_b200(args, world, rank, local):
 
     # ---- e2e through the upstream C ABI with host buffers
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and not split:
         e2e = run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world)
 
     line = {
         "metric": "btda_refill_hbm_gbs", "value": round(value, 3), "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(mean_ms_max, 5), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": round(mean_ms_max, 5), "higher_is_better": True,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD_NAME, "nnz_C": P.nnz, "terms": P.terms,
+        "config": {"workload": WORKLOAD_NAME, "nnz_C": nnz_C, "terms": P.terms,
                    "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"{world} independent products (one per GPU)" if world > 1 else "1 GPU"},
+                   "parallelism": (f"one product split by output rows over {world} GPUs" if split else
+                                   f"{world} independent products (one per GPU)") if world > 1 else "1 GPU"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_kind": f"{peak_kind} (copy bandwidth)",

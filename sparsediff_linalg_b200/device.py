@@ -296,3 +296,21 @@ def btda_product(A_p, A_i, A_n, B_p, B_i, B_n, stream=None):
     P = Product(T.Tp, T.Ti, A_p, A_i, A_n, L_map=T.src, stream=stream)
     P._owner = T  # the product's L arrays belong to the transpose plan: keep it alive with P
     return P, T
+
+
+def btda_product_rows(A_p, A_i, A_n, B_p, B_i, B_n, r0, r1, transpose=None, stream=None):
+    """Rows r0 .. r1 - 1 of C = B^T D A (columns r0 .. r1 - 1 of B) as a product of
+    their own: L is the slice of B's CSC over those columns, A is whole. Its fill
+    takes the full value arrays (B.x, d, A.x) and writes exactly those rows of C, in
+    the bits of the whole product. `transpose` shares B's transpose plan between the
+    slices (built here when None). Returns (product, transpose)."""
+    m = A_p.numel() - 1
+    T = transpose if transpose is not None else Transpose(B_p, B_i, m, B_n, stream=stream)
+    if not (0 <= r0 <= r1 <= B_n):
+        raise ValueError("row range outside the product")
+    tp = T.Tp[r0:r1 + 1].cpu()
+    s0, s1 = int(tp[0]), int(tp[-1])
+    Lp = torch.as_tensor((tp - s0).to(torch.int32), device=A_p.device)
+    P = Product(Lp, T.Ti[s0:s1], A_p, A_i, A_n, L_map=T.src[s0:s1], stream=stream)
+    P._owner = T
+    return P, T

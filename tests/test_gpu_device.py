@@ -34,6 +34,38 @@ def test_btda_device_fused_csc(sdl, orc):
     assert np.array_equal(bits(Cx.cpu().numpy()), bits(wx))
 
 
+def test_btda_row_slices_equal_the_whole_product(sdl, orc):
+    """A single product split by output rows (as ranks would hold it): the slices'
+    structures and values, concatenated, are the whole product's, bit for bit."""
+    import torch
+    from sparsediff_linalg_b200.device import btda_product, btda_product_rows
+    from sparsediff_linalg_b200.sharding import btda_row_weights, row_ranges
+    rng = np.random.default_rng(22)
+    A = wl.fixed_rowlen_csr(6000, 3000, 8, rng)
+    lens = rng.integers(1, 20, 6000)
+    B = wl.variable_rowlen_csr(6000, 2500, lens, rng)
+    d = rng.uniform(0.1, 10, 6000)
+    P, Tr = btda_product(T(A[0]), T(A[1]), A[4], T(B[0]), T(B[1]), B[4])
+    Cx = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    vals = (T(B[2]), T(d), T(A[2]))
+    P.fill(*vals, Cx)
+    ranges = row_ranges(btda_row_weights(A[0], B[0], B[1], B[4]), 3)
+    cp, ci, cx = [np.zeros(1, np.int32)], [], []
+    for r0, r1 in ranges:
+        Q, _ = btda_product_rows(T(A[0]), T(A[1]), A[4], T(B[0]), T(B[1]), B[4], r0, r1, transpose=Tr)
+        Qx = torch.empty(max(1, Q.nnz), dtype=torch.float64, device="cuda")
+        Q.fill(*vals, Qx)
+        torch.cuda.synchronize()
+        assert Q.m == r1 - r0
+        cp.append(Q.Cp.cpu().numpy()[1:] + cp[-1][-1])
+        ci.append(Q.Ci.cpu().numpy())
+        cx.append(Qx[:Q.nnz].cpu().numpy())
+    torch.cuda.synchronize()
+    assert np.array_equal(np.concatenate(cp), P.Cp.cpu().numpy())
+    assert np.array_equal(np.concatenate(ci), P.Ci.cpu().numpy())
+    assert np.array_equal(bits(np.concatenate(cx)), bits(Cx.cpu().numpy()))
+
+
 def test_kron_blocks(sdl, orc):
     import torch
     from sparsediff_linalg_b200.device import Product

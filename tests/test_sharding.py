@@ -61,3 +61,34 @@ def test_partition_properties(world):
     assert flat == list(range(100))
     loads = [sum(weights[i] for i in s) for s in shards]
     assert max(loads) - min(loads) <= max(weights)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_row_ranges_contiguous_and_balanced(world):
+    import numpy as np
+    from sparsediff_linalg_b200.sharding import row_ranges
+    rng = np.random.default_rng(5)
+    w = rng.integers(0, 300, 10000).astype(float)
+    w[:50] = 5000                                    # a heavy head
+    rr = row_ranges(w, world)
+    assert rr[0][0] == 0 and rr[-1][1] == len(w)
+    assert all(a[1] == b[0] for a, b in zip(rr, rr[1:]))
+    loads = [w[a:b].sum() for a, b in rr]
+    assert max(loads) - min(loads) <= 2 * w.max()
+    assert row_ranges(w, world) == rr                # deterministic
+
+
+def test_btda_row_weights_matches_terms():
+    import numpy as np
+    from sparsediff_linalg_b200 import workloads as wl
+    from sparsediff_linalg_b200.sharding import btda_row_weights
+    rng = np.random.default_rng(6)
+    A = wl.small_random_csr(40, 30, 0.2, rng)
+    B = wl.small_random_csr(40, 25, 0.2, rng)
+    w = btda_row_weights(A[0], B[0], B[1], 25)
+    lens = np.diff(A[0])
+    want = np.zeros(25)
+    for k in range(40):
+        for q in range(B[0][k], B[0][k + 1]):
+            want[B[1][q]] += lens[k]
+    assert np.array_equal(w, want)
