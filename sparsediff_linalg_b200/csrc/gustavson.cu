@@ -1542,8 +1542,6 @@ void build_big_lists(const ProductDesc &d, Product &P, const long long *ub, cons
     P.big_lists = true;
 }
 
-// Everything the refill needs once C's structure is known: row classes, the
-// compiled tile schedule and the larger rows' scratch.
 // Checks every index the tile refill will use, once per schedule: per tile, its
 // window and output range, its words inside the word array, and for every term
 // word that is not a list word its entry, the entry's A position for that term and
@@ -1601,6 +1599,8 @@ __global__ void k_validate_schedule(const TileDesc *__restrict__ tiles, int ntil
     }
 }
 
+// Everything the refill needs once C's structure is known: row classes, the
+// compiled tile schedule and the larger rows' scratch.
 void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
 {
     Runtime &rt = runtime();
