@@ -254,8 +254,29 @@ void validate_compressed(const int *d_p, const int *d_idx, int rows, int cols, i
 
 // ------------------------------------------------------------------ gather
 namespace {
-__global__ void k_gather(const int *__restrict__ src, const double *__restrict__ x,
-                         double *__restrict__ out, int n)
+// out[k] = x[src[k]], four consecutive positions per thread: one 16-byte load of
+// their sources, four independent gathers, two 16-byte stores. The positions and
+// the output are streamed (evict-first), so the gathered array keeps its place in
+// L2 while the permutation revisits it. The last n % 4 positions go to the first
+// threads of the grid.
+__global__ void k_gather(const int4 *__restrict__ src4, const double *__restrict__ x, double2 *__restrict__ out2,
+                         long long n4, const int *__restrict__ src_tail, double *__restrict__ out_tail, int ntail)
+{
+    const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long k = first; k < n4; k += step)
+    {
+        const int4 q = __ldcs(src4 + k);
+        const double a = x[q.x], b = x[q.y], c = x[q.z], d = x[q.w];
+        __stcs(out2 + 2 * k, make_double2(a, b));
+        __stcs(out2 + 2 * k + 1, make_double2(c, d));
+    }
+    if (first < ntail) out_tail[first] = x[src_tail[first]];
+}
+
+// The same for buffers that are not 16-byte aligned.
+__global__ void k_gather_unaligned(const int *__restrict__ src, const double *__restrict__ x,
+                                   double *__restrict__ out, int n)
 {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x)
@@ -267,8 +288,17 @@ void gather_values(const int *d_src, const double *d_x, double *d_out, int n, cu
 {
     if (n <= 0) return;
     Runtime &rt = runtime();
-    int grid = (int)std::min<long long>((n + 255) / 256, (long long)rt.num_sms * 8);
-    SDL_LAUNCH(k_gather, grid, 256, 0, s, d_src, d_x, d_out, n);
+    if (((uintptr_t)d_src | (uintptr_t)d_out) & 15)
+    {
+        int grid = (int)std::min<long long>((n + 255) / 256, (long long)rt.num_sms * 8);
+        SDL_LAUNCH(k_gather_unaligned, grid, 256, 0, s, d_src, d_x, d_out, n);
+        return;
+    }
+    const long long n4 = n / 4;
+    const int ntail = n - (int)(4 * n4);
+    int grid = (int)std::max<long long>(1, std::min<long long>((n4 + 255) / 256, (long long)rt.num_sms * 8));
+    SDL_LAUNCH(k_gather, grid, 256, 0, s, reinterpret_cast<const int4 *>(d_src), d_x,
+               reinterpret_cast<double2 *>(d_out), n4, d_src + 4 * n4, d_out + 4 * n4, ntail);
 }
 
 } // namespace sdl
