@@ -1,14 +1,23 @@
-// Batched refill engine (sdl_batch_*): many products refilled by two launches over
-// the union of their compiled schedules (the entry values of every product, then
-// every product's tiles), replayed from a CUDA graph. The plain alternative -- one
-// sdl_product_fill per product -- pays two launches (and their ramp-up and tail)
-// per product; here all products share one grid and one graph launch. Each
-// product's schedule and entry-value scratch stay where the product keeps them;
-// the kernels find them through per-product pointer tables.
+// Batched refill engine (sdl_batch_*): many products refilled by a few launches
+// over the union of their compiled schedules, replayed from a CUDA graph. The
+// products are cut into consecutive groups whose entry values and entry records
+// fit in L2 next to the next group's; per group, one launch computes the entry
+// values of every product of the group (on a side stream) and one persistent
+// launch refills every tile of the group (on the caller's stream, after it), so
+// the refill reads the entry values from L2 instead of HBM, and the entry values
+// of group g + 1 are computed while group g is refilled (they wait for the refill
+// of group g - 1 only, so they do not run further ahead). The plain alternative --
+// one sdl_product_fill per product -- pays two launches (and their ramp-up and
+// tail) per product. Each product's schedule and entry-value scratch stay where the
+// product keeps them; the kernels find them through per-product pointer tables.
 #include <memory>
 #include <vector>
 
 #include "capi_common.h"
+
+#ifndef SDL_BATCH_GROUP_MB
+#define SDL_BATCH_GROUP_MB 64
+#endif
 
 namespace sdl {
 const Product *product_of(const sdl_product *P);
@@ -30,13 +39,24 @@ struct sdl_batch
     DevBuf<ProdPtrs> ptrs;
     std::vector<ProdPtrs> host_ptrs;
     std::vector<int> with_big; // products that have rows beyond the tile budget
+    // group g: tiles [group_tiles[g], group_tiles[g + 1]) and entry chunks
+    // [group_chunks[g], group_chunks[g + 1])
+    std::vector<int> group_tiles, group_chunks;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    cudaStream_t graph_stream = nullptr;
+    // side stream of the entry-value launches and the events that order them
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    std::vector<cudaEvent_t> entry_done, refill_done; // per group
     ~sdl_batch()
     {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : entry_done) cudaEventDestroy(e);
+        for (cudaEvent_t e : refill_done) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
     }
 };
 
@@ -68,6 +88,12 @@ extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, 
         std::vector<ProdSched> hs(count);
         std::vector<EntChunk> chunks;
         int t_off = 0;
+        // a group closes once its products' entry values and entry records (16 bytes
+        // per entry) reach the budget
+        const long long group_bytes = (long long)SDL_BATCH_GROUP_MB << 20;
+        long long in_group = 0;
+        B->group_tiles.assign(1, 0);
+        B->group_chunks.assign(1, 0);
         for (int i = 0; i < count; ++i)
         {
             const Product *P = B->prods[i];
@@ -77,7 +103,33 @@ extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, 
                 rebase_tiles(P->tiles.get(), P->ntiles, i, B->tiles.get() + t_off, s);
                 t_off += P->ntiles;
             }
-            if ((P->num_count[NUM_TILE] && P->ntiles) || P->big_lists) append_entry_chunks(hs[i].nV, i, 2048, chunks);
+            if ((P->num_count[NUM_TILE] && P->ntiles) || P->big_lists)
+            {
+                append_entry_chunks(hs[i].nV, i, 2048, chunks);
+                in_group += 16 * hs[i].nV;
+            }
+            if (group_bytes > 0 && in_group >= group_bytes)
+            {
+                B->group_tiles.push_back(t_off);
+                B->group_chunks.push_back((int)chunks.size());
+                in_group = 0;
+            }
+        }
+        if (t_off > B->group_tiles.back() || (int)chunks.size() > B->group_chunks.back())
+        {
+            B->group_tiles.push_back(t_off);
+            B->group_chunks.push_back((int)chunks.size());
+        }
+        SDL_CUDA(cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking));
+        SDL_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+        SDL_CUDA(cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming));
+        const size_t ngroups = B->group_tiles.size() - 1;
+        B->entry_done.assign(ngroups, nullptr);
+        B->refill_done.assign(ngroups, nullptr);
+        for (size_t g = 0; g < ngroups; ++g)
+        {
+            SDL_CUDA(cudaEventCreateWithFlags(&B->entry_done[g], cudaEventDisableTiming));
+            SDL_CUDA(cudaEventCreateWithFlags(&B->refill_done[g], cudaEventDisableTiming));
         }
         if (count)
             SDL_CUDA(cudaMemcpyAsync(B->scheds.get(), hs.data(), count * sizeof(ProdSched),
@@ -115,8 +167,21 @@ extern "C" sdl_status sdl_batch_refill(sdl_batch *B, void *stream)
         if (s == cudaStreamLegacy)
             fail(SDL_ERR_INVALID, "batched refills need a non-default stream (graph capture)");
         auto enqueue = [&]() {
-            entry_values_batched(B->chunks.get(), B->nchunks, B->ptrs.get(), B->scheds.get(), s);
-            tile_refill(B->tiles.get(), B->ntiles, B->ptrs.get(), B->scheds.get(), s);
+            SDL_CUDA(cudaEventRecord(B->fork, s));
+            SDL_CUDA(cudaStreamWaitEvent(B->side, B->fork, 0));
+            for (size_t g = 0; g < B->entry_done.size(); ++g)
+            {
+                const int c0 = B->group_chunks[g], t0 = B->group_tiles[g];
+                if (g >= 2) SDL_CUDA(cudaStreamWaitEvent(B->side, B->refill_done[g - 2], 0));
+                entry_values_batched(B->chunks.get() + c0, B->group_chunks[g + 1] - c0, B->ptrs.get(),
+                                     B->scheds.get(), B->side);
+                SDL_CUDA(cudaEventRecord(B->entry_done[g], B->side));
+                SDL_CUDA(cudaStreamWaitEvent(s, B->entry_done[g], 0));
+                tile_refill(B->tiles.get() + t0, B->group_tiles[g + 1] - t0, B->ptrs.get(), B->scheds.get(), s);
+                SDL_CUDA(cudaEventRecord(B->refill_done[g], s));
+            }
+            SDL_CUDA(cudaEventRecord(B->join, B->side));
+            SDL_CUDA(cudaStreamWaitEvent(s, B->join, 0));
             for (int i : B->with_big)
             {
                 const ProdPtrs &pp = B->host_ptrs[i];
