@@ -132,11 +132,13 @@ sdl_status sdl_product_fill_noalloc(const sdl_product *P, const double *Lx, cons
                                     const double *Ax, double *Cx, void *stream);
 
 /* ------------------------------------------------------------------------
-   Batched refill: many products (uneven sizes, fixed patterns) refilled by one
-   persistent launch over the union of their compiled tile schedules, captured
-   into a CUDA graph on the first refill and replayed afterwards. Rows with more
-   than the tile budget of terms are refilled by per-product launches inside the
-   same graph.
+   Batched refill: many products (uneven sizes, fixed patterns) refilled by a few
+   persistent launches over the union of their compiled tile schedules, captured
+   into a CUDA graph on the first refill and replayed afterwards. The products are
+   cut, in order, into groups whose entry values and entry records (16 bytes per
+   entry) reach a size (64 MiB by default); each group's entry values are computed
+   on a side stream while the previous group is refilled. Rows with more than the
+   tile budget of terms are refilled by per-product launches inside the same graph.
    ------------------------------------------------------------------------ */
 typedef struct sdl_batch sdl_batch;
 /* The products must outlive the batch. Synchronises the stream. */
@@ -147,6 +149,11 @@ sdl_status sdl_batch_create(sdl_product *const *products, int count, void *strea
    the pointers from a device table. */
 sdl_status sdl_batch_bind(sdl_batch *B, int i, const double *Lx, const double *d,
                           const double *Ax, double *Cx);
+/* Bytes of entry values and records per group (0: one group for the whole batch).
+   Only before the first sdl_batch_refill. */
+sdl_status sdl_batch_set_group_bytes(sdl_batch *B, long long bytes);
+/* Number of product groups of the batch. */
+sdl_status sdl_batch_groups(const sdl_batch *B, int *groups);
 /* One refill of every product of the batch, asynchronous on the stream. */
 sdl_status sdl_batch_refill(sdl_batch *B, void *stream);
 /* The same refill as sdl_batch_refill done the plain way: one sdl_product_fill

@@ -107,6 +107,8 @@ EXTENSION_SIGNATURES = {
     "sdl_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, vp, C.POINTER(vp)]),
     "sdl_batch_bind": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
     "sdl_batch_refill": (C.c_int, [vp, vp]),
+    "sdl_batch_set_group_bytes": (C.c_int, [vp, C.c_longlong]),
+    "sdl_batch_groups": (C.c_int, [vp, c_int_p]),
     "sdl_batch_refill_unbatched": (C.c_int, [vp, vp]),
     "sdl_batch_info": (C.c_int, [vp, c_int_p, c_int_p, C.POINTER(C.c_longlong)]),
     "sdl_batch_destroy": (None, [vp]),

@@ -15,9 +15,8 @@
 
 #include "capi_common.h"
 
-#ifndef SDL_BATCH_GROUP_MB
-#define SDL_BATCH_GROUP_MB 64
-#endif
+// default bytes of entry values and entry records (16 per entry) of a group
+constexpr long long kGroupBytes = 64LL << 20;
 
 namespace sdl {
 const Product *product_of(const sdl_product *P);
@@ -39,8 +38,12 @@ struct sdl_batch
     DevBuf<ProdPtrs> ptrs;
     std::vector<ProdPtrs> host_ptrs;
     std::vector<int> with_big; // products that have rows beyond the tile budget
+    // per product: end of its tiles / entry chunks, bytes of its entry values and records
+    std::vector<int> prod_tile_end, prod_chunk_end;
+    std::vector<long long> prod_bytes;
     // group g: tiles [group_tiles[g], group_tiles[g + 1]) and entry chunks
     // [group_chunks[g], group_chunks[g + 1])
+    long long group_bytes = kGroupBytes;
     std::vector<int> group_tiles, group_chunks;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -48,17 +51,59 @@ struct sdl_batch
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     std::vector<cudaEvent_t> entry_done, refill_done; // per group
+    void drop_group_events()
+    {
+        for (cudaEvent_t e : entry_done) cudaEventDestroy(e);
+        for (cudaEvent_t e : refill_done) cudaEventDestroy(e);
+        entry_done.clear();
+        refill_done.clear();
+    }
     ~sdl_batch()
     {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        for (cudaEvent_t e : entry_done) cudaEventDestroy(e);
-        for (cudaEvent_t e : refill_done) cudaEventDestroy(e);
+        drop_group_events();
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);
     }
 };
+
+namespace {
+// Cuts the products, in order, into groups: a group closes once its products'
+// entry values and records reach B.group_bytes (0: one group).
+void make_groups(sdl_batch &B)
+{
+    B.group_tiles.assign(1, 0);
+    B.group_chunks.assign(1, 0);
+    long long in_group = 0;
+    const size_t n = B.prods.size();
+    for (size_t i = 0; i < n; ++i)
+    {
+        in_group += B.prod_bytes[i];
+        if (B.group_bytes > 0 && in_group >= B.group_bytes)
+        {
+            B.group_tiles.push_back(B.prod_tile_end[i]);
+            B.group_chunks.push_back(B.prod_chunk_end[i]);
+            in_group = 0;
+        }
+    }
+    if (B.ntiles > B.group_tiles.back() || B.nchunks > B.group_chunks.back())
+    {
+        B.group_tiles.push_back(B.ntiles);
+        B.group_chunks.push_back(B.nchunks);
+    }
+    B.drop_group_events();
+    const size_t ngroups = B.group_tiles.size() - 1;
+    B.entry_done.assign(ngroups, nullptr);
+    B.refill_done.assign(ngroups, nullptr);
+    for (size_t g = 0; g < ngroups; ++g)
+    {
+        SDL_CUDA(cudaEventCreateWithFlags(&B.entry_done[g], cudaEventDisableTiming));
+        SDL_CUDA(cudaEventCreateWithFlags(&B.refill_done[g], cudaEventDisableTiming));
+    }
+}
+} // namespace
 
 extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, void *stream,
                                        sdl_batch **out)
@@ -88,12 +133,9 @@ extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, 
         std::vector<ProdSched> hs(count);
         std::vector<EntChunk> chunks;
         int t_off = 0;
-        // a group closes once its products' entry values and entry records (16 bytes
-        // per entry) reach the budget
-        const long long group_bytes = (long long)SDL_BATCH_GROUP_MB << 20;
-        long long in_group = 0;
-        B->group_tiles.assign(1, 0);
-        B->group_chunks.assign(1, 0);
+        B->prod_tile_end.assign(count, 0);
+        B->prod_chunk_end.assign(count, 0);
+        B->prod_bytes.assign(count, 0);
         for (int i = 0; i < count; ++i)
         {
             const Product *P = B->prods[i];
@@ -106,41 +148,43 @@ extern "C" sdl_status sdl_batch_create(sdl_product *const *products, int count, 
             if ((P->num_count[NUM_TILE] && P->ntiles) || P->big_lists)
             {
                 append_entry_chunks(hs[i].nV, i, 2048, chunks);
-                in_group += 16 * hs[i].nV;
+                B->prod_bytes[i] = 16 * hs[i].nV;
             }
-            if (group_bytes > 0 && in_group >= group_bytes)
-            {
-                B->group_tiles.push_back(t_off);
-                B->group_chunks.push_back((int)chunks.size());
-                in_group = 0;
-            }
-        }
-        if (t_off > B->group_tiles.back() || (int)chunks.size() > B->group_chunks.back())
-        {
-            B->group_tiles.push_back(t_off);
-            B->group_chunks.push_back((int)chunks.size());
+            B->prod_tile_end[i] = t_off;
+            B->prod_chunk_end[i] = (int)chunks.size();
         }
         SDL_CUDA(cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking));
         SDL_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
         SDL_CUDA(cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming));
-        const size_t ngroups = B->group_tiles.size() - 1;
-        B->entry_done.assign(ngroups, nullptr);
-        B->refill_done.assign(ngroups, nullptr);
-        for (size_t g = 0; g < ngroups; ++g)
-        {
-            SDL_CUDA(cudaEventCreateWithFlags(&B->entry_done[g], cudaEventDisableTiming));
-            SDL_CUDA(cudaEventCreateWithFlags(&B->refill_done[g], cudaEventDisableTiming));
-        }
         if (count)
             SDL_CUDA(cudaMemcpyAsync(B->scheds.get(), hs.data(), count * sizeof(ProdSched),
                                      cudaMemcpyHostToDevice, s));
         B->nchunks = (int)chunks.size();
+        make_groups(*B);
         B->chunks.reset(std::max<size_t>(1, chunks.size()));
         if (!chunks.empty())
             SDL_CUDA(cudaMemcpyAsync(B->chunks.get(), chunks.data(), chunks.size() * sizeof(EntChunk),
                                      cudaMemcpyHostToDevice, s));
         SDL_CUDA(cudaStreamSynchronize(s));
         *out = B.release();
+    });
+}
+
+extern "C" sdl_status sdl_batch_set_group_bytes(sdl_batch *B, long long bytes)
+{
+    return guard_status("sdl_batch_set_group_bytes", [&]() {
+        if (!B || bytes < 0) fail(SDL_ERR_INVALID, "bad batch or group size");
+        if (B->exec) fail(SDL_ERR_INVALID, "the batch has been refilled: its groups are fixed");
+        B->group_bytes = bytes;
+        make_groups(*B);
+    });
+}
+
+extern "C" sdl_status sdl_batch_groups(const sdl_batch *B, int *groups)
+{
+    return guard_status("sdl_batch_groups", [&]() {
+        if (!B || !groups) fail(SDL_ERR_INVALID, "NULL argument");
+        *groups = (int)B->entry_done.size();
     });
 }
 

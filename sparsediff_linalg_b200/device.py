@@ -253,8 +253,8 @@ class BlocksAta:
 
 
 class Batch:
-    """Batched refill of many products: one persistent launch over all their tiles,
-    replayed from a CUDA graph (sdl_batch_*)."""
+    """Batched refill of many products: a few grouped persistent launches over all
+    their tiles, replayed from a CUDA graph (sdl_batch_*)."""
 
     def __init__(self, products, stream=None):
         L = lib()
@@ -267,6 +267,17 @@ class Batch:
         check(L.sdl_batch_info(h, C.byref(t), C.byref(b), C.byref(n)))
         self.tiles, self.big_rows, self.terms = t.value, b.value, n.value
         self._bound = {}
+
+    def set_group_bytes(self, nbytes):
+        """Bytes of entry values and records per product group (0: one group);
+        only before the first refill."""
+        check(lib().sdl_batch_set_group_bytes(self.handle, int(nbytes)))
+
+    @property
+    def groups(self):
+        g = C.c_int()
+        check(lib().sdl_batch_groups(self.handle, C.byref(g)))
+        return g.value
 
     def bind(self, i, Lx, d, Ax, Cx):
         self._bound[i] = (Lx, d, Ax, Cx)

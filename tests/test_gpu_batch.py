@@ -1,5 +1,7 @@
-"""Batched refill engine: one persistent launch (graph-replayed) over many
-products gives exactly the bits of each product's own refill, and of the oracle."""
+"""Batched refill engine: grouped persistent launches (graph-replayed) over many
+products give exactly the bits of each product's own refill, and of the oracle,
+with one group, the default groups and a group per few products (the entry
+values of the next group computed on the side stream while a group refills)."""
 import numpy as np
 import pytest
 
@@ -8,7 +10,8 @@ from sparsediff_linalg_b200 import workloads as wl
 pytestmark = pytest.mark.gpu
 
 
-def test_batch_matches_per_product_fills(sdl, orc):
+@pytest.mark.parametrize("group_bytes", [None, 0, 1 << 19])
+def test_batch_matches_per_product_fills(sdl, orc, group_bytes):
     import torch
     from sparsediff_linalg_b200.device import Batch, btda_product
     inst = wl.batched_device(seed=11, count=24, lo=200, hi=6000)
@@ -19,6 +22,12 @@ def test_batch_matches_per_product_fills(sdl, orc):
         outs.append(torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda"))
         refs.append(torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda"))
     B = Batch([p for p, _ in prods])
+    if group_bytes is not None:
+        B.set_group_bytes(group_bytes)
+    if group_bytes == 0:
+        assert B.groups == 1
+    if group_bytes == 1 << 19:
+        assert B.groups >= 5
     s = torch.cuda.Stream()
     gen = torch.Generator(device="cuda")
     gen.manual_seed(5)
@@ -55,3 +64,6 @@ def test_batch_matches_per_product_fills(sdl, orc):
         B.refill_unbatched(stream=s)
     s.synchronize()
     assert np.array_equal(outs[3][:P.nnz].cpu().numpy().view(np.int64), wx.view(np.int64))
+    # the groups are fixed once the graph exists
+    with pytest.raises(Exception):
+        B.set_group_bytes(0)
