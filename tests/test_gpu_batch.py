@@ -67,3 +67,57 @@ def test_batch_matches_per_product_fills(sdl, orc, group_bytes):
     # the groups are fixed once the graph exists
     with pytest.raises(Exception):
         B.set_group_bytes(0)
+
+
+def test_batch_with_heavy_rows_and_unit_products(sdl):
+    """Products with rows beyond the tile budget (heavy-row term lists), a unit-valued
+    product and small B^T D A products in one batch cut into several groups: every
+    output is bit-identical to the product's own fill, eagerly and from the graph."""
+    import torch
+    from sparsediff_linalg_b200.device import Batch, Product, btda_product
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(9)
+    prods, keep, vals = [], [], []
+    for seed in (41, 42):
+        (Ap, Ai, Ax), (Bp, Bi, Bx), _ = wl.skewed_device(seed=seed, m=6000, n=6000, target=120_000, cap=2000)
+        keep.append((Ap, Ai, Bp, Bi))
+        prods.append(Product(Ap, Ai, Bp, Bi, 6000))
+        vals.append(lambda Ai=Ai, Bi=Bi: (torch.randn(Ai.numel(), generator=gen, device="cuda",
+                                                      dtype=torch.float64), None,
+                                          torch.randn(Bi.numel(), generator=gen, device="cuda",
+                                                      dtype=torch.float64)))
+    # the last structure again, unit-valued (no L values, no d)
+    Ap, Ai, Bp, Bi = keep[-1]
+    prods.append(Product(Ap, Ai, Bp, Bi, 6000))
+    vals.append(lambda Bi=Bi: (None, None, torch.randn(Bi.numel(), generator=gen, device="cuda",
+                                                       dtype=torch.float64)))
+    for k in wl.batched_device(seed=12, count=6, lo=300, hi=3000):
+        P, T = btda_product(k["Ap"], k["Ai"], k["n"], k["Bp"], k["Bi"], k["n"])
+        keep.append(T)
+        prods.append(P)
+        vals.append(lambda k=k: (torch.randn(k["Bi"].numel(), generator=gen, device="cuda", dtype=torch.float64),
+                                 torch.rand(k["m"], generator=gen, device="cuda", dtype=torch.float64) + 0.5,
+                                 torch.randn(k["Ai"].numel(), generator=gen, device="cuda",
+                                             dtype=torch.float64)))
+    B = Batch(prods)
+    assert B.big_rows > 0
+    B.set_group_bytes(1 << 18)
+    assert B.groups >= 3
+    outs = [torch.full((max(1, P.nnz),), float("nan"), dtype=torch.float64, device="cuda") for P in prods]
+    refs = [torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda") for P in prods]
+    s = torch.cuda.Stream()
+    for rnd in range(3):
+        cur = [v() for v in vals]
+        for i, (lx, d, ax) in enumerate(cur):
+            B.bind(i, lx, d, ax, outs[i])
+        with torch.cuda.stream(s):
+            B.refill(stream=s)
+        s.synchronize()
+        for i, P in enumerate(prods):
+            lx, d, ax = cur[i]
+            P.fill(lx, d, ax, refs[i])
+        torch.cuda.synchronize()
+        for i, P in enumerate(prods):
+            got = outs[i][:P.nnz].cpu().numpy().view(np.int64)
+            want = refs[i][:P.nnz].cpu().numpy().view(np.int64)
+            assert np.array_equal(got, want), f"round {rnd}, product {i}"
