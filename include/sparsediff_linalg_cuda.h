@@ -146,7 +146,8 @@ sdl_status sdl_batch_create(sdl_product *const *products, int count, void *strea
                             sdl_batch **out);
 /* Device value arrays of product i used by the following refills (as in
    sdl_product_fill). Rebinding after the first refill is allowed: the graph reads
-   the pointers from a device table. */
+   the pointers from a device table. The table is written synchronously, so rebind
+   only while no refill of the batch is in flight. */
 sdl_status sdl_batch_bind(sdl_batch *B, int i, const double *Lx, const double *d,
                           const double *Ax, double *Cx);
 /* Bytes of entry values and records per group (0: one group for the whole batch).
