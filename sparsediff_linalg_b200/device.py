@@ -325,3 +325,43 @@ def btda_product_rows(A_p, A_i, A_n, B_p, B_i, B_n, r0, r1, transpose=None, stre
     P = Product(Lp, T.Ti[s0:s1], A_p, A_i, A_n, L_map=T.src[s0:s1], stream=stream)
     P._owner = T
     return P, T
+
+
+def spgemm_product_rows(A_p, A_i, B_p, B_i, B_n, r0, r1, stream=None):
+    """Rows r0 .. r1 - 1 of C = A B as a product of their own: L is the slice of A's
+    rows, B is whole. Returns (product, (s0, s1)): its fill takes A.x[s0:s1] as the
+    L values and the whole B.x, and writes exactly those rows of C, in the bits of
+    the whole product."""
+    m = A_p.numel() - 1
+    if not (0 <= r0 <= r1 <= m):
+        raise ValueError("row range outside the product")
+    ap = A_p[r0:r1 + 1].cpu()
+    s0, s1 = int(ap[0]), int(ap[-1])
+    Lp = torch.as_tensor((ap - s0).to(torch.int32), device=A_p.device)
+    Li = A_i[s0:s1]
+    P = Product(Lp, Li, B_p, B_i, B_n, stream=stream)
+    return P, (s0, s1)
+
+
+class KeyGrouping:
+    """Stable grouping of positions 0 .. N-1 by int32 keys in [0, nkeys): the
+    library's stable transpose of the one-entry-per-row structure. `offsets`
+    (nkeys + 1), `perm` (positions in key order, ties in position order),
+    `gather(x)` = x[perm] for float64 x (the library's value gather)."""
+
+    def __init__(self, keys, nkeys, stream=None):
+        n = int(keys.numel())
+        self._p = torch.arange(n + 1, dtype=torch.int32, device=keys.device)
+        self._t = Transpose(self._p, keys.contiguous(), n, nkeys, stream=stream)
+        self.offsets = self._t.Tp
+        self.perm = self._t.src
+
+    def gather(self, x, stream=None):
+        out = torch.empty(max(1, int(self.perm.numel())), dtype=torch.float64, device=x.device)
+        if self.perm.numel():
+            self._t.fill(x.contiguous(), out, stream=stream)
+        return out[:int(self.perm.numel())]
+
+
+def group_by_key(keys, nkeys):
+    return KeyGrouping(keys, nkeys)

@@ -66,6 +66,32 @@ def test_btda_row_slices_equal_the_whole_product(sdl, orc):
     assert np.array_equal(bits(np.concatenate(cx)), bits(Cx.cpu().numpy()))
 
 
+def test_spgemm_row_slices_equal_the_whole_product(sdl):
+    """C = A B of skewed operands (rows beyond the tile budget included) split by
+    output rows: the slices, concatenated, are the whole product bit for bit."""
+    import torch
+    from sparsediff_linalg_b200.device import Product, spgemm_product_rows
+    from sparsediff_linalg_b200.sharding import row_ranges, spgemm_row_weights
+    (Ap, Ai, Ax), (Bp, Bi, Bx), _ = wl.skewed_device(seed=31, m=8000, n=8000, target=160_000, cap=3000)
+    P = Product(Ap, Ai, Bp, Bi, 8000)
+    Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda")
+    P.fill(Ax, None, Bx, Cx)
+    ranges = row_ranges(spgemm_row_weights(Ap.cpu().numpy(), Ai.cpu().numpy(), Bp.cpu().numpy()), 3)
+    cp, ci, cx = [np.zeros(1, np.int32)], [], []
+    for r0, r1 in ranges:
+        Q, (s0, s1) = spgemm_product_rows(Ap, Ai, Bp, Bi, 8000, r0, r1)
+        Qx = torch.empty(max(1, Q.nnz), dtype=torch.float64, device="cuda")
+        Q.fill(Ax[s0:s1], None, Bx, Qx)
+        torch.cuda.synchronize()
+        assert Q.m == r1 - r0
+        cp.append(Q.Cp.cpu().numpy()[1:] + cp[-1][-1])
+        ci.append(Q.Ci.cpu().numpy())
+        cx.append(Qx[:Q.nnz].cpu().numpy())
+    assert np.array_equal(np.concatenate(cp), P.Cp.cpu().numpy())
+    assert np.array_equal(np.concatenate(ci), P.Ci.cpu().numpy())
+    assert np.array_equal(bits(np.concatenate(cx)), bits(Cx[:P.nnz].cpu().numpy()))
+
+
 def test_kron_blocks(sdl, orc):
     import torch
     from sparsediff_linalg_b200.device import Product
@@ -115,3 +141,41 @@ def test_btda_full_size_config(sdl, orc):
     assert P.nnz == len(wi)
     assert np.array_equal(P.Cp.cpu().numpy(), wp) and np.array_equal(P.Ci.cpu().numpy(), wi)
     assert np.array_equal(bits(Cx.cpu().numpy()), bits(wx))
+
+
+def test_sharded_csr_to_csc_one_rank_nccl(sdl):
+    """The column-partitioned conversion on one NCCL rank with the library's stable
+    grouping (its all-to-all exchanges stay on the device): the same CSC as the
+    one-GPU transpose, bit for bit, and the same values after a refill."""
+    import socket
+    import torch
+    import torch.distributed as dist
+    from sparsediff_linalg_b200.device import Transpose, group_by_key
+    from sparsediff_linalg_b200.sharding import ShardedCsrToCsc
+    rng = np.random.default_rng(44)
+    m, n = 3000, 2200
+    A = wl.variable_rowlen_csr(m, n, rng.integers(0, 12, m), rng)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        p, i, x = T(A[0]), T(A[1]), T(A[2])
+        S = ShardedCsrToCsc(p, i, 0, m, n, group_by_key, dist)
+        tx = S.fill(x)
+        R = Transpose(p, i, m, n)
+        rx = torch.empty(max(1, i.numel()), dtype=torch.float64, device="cuda")
+        R.fill(x, rx)
+        torch.cuda.synchronize()
+        assert (S.c0, S.c1) == (0, n)
+        assert np.array_equal(S.Tp.cpu().numpy(), R.Tp.cpu().numpy())
+        assert np.array_equal(S.Ti.cpu().numpy(), R.Ti.cpu().numpy())
+        assert np.array_equal(bits(tx.cpu().numpy()), bits(rx[:i.numel()].cpu().numpy()))
+        x2 = x * -3.0
+        tx2 = S.fill(x2)
+        R.fill(x2, rx)
+        torch.cuda.synchronize()
+        assert np.array_equal(bits(tx2.cpu().numpy()), bits(rx[:i.numel()].cpu().numpy()))
+    finally:
+        dist.destroy_process_group()
