@@ -451,9 +451,9 @@ def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world):
 
 def run_batched(args, dev, refills=20):
     """512 uneven B^T D A instances (rows log-uniform 1k..64k, cols = rows / 2, 4..16
-    nnz per row), fixed patterns, `refills` value refills: batched (one persistent
-    launch per refill, replayed from a CUDA graph) vs plain (one refill launch per
-    product). Inputs total several GB, far above L2, so no flush is needed."""
+    nnz per row), fixed patterns, `refills` value refills: batched (grouped
+    persistent launches per refill, replayed from a CUDA graph) vs plain (one
+    refill per product). Inputs total several GB, far above L2, so no flush is needed."""
     import torch
     from sparsediff_linalg_b200 import workloads as wl
     from sparsediff_linalg_b200.device import Batch, btda_product
@@ -512,7 +512,7 @@ def run_batched(args, dev, refills=20):
     ms_batched = timed(lambda st: Bt.refill(stream=st))
     ms_plain = timed(lambda st: Bt.refill_unbatched(stream=st))
     terms = sum(p.terms for p, _ in prods)
-    return {"instances": len(inst), "refills": refills, "tiles": Bt.tiles,
+    return {"instances": len(inst), "refills": refills, "tiles": Bt.tiles, "groups": Bt.groups,
             "rows": int(sum(k["m"] for k in inst)),
             "nnz_A": int(sum(k["Ai"].numel() for k in inst)), "terms": int(terms),
             "nnz_C": int(sum(p.nnz for p, _ in prods)), "algorithmic_bytes": int(B_alg),
