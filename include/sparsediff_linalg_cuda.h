@@ -103,8 +103,10 @@ void sdl_product_destroy(sdl_product *P);
    and values are unchanged; only the schedule moves). Candidate symbolic bin
    thresholds (warp-kernel row limit 128 / 512 terms, 4 / 8 / 16 warps per CTA)
    are timed on the pattern; then candidate tile budgets (TILE_T, 3/4, 1/2 of it)
-   and resident refill CTAs per SM (all that fit, 4, 3) by `reps` refills each
-   with placeholder values, L2 flushed before each; P keeps the fastest plan
+   and resident refill CTAs per SM (all that fit, 4, 3), and the small-tile
+   refill (128-thread CTAs over tiles and tile rows of at most TILE_T / 2 terms),
+   by `reps` refills each with placeholder values, L2 flushed before each; P keeps
+   the fastest plan
    (the as-given plan unless a candidate beats it). The row offsets / column
    indices sdl_product_info returned before are released: ask again. Allocates;
    synchronises the stream. */
@@ -115,6 +117,17 @@ sdl_status sdl_product_autotune(sdl_product *P, int reps, void *stream);
 sdl_status sdl_product_tuning(const sdl_product *P, int *warp_max_terms, int *rows_per_cta_warp,
                               int *tile_budget, int *refill_ctas_per_sm, double *refill_us,
                               double *default_refill_us, int *candidates, double *tune_ms);
+/* Re-plans P with a given refill configuration (structure unchanged): tile budget
+   and largest tile row in terms (0: TILE_T = 1024), refill CTA threads (256, or 128:
+   used when every tile window fits the small-tile refill, i.e. budget and largest
+   row at most 512), resident refill CTAs per SM (0: all that fit). The row offsets
+   / column indices sdl_product_info returned before are released. Allocates;
+   synchronises the stream. */
+sdl_status sdl_product_replan(sdl_product *P, int tile_budget, int tile_max_terms, int refill_threads,
+                              int refill_ctas_per_sm, void *stream);
+/* Threads of P's refill CTAs (256, or 128 for the small-tile refill) and the largest
+   row (terms) its tiles take. Any pointer may be NULL. */
+sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, int *tile_max_terms);
 
 /* No upstream counterpart. Same result as sdl_product_fill, bit for bit, for
    callers that cannot call cudaMalloc while they refill: device memory wholly

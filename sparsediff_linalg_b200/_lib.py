@@ -102,6 +102,8 @@ EXTENSION_SIGNATURES = {
     "sdl_product_autotune": (C.c_int, [vp, C.c_int, vp]),
     "sdl_product_tuning": (C.c_int, [vp, c_int_p, c_int_p, c_int_p, c_int_p, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), c_int_p, C.POINTER(C.c_double)]),
+    "sdl_product_refill_shape": (C.c_int, [vp, c_int_p, c_int_p]),
+    "sdl_product_replan": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]),
     "sdl_product_destroy": (None, [vp]),
     "sdl_product_fill_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp]),
     "sdl_batch_create": (C.c_int, [C.POINTER(vp), C.c_int, vp, C.POINTER(vp)]),

@@ -126,6 +126,30 @@ extern "C" sdl_status sdl_product_tuning(const sdl_product *P, int *warp_max_ter
     });
 }
 
+extern "C" sdl_status sdl_product_replan(sdl_product *P, int tile_budget, int tile_max_terms,
+                                         int refill_threads, int refill_ctas_per_sm, void *stream)
+{
+    return guard_status("sdl_product_replan", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        TuneConfig c = P->P.cfg;
+        c.tile_budget = tile_budget;
+        c.tile_max_terms = tile_max_terms;
+        c.refill_threads = refill_threads;
+        c.refill_ctas_per_sm = refill_ctas_per_sm;
+        product_replan(P->P, c, pick_stream(stream));
+    });
+}
+
+extern "C" sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, int *tile_max_terms)
+{
+    return guard_status("sdl_product_refill_shape", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        const TuneConfig &c = P->P.cfg;
+        if (refill_threads) *refill_threads = small_tile_refill(P->P) ? c.refill_threads : 256;
+        if (tile_max_terms) *tile_max_terms = c.tile_max_terms > 0 ? c.tile_max_terms : TILE_T;
+    });
+}
+
 extern "C" sdl_status sdl_product_info(const sdl_product *P, int *m, int *n, int *nnz,
                                        long long *terms, const int **Cp, const int **Ci)
 {

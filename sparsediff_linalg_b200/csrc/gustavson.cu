@@ -149,7 +149,7 @@ __global__ void k_mask_classes(const unsigned char *__restrict__ mask, int m_out
 // entries never join a tile (the 18-bit entry index of a term word stays in range).
 constexpr int TILE_MAX_LROW = 131072;
 __global__ void k_num_classify(const long long *__restrict__ ub, const int *__restrict__ Cp,
-                               const int *__restrict__ Lp, int L_m, int m_out,
+                               const int *__restrict__ Lp, int L_m, int m_out, int tile_max,
                                unsigned char *__restrict__ cls, long long *__restrict__ weight)
 {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
@@ -162,7 +162,7 @@ __global__ void k_num_classify(const long long *__restrict__ ub, const int *__re
         int c;
         if (u == 0)
             c = 255;
-        else if (u <= TILE_T && lenL <= TILE_MAX_LROW)
+        else if (u <= tile_max && lenL <= TILE_MAX_LROW)
             c = NUM_TILE;
         else if (nr <= 2048)
             c = NUM_C2K;
@@ -741,7 +741,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tile_schedule(
 // i = b * L_nnz + (index of the value), so L.x is read in order and kv gives the
 // entry's row of A; otherwise i = b * L_nnz + ii. Each thread takes EV_ILP entries,
 // spaced one grid apart, and issues all their loads before the first store.
-constexpr int EV_ILP = 4;
+#ifndef SDL_EV_ILP
+#define SDL_EV_ILP 4
+#endif
+constexpr int EV_ILP = SDL_EV_ILP;
 __device__ __forceinline__ void entry_values_run(const ProdSched &S, const ProdPtrs &P, long long first,
                                                  long long end, long long step)
 {
@@ -810,10 +813,24 @@ __global__ void __launch_bounds__(256) k_entry_values_batched(const EntChunk *__
 #ifndef SDL_REFILL_UNROLL
 #define SDL_REFILL_UNROLL 4
 #endif
-constexpr int REFILL_THREADS = 256;
 constexpr int RUNROLL = SDL_REFILL_UNROLL; // terms per thread whose loads are in flight together
-constexpr int RSTEP = RUNROLL * REFILL_THREADS;
-constexpr int WIN = TILE_ACC; // outputs of a tile window
+// Refill CTAs: 256 threads with windows of TILE_ACC outputs (every plan; the batched
+// refill), or 128 threads with windows of TILE_ACC / 2 for plans whose tiles have at
+// most that many outputs (tile budget and tile rows of at most TILE_T / 2 terms: a
+// tile then holds fewer than TILE_T terms), twice as many CTAs per SM and a barrier
+// among 4 warps instead of 8.
+constexpr int REFILL_THREADS = 256;
+constexpr int REFILL_THREADS_SMALL = 128;
+template <int NT>
+__host__ __device__ constexpr int win_of()
+{
+    return NT == REFILL_THREADS ? TILE_ACC : TILE_ACC / 2;
+}
+template <int NT>
+__host__ __device__ constexpr int refill_minb()
+{
+    return NT == REFILL_THREADS ? SDL_REFILL_MINB : 2 * SDL_REFILL_MINB;
+}
 
 
 // Base pointers of the product a tile belongs to: kernel parameters for a single
@@ -860,18 +877,20 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
 
 // Shared memory of a refill CTA: two windows, a ring of four tile descriptors and,
 // for batched refills, the resolved base pointers of each descriptor's product.
+template <int NT>
 __host__ __device__ constexpr size_t refill_smem_bytes()
 {
-    return 2 * (size_t)WIN * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase);
+    return 2 * (size_t)win_of<NT>() * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase);
 }
 
+template <int NT>
 __device__ __forceinline__ void load_terms(const unsigned *__restrict__ W, int nterms, int base,
                                            unsigned (&w)[RUNROLL])
 {
 #pragma unroll
     for (int j = 0; j < RUNROLL; ++j)
     {
-        const int u = base + threadIdx.x + j * REFILL_THREADS;
+        const int u = base + threadIdx.x + j * NT;
         w[j] = u < nterms ? W[u] : (TERM_LIST << 12); // a list word is skipped by the term pass
     }
 }
@@ -956,11 +975,13 @@ __device__ __forceinline__ ProdBase base_of(const ProdBase *bse, int slot, const
 // coalesced, and cleared; two windows alternate, so a tile needs one barrier. The
 // words of the next step -- or of the next tile, whose descriptor is read two
 // tiles ahead -- are loaded while a step's gathers are in flight.
-template <bool BATCHED>
-__global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill(
+template <bool BATCHED, int NT>
+__global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
     const TileDesc *__restrict__ tiles, int ntiles, const ProdPtrs *__restrict__ ptrs,
     const ProdSched *__restrict__ scheds, ProdPtrs P1, ProdSched S1, int *__restrict__ err)
 {
+    constexpr int WIN = win_of<NT>();
+    constexpr int RSTEP = RUNROLL * NT;
     extern __shared__ __align__(16) double rsm[];
     TileDesc *dsc = reinterpret_cast<TileDesc *>(rsm + 2 * WIN);
     ProdBase *bse = reinterpret_cast<ProdBase *>(dsc + 4);
@@ -968,14 +989,14 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
     const int G = gridDim.x;
     int t = blockIdx.x;
     if (t >= ntiles) return;
-    for (int i = tid; i < 2 * WIN; i += REFILL_THREADS) rsm[i] = 0.0;
+    for (int i = tid; i < 2 * WIN; i += NT) rsm[i] = 0.0;
     copy_desc<BATCHED>(dsc, bse, tiles + t, ptrs, scheds, P1, S1);
     if (t + G < ntiles) copy_desc<BATCHED>(dsc + 1, bse + 1, tiles + t + G, ptrs, scheds, P1, S1);
     __syncthreads();
     unsigned w[RUNROLL];
     {
         const ProdBase pb = base_of<BATCHED>(bse, 0, P1, S1);
-        load_terms(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
+        load_terms<NT>(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
     }
     // launched as a programmatic dependent of the entry-value kernel: everything
     // above overlaps its tail; V is read only after it has completed (a no-op for
@@ -1008,19 +1029,19 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
             for (int j = 0; j < RUNROLL; ++j)
             {
                 v[j] = term[j] ? (pb.V ? pb.V[es[j].y] : 1.0) : 0.0;
-                x[j] = term[j] ? pb.Ax[es[j].x + base + tid + j * REFILL_THREADS] : 0.0;
+                x[j] = term[j] ? pb.Ax[es[j].x + base + tid + j * NT] : 0.0;
             }
             unsigned wn[RUNROLL];
             if (!last)
-                load_terms(pb.W + D.word_begin, nterms, base + RSTEP, wn);
+                load_terms<NT>(pb.W + D.word_begin, nterms, base + RSTEP, wn);
             else if (has1)
             {
                 const TileDesc &Dn = dsc[(k + 1) & 3];
                 const ProdBase pn = base_of<BATCHED>(bse, (k + 1) & 3, P1, S1);
-                load_terms(pn.W + Dn.word_begin, Dn.nterms, 0, wn);
+                load_terms<NT>(pn.W + Dn.word_begin, Dn.nterms, 0, wn);
             }
             else
-                load_terms(nullptr, 0, 0, wn); // nothing: list words
+                load_terms<NT>(nullptr, 0, 0, wn); // nothing: list words
 #pragma unroll
             for (int j = 0; j < RUNROLL; ++j)
             {
@@ -1041,7 +1062,7 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
         {
             const unsigned *hdr = pb.X + D.x_begin;
             const unsigned *items = hdr + D.nlist + 1;
-            for (int l = tid; l < D.nlist; l += REFILL_THREADS)
+            for (int l = tid; l < D.nlist; l += NT)
             {
                 const unsigned h = hdr[l];
                 const int p = (int)(h & 0xfffu);
@@ -1054,7 +1075,7 @@ __global__ void __launch_bounds__(REFILL_THREADS, SDL_REFILL_MINB) k_tile_refill
             __syncthreads();
         }
         double *C = pb.C + D.out_begin;
-        for (int o = tid; o < nout; o += REFILL_THREADS)
+        for (int o = tid; o < nout; o += NT)
         {
             C[o] = win[o];
             win[o] = 0.0;
@@ -1599,6 +1620,16 @@ __global__ void k_validate_schedule(const TileDesc *__restrict__ tiles, int ntil
     }
 }
 
+// Largest window (outputs) of the plan's tiles.
+__global__ void k_tile_max_out(const TileDesc *__restrict__ tiles, int ntiles, int *__restrict__ out)
+{
+    int m = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles;
+         t += (long long)gridDim.x * blockDim.x)
+        m = max(m, tiles[t].nout);
+    atomicMax(out, m);
+}
+
 // Everything the refill needs once C's structure is known: row classes, the
 // compiled tile schedule and the larger rows' scratch.
 void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
@@ -1607,8 +1638,10 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     const int m_out = P.m_out;
     DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1);
     DevBuf<unsigned char> rcls(m_out);
+    // rows with more terms than tile_max leave the tiles for the larger-row kernels
+    const int tile_max = P.cfg.tile_max_terms > 0 ? std::min(TILE_T, P.cfg.tile_max_terms) : TILE_T;
     SDL_LAUNCH(k_num_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub, P.Cp.get(), d.Lp, d.L_m,
-               m_out, rcls.get(), weight.get());
+               m_out, tile_max, rcls.get(), weight.get());
     bin_items(rcls.get(), m_out, NUM_NBINS, P.num_rows, P.num_count, P.num_offset, s);
     exclusive_scan_i64(weight.get(), wpref.get(), m_out, s);
     DevBuf<int> flag(m_out), tile_of((size_t)m_out + 1);
@@ -1671,6 +1704,12 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
                    P.W.get(), word_total, P.X.get(), x_total, P.ES.get(), nV, (long long)d.A_nnz,
                    (long long)P.nnz, rt.d_error);
         if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: the refill schedule failed its bounds check");
+        DevBuf<int> mo(1);
+        SDL_CUDA(cudaMemsetAsync(mo.get(), 0, sizeof(int), s));
+        SDL_LAUNCH(k_tile_max_out, grid_for(P.ntiles, 256, rt.num_sms * 4), 256, 0, s, P.tiles.get(), P.ntiles,
+                   mo.get());
+        SDL_CUDA(cudaMemcpyAsync(&P.max_tile_out, mo.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaStreamSynchronize(s));
     }
     build_big_lists(d, P, ub, na, s);
     if (P.num_count[NUM_GMEM] && !P.big_lists)
@@ -1961,52 +2000,71 @@ void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStrea
     SDL_LAUNCH(k_rebase_tiles, grid_for(n, 256, runtime().num_sms * 4), 256, 0, s, src, n, prod, dst);
 }
 
+namespace {
+// Resident refill CTAs per SM of one kernel instance (its attributes are set on the
+// first call, which is an eager one).
+template <bool BATCHED, int NT>
+int refill_per_sm()
+{
+    static int per_sm = 0;
+    if (!per_sm)
+    {
+        set_smem(k_tile_refill<BATCHED, NT>, refill_smem_bytes<NT>());
+        int n = 0;
+        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT>, NT,
+                                                               refill_smem_bytes<NT>()));
+        per_sm = std::max(1, n);
+    }
+    return per_sm;
+}
+
+template <bool BATCHED, int NT>
+void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
+                   cudaStream_t s, const ProdPtrs &vals, const ProdSched &sched, int ctas_per_sm)
+{
+    const int per_sm = refill_per_sm<BATCHED, NT>();
+    const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm) : per_sm;
+    const int grid = std::min(ntiles, runtime().num_sms * use);
+    if (BATCHED)
+    {
+        SDL_LAUNCH((k_tile_refill<BATCHED, NT>), grid, NT, refill_smem_bytes<NT>(), s, tiles, ntiles, ptrs, scheds,
+                   vals, sched, runtime().d_error);
+        return;
+    }
+    // programmatic dependent launch: the CTAs start while the entry-value kernel
+    // ahead of it on the stream drains (the kernel waits before reading V)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = refill_smem_bytes<NT>();
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill<BATCHED, NT>, tiles, ntiles, ptrs, scheds, vals, sched,
+                                runtime().d_error));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+} // namespace
+
+bool small_tile_refill(const Product &P)
+{
+    return P.cfg.refill_threads == REFILL_THREADS_SMALL && P.max_tile_out <= win_of<REFILL_THREADS_SMALL>();
+}
+
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
-                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm)
+                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm, bool small)
 {
     if (ntiles <= 0) return;
-    // kernel attributes and resident CTAs per SM, set once (outside any capture)
-    static int per_sm[2] = {0, 0};
-    const int b = ptrs ? 1 : 0;
-    if (!per_sm[b])
-    {
-        if (b)
-        {
-            set_smem(k_tile_refill<true>, refill_smem_bytes());
-            SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[b], k_tile_refill<true>,
-                                                                   REFILL_THREADS, refill_smem_bytes()));
-        }
-        else
-        {
-            set_smem(k_tile_refill<false>, refill_smem_bytes());
-            SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[b], k_tile_refill<false>,
-                                                                   REFILL_THREADS, refill_smem_bytes()));
-        }
-        per_sm[b] = std::max(1, per_sm[b]);
-    }
-    const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm[b]) : per_sm[b];
-    const int grid = std::min(ntiles, runtime().num_sms * use);
-    if (b)
-        SDL_LAUNCH(k_tile_refill<true>, grid, REFILL_THREADS, refill_smem_bytes(), s, tiles, ntiles, ptrs,
-                   scheds, vals, sched, runtime().d_error);
+    if (ptrs)
+        launch_refill<true, REFILL_THREADS>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
+    else if (small)
+        launch_refill<false, REFILL_THREADS_SMALL>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
     else
-    {
-        // programmatic dependent launch: the CTAs start while the entry-value kernel
-        // ahead of it on the stream drains (the kernel waits before reading V)
-        cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = dim3(REFILL_THREADS);
-        cfg.dynamicSmemBytes = refill_smem_bytes();
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill<false>, tiles, ntiles, ptrs, scheds, vals, sched,
-                                    runtime().d_error));
-        g_launches.fetch_add(1, std::memory_order_relaxed);
-    }
+        launch_refill<false, REFILL_THREADS>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
 }
 
 void big_rows_refill(const Product &P, const double *Lx, const double *dvec, const double *Ax,
@@ -2092,7 +2150,8 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
         const ProdSched S = sched_of(P);
         const ProdPtrs vals{Lx, dvec, Ax, Cx};
         entry_values(S, vals, s);
-        tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm);
+        tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm,
+                    small_tile_refill(P));
     }
     if (P.big_lists)
     {
@@ -2135,6 +2194,27 @@ __global__ void k_tune_fill(double *x, long long n, double v)
         x[i] = v;
 }
 } // namespace
+
+void product_replan(Product &P, const TuneConfig &c, cudaStream_t s)
+{
+    if (c.refill_threads != REFILL_THREADS && c.refill_threads != REFILL_THREADS_SMALL)
+        fail(SDL_ERR_INVALID, "refill threads must be 256 or 128");
+    if (c.tile_budget < 0 || c.tile_budget > TILE_T || c.tile_max_terms < 0 || c.tile_max_terms > TILE_T ||
+        c.refill_ctas_per_sm < 0)
+        fail(SDL_ERR_INVALID, "tile budget / largest tile row must lie in [0, TILE_T]");
+    if (P.m_out == 0) return;
+    Runtime &rt = runtime();
+    Product Q;
+    product_symbolic(P.desc, c, Q, s);
+    if (Q.nnz != P.nnz || Q.m_out != P.m_out) fail(SDL_ERR_INTERNAL, "replan: the plan has another structure");
+    SDL_LAUNCH(k_tune_diff, grid_for(P.m_out + 1, 256, rt.num_sms * 8), 256, 0, s, Q.Cp.get(), P.Cp.get(),
+               (long long)P.m_out + 1, rt.d_error);
+    if (P.nnz > 0)
+        SDL_LAUNCH(k_tune_diff, grid_for(P.nnz, 256, rt.num_sms * 8), 256, 0, s, Q.Ci.get(), P.Ci.get(),
+                   (long long)P.nnz, rt.d_error);
+    if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "replan: the plan has another structure");
+    P = std::move(Q);
+}
 
 TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
 {
@@ -2241,6 +2321,28 @@ TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
             Q.cfg = best_cfg;
             best = std::move(Q);
             have_best = true;
+        }
+    }
+    // stage 3: the small-tile refill (128-thread CTAs, tiles and tile rows of at most
+    // TILE_T / 2 terms; larger rows leave the tiles), when its windows fit
+    {
+        Product Q;
+        TuneConfig c = sym_best;
+        c.tile_budget = TILE_T / 2;
+        c.tile_max_terms = TILE_T / 2;
+        c.refill_threads = REFILL_THREADS_SMALL;
+        c.refill_ctas_per_sm = 0;
+        build(c, Q);
+        if (small_tile_refill(Q))
+        {
+            const double us = refill_us(Q);
+            if (us < best_us)
+            {
+                best_us = us;
+                best_cfg = Q.cfg;
+                best = std::move(Q);
+                have_best = true;
+            }
         }
     }
     SDL_CUDA(cudaEventDestroy(e0));

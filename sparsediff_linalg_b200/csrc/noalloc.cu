@@ -83,7 +83,8 @@ extern "C" sdl_status sdl_product_fill_noalloc(const sdl_product *Ph, const doub
             const ProdSched S = sched_of(*P);
             const ProdPtrs vals{Lx, d, Ax, Cx};
             entry_values(S, vals, s);
-            tile_refill(P->tiles.get(), P->ntiles, nullptr, nullptr, s, vals, S, P->cfg.refill_ctas_per_sm);
+            tile_refill(P->tiles.get(), P->ntiles, nullptr, nullptr, s, vals, S, P->cfg.refill_ctas_per_sm,
+                        small_tile_refill(*P));
         }
         big_rows_refill_scratch(*P, Lx, d, Ax, Cx, posmap, slots, s);
     });

@@ -243,6 +243,11 @@ struct TuneConfig
     // resident refill CTAs per SM (0: as many as fit)
     int tile_budget = 0; // 0: TILE_T
     int refill_ctas_per_sm = 0;
+    // rows with more terms leave the tiles for the larger-row kernels (0: TILE_T);
+    // refill CTA threads: 256, or 128 for plans whose tiles have at most TILE_T
+    // outputs (tile budget and tile_max_terms at most TILE_T / 2)
+    int tile_max_terms = 0;
+    int refill_threads = 256;
 };
 // Autotuner results: the chosen configuration and what it measured.
 struct TuneResult
@@ -276,6 +281,7 @@ struct Product
     int num_offset[NUM_NBINS + 1] = {0};
     // Compiled refill schedule of the tile rows.
     int ntiles = 0;
+    int max_tile_out = 0; // largest tile window of the plan
     DevBuf<TileDesc> tiles;
     DevBuf<unsigned> W, X; // term words, list sections
     DevBuf<int2> ES;       // per entry: {A.p[k] - tile term offset, V slot} (L_nnz * blocks)
@@ -295,6 +301,9 @@ struct Product
     // per-row statistics kept for the learned scheduler (optional)
     DevBuf<long long> row_terms; // ub per row
 };
+
+// Re-plans P with configuration c (same structure; the schedule follows c).
+void product_replan(Product &P, const TuneConfig &c, cudaStream_t s);
 
 // Autotuner: re-plans P (built by product_symbolic) for its own pattern. Candidate
 // symbolic configurations are timed on the pattern, then candidate tile budgets and
@@ -336,7 +345,9 @@ void append_entry_chunks(long long nV, int prod, int chunk, std::vector<EntChunk
 // with null tables, from `vals` / `sched`.
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
                  cudaStream_t s, ProdPtrs vals = ProdPtrs{}, ProdSched sched = ProdSched{},
-                 int ctas_per_sm = 0);
+                 int ctas_per_sm = 0, bool small = false);
+// Whether a single product's refill runs the 128-thread small-tile kernel.
+bool small_tile_refill(const Product &P);
 // Copies `n` descriptors, setting `prod`.
 void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s);
 // The larger rows of one product from their output-major term lists (needs

@@ -82,6 +82,17 @@ class Product:
         self._init_from_handle(self.handle)
         return self.tuning()
 
+    def replan(self, tile_budget=0, tile_max_terms=0, refill_threads=256, refill_ctas_per_sm=0, stream=None):
+        """Re-plan with a given refill configuration (sdl_product_replan)."""
+        check(lib().sdl_product_replan(self.handle, tile_budget, tile_max_terms, refill_threads,
+                                       refill_ctas_per_sm, _stream(stream)))
+        self._init_from_handle(self.handle)
+
+    def refill_shape(self):
+        th, tm = C.c_int(), C.c_int()
+        check(lib().sdl_product_refill_shape(self.handle, C.byref(th), C.byref(tm)))
+        return th.value, tm.value
+
     def tuning(self):
         """The plan's configuration and what the autotuner measured."""
         i = [C.c_int() for _ in range(5)]
@@ -89,8 +100,11 @@ class Product:
         check(lib().sdl_product_tuning(self.handle, C.byref(i[0]), C.byref(i[1]), C.byref(i[2]),
                                        C.byref(i[3]), C.byref(f[0]), C.byref(f[1]), C.byref(i[4]),
                                        C.byref(f[2])))
+        th, tm = C.c_int(), C.c_int()
+        check(lib().sdl_product_refill_shape(self.handle, C.byref(th), C.byref(tm)))
         return {"warp_max_terms": i[0].value, "rows_per_cta_warp": i[1].value, "tile_budget": i[2].value,
-                "refill_ctas_per_sm": i[3].value, "refill_us": round(f[0].value, 2),
+                "refill_ctas_per_sm": i[3].value, "refill_threads": th.value, "tile_max_terms": tm.value,
+                "refill_us": round(f[0].value, 2),
                 "default_refill_us": round(f[1].value, 2), "candidates": i[4].value,
                 "tune_ms": round(f[2].value, 1)}
 
