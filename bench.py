@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-conversions", action="store_true")
     ap.add_argument("--no-dense", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--small-tiles", action="store_true",
+                    help="plan the headline product for the small-tile refill (128-thread CTAs, "
+                         "512-term tiles) instead of autotuning it (reproducible profiles)")
     ap.add_argument("--split-rows", action="store_true",
                     help="N > 1: one headline product split by output rows across the ranks "
                          "(strong scaling) instead of one product per rank (weak scaling)")
@@ -287,7 +290,11 @@ def run_b200(args, world, rank, local):
     # the product's plan picked by the autotuner on this pattern (timed refills
     # below run with it); it reports the as-given plan's refill time beside its own
     tune = None
-    if not args.no_autotune:
+    if args.small_tiles:
+        P.replan(tile_budget=512, tile_max_terms=512, refill_threads=128, stream=stream)
+        tune = P.tuning()
+        torch.cuda.synchronize()
+    elif not args.no_autotune:
         tune = P.autotune(reps=5, stream=stream)
         torch.cuda.synchronize()
     Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev)
