@@ -453,7 +453,8 @@ def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world):
     return {"value": round(world * B_alg / t / 1e9, 3), "unit": "GB/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": round(t * 1e3, 4),
-            "api": "BTDA_matrices_fill_values (host buffers, pageable)"}
+            "api": "BTDA_matrices_fill_values (host value arrays from the library's constructors, "
+                   "page-locked in place on their first transfer; d a caller-owned host array)"}
 
 
 def run_batched(args, dev, refills=20):
