@@ -145,18 +145,19 @@ def _csc_worker(rank, world, port, csr, n, out):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_sharded_csr_to_csc_gloo(world):
+@pytest.mark.parametrize("world,m,n", [(2, 70, 55), (3, 70, 55), (4, 3, 5)])
+def test_sharded_csr_to_csc_gloo(world, m, n):
     """Rows spread over `world` gloo ranks -> columns spread over them, with one
     all-to-all: reassembled, the CSC is the stable transpose (rows ascending in every
     column), and a value refill moves the new values the same way."""
     import multiprocessing as mp
     import numpy as np
     rng = np.random.default_rng(40 + world)
-    m, n = 70, 55
-    dense = (rng.random((m, n)) < 0.12) * rng.standard_normal((m, n))
-    dense[5] = 0.0          # an empty row
-    dense[:, 7] = 0.0       # an empty column
+    dense = (rng.random((m, n)) < (0.12 if m > 10 else 0.5)) * rng.standard_normal((m, n))
+    if m > 10:
+        dense[5] = 0.0      # an empty row
+        dense[:, 7] = 0.0   # an empty column
+    # (4 ranks over 3 rows and 5 columns: one rank holds no rows, some hold no columns)
     p = np.concatenate([[0], np.cumsum((dense != 0).sum(1))]).astype(np.int32)
     i = np.nonzero(dense)[1].astype(np.int32)
     x = dense[dense != 0].astype(np.float64)
@@ -174,9 +175,11 @@ def test_sharded_csr_to_csc_gloo(world):
     assert all(res[r][2] == res[r + 1][1] for r in range(world - 1))
     Tp = [np.zeros(1, np.int64)]
     Ti, Tx, Tx2 = [], [], []
+    off = 0
     for _, c0, c1, tp, ti, tx, tx2 in res:
-        assert len(tp) == c1 - c0 + 1
-        Tp.append(tp[1:].astype(np.int64) + Tp[-1][-1])
+        assert len(tp) == c1 - c0 + 1 and tp[0] == 0 and tp[-1] == len(ti)
+        Tp.append(tp[1:].astype(np.int64) + off)
+        off += len(ti)
         Ti.append(ti)
         Tx.append(tx)
         Tx2.append(tx2)
