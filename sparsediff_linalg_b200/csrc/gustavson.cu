@@ -1074,12 +1074,30 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
             }
             __syncthreads();
         }
+        // write-back (and clear) two outputs per 16-byte access where the tile's
+        // first output is 16-byte aligned in C
         double *C = pb.C + D.out_begin;
-        for (int o = tid; o < nout; o += NT)
+        if ((reinterpret_cast<uintptr_t>(C) & 15) == 0)
         {
-            C[o] = win[o];
-            win[o] = 0.0;
+            double2 *C2 = reinterpret_cast<double2 *>(C);
+            double2 *w2 = reinterpret_cast<double2 *>(win);
+            for (int o = tid; o < (nout >> 1); o += NT)
+            {
+                C2[o] = w2[o];
+                w2[o] = make_double2(0.0, 0.0);
+            }
+            if ((nout & 1) && tid == 0)
+            {
+                C[nout - 1] = win[nout - 1];
+                win[nout - 1] = 0.0;
+            }
         }
+        else
+            for (int o = tid; o < nout; o += NT)
+            {
+                C[o] = win[o];
+                win[o] = 0.0;
+            }
         if (!has1) break;
         t += G; // the words of the next tile were loaded by the last step
     }
