@@ -55,20 +55,50 @@ __global__ void k_coal_starts(const unsigned *__restrict__ keys, const uint2 *__
     if (blockIdx.x == 0 && threadIdx.x == 0) ostart[nout] = n;
 }
 
+// A thread per output, four outputs (one grid stride apart) at a time: the first
+// triplet of each is fetched before any is summed, so four dependent chains (start
+// -> position -> value) are in flight together; further triplets of an output (the
+// duplicates) follow in ascending order. Each output is summed from +0.0 in
+// ascending triplet order.
+constexpr int COAL_ILP = 4;
 __global__ void k_coal_fill(const int *__restrict__ ostart, const int *__restrict__ perm, const double *__restrict__ x,
                             const double *__restrict__ f, int nout, double *__restrict__ C)
 {
-    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < nout;
-         o += (long long)gridDim.x * blockDim.x)
+    const long long step = (long long)gridDim.x * blockDim.x;
+    for (long long base = blockIdx.x * (long long)blockDim.x + threadIdx.x; base < nout; base += step * COAL_ILP)
     {
-        double acc = 0.0;
-        const int q1 = ostart[o + 1];
-        for (int q = ostart[o]; q < q1; ++q)
+        int q0[COAL_ILP], q1[COAL_ILP];
+#pragma unroll
+        for (int j = 0; j < COAL_ILP; ++j)
         {
-            const int t = perm[q];
-            acc = __dadd_rn(acc, f ? __dmul_rn(f[t], x[t]) : x[t]);
+            const long long o = base + j * step;
+            q0[j] = q1[j] = 0;
+            if (o < nout)
+            {
+                q0[j] = ostart[o];
+                q1[j] = ostart[o + 1];
+            }
         }
-        C[o] = acc;
+        int t[COAL_ILP];
+#pragma unroll
+        for (int j = 0; j < COAL_ILP; ++j) t[j] = q0[j] < q1[j] ? perm[q0[j]] : -1;
+        double v[COAL_ILP];
+#pragma unroll
+        for (int j = 0; j < COAL_ILP; ++j)
+            v[j] = t[j] < 0 ? 0.0 : (f ? __dmul_rn(f[t[j]], x[t[j]]) : x[t[j]]);
+#pragma unroll
+        for (int j = 0; j < COAL_ILP; ++j)
+        {
+            const long long o = base + j * step;
+            if (o >= nout) continue;
+            double acc = __dadd_rn(0.0, v[j]);
+            for (int q = q0[j] + 1; q < q1[j]; ++q)
+            {
+                const int tq = perm[q];
+                acc = __dadd_rn(acc, f ? __dmul_rn(f[tq], x[tq]) : x[tq]);
+            }
+            C[o] = acc;
+        }
     }
 }
 
