@@ -402,6 +402,14 @@ def run_b200(args, world, rank, local):
         "spgemm_2000": {"symbolic_ms": round(sp_sym_ms, 3), "numeric_us": round(sp_num_us, 2),
                         "nnz_C": SP.nnz},
     }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the same product by the upstream library on one host core (alloc, then fills)
+        try:
+            r = reference_spgemm_times(SA, SB, 50)
+            line["spgemm_2000"]["upstream_cpu"] = {"alloc_ms": round(r[0] * 1e3, 3),
+                                                   "fill_us": round(r[1] * 1e6, 2), "nnz_C": int(r[2])}
+        except Exception as e:  # the timing library is built with the oracle
+            line["spgemm_2000"]["upstream_cpu"] = {"unavailable": str(e)[:200]}
     if e2e is not None:
         line["e2e"] = e2e
     if batched is not None:
