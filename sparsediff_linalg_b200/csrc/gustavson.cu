@@ -2159,39 +2159,50 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
     }
 }
 
+// Whether a single product's entry values are L.x itself: no d, one block, and the
+// values kept in L's value order (L_map a permutation) or no L_map at all. The refill
+// then reads L.x where it would read V, and the entry-value launch is skipped.
+bool entry_values_are_lx(const Product &P, const double *Lx, const double *dvec)
+{
+    return Lx && !dvec && P.desc.blocks == 1 && (P.kv.get() || !P.desc.L_map);
+}
+
 void product_numeric(const Product &P, const double *Lx, const double *dvec, const double *Ax,
                      double *Cx, cudaStream_t s)
 {
     if (P.nnz == 0) return;
+    ProdSched S = sched_of(P);
+    const ProdPtrs vals{Lx, dvec, Ax, Cx};
+    const bool direct = entry_values_are_lx(P, Lx, dvec);
+    if (direct) S.V = const_cast<double *>(Lx); // read only
     if (P.num_count[NUM_TILE])
     {
-        const ProdSched S = sched_of(P);
-        const ProdPtrs vals{Lx, dvec, Ax, Cx};
-        entry_values(S, vals, s);
+        if (!direct) entry_values(S, vals, s);
         tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm,
                     small_tile_refill(P));
     }
     if (P.big_lists)
     {
-        if (!P.num_count[NUM_TILE]) entry_values(sched_of(P), ProdPtrs{Lx, dvec, Ax, Cx}, s);
-        big_lists_refill(P, nullptr, s, ProdPtrs{Lx, dvec, Ax, Cx});
+        if (!P.num_count[NUM_TILE] && !direct) entry_values(S, vals, s);
+        big_lists_refill(P, nullptr, s, vals, S.V);
     }
     else
         big_rows_refill(P, Lx, dvec, Ax, Cx, s);
 }
 
-void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs vals)
+void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs vals, const double *V)
 {
     if (!P.big_lists || P.big_outputs == 0) return;
     const int grid = (P.big_outputs + 255) / 256;
     const long long nV = (long long)P.desc.L_nnz * P.desc.blocks;
+    if (!V) V = P.V.get();
     if (ptrs)
         SDL_LAUNCH(k_big_refill<true>, grid, 256, 0, s, P.brows.get(), P.nbig, P.bout_off.get(), P.big_outputs,
-                   P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, P.V.get(), nV, (long long)P.desc.A_nnz,
+                   P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, V, nV, (long long)P.desc.A_nnz,
                    runtime().d_error);
     else
         SDL_LAUNCH(k_big_refill<false>, grid, 256, 0, s, P.brows.get(), P.nbig, P.bout_off.get(), P.big_outputs,
-                   P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, P.V.get(), nV, (long long)P.desc.A_nnz,
+                   P.bostart.get(), P.bpairs.get(), P.Cp.get(), ptrs, vals, V, nV, (long long)P.desc.A_nnz,
                    runtime().d_error);
 }
 

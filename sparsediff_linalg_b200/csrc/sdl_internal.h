@@ -352,7 +352,9 @@ bool small_tile_refill(const Product &P);
 void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s);
 // The larger rows of one product from their output-major term lists (needs
 // P.big_lists), values as in tile_refill.
-void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs vals = ProdPtrs{});
+// V: the entry values to read (null: the product's own scratch).
+void big_lists_refill(const Product &P, const ProdPtrs *ptrs, cudaStream_t s, ProdPtrs vals = ProdPtrs{},
+                      const double *V = nullptr);
 // The larger rows of one product (CTA kernels), for the given values; with `vals`
 // (a device ProdPtrs) the kernels read the value pointers from there instead.
 void big_rows_refill(const Product &P, const double *Lx, const double *d, const double *Ax,
