@@ -80,9 +80,12 @@ extern "C" sdl_status sdl_product_fill_noalloc(const sdl_product *Ph, const doub
             1, std::min<long long>(runtime().num_sms, STATIC_POSMAP_INTS / std::max(1, P->n)));
         if (P->num_count[NUM_TILE])
         {
-            const ProdSched S = sched_of(*P);
+            ProdSched S = sched_of(*P);
             const ProdPtrs vals{Lx, d, Ax, Cx};
-            entry_values(S, vals, s);
+            if (entry_values_are_lx(*P, Lx, d))
+                S.V = const_cast<double *>(Lx); // read only
+            else
+                entry_values(S, vals, s);
             tile_refill(P->tiles.get(), P->ntiles, nullptr, nullptr, s, vals, S, P->cfg.refill_ctas_per_sm,
                         small_tile_refill(*P));
         }

@@ -348,6 +348,9 @@ void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const 
                  int ctas_per_sm = 0, bool small = false);
 // Whether a single product's refill runs the 128-thread small-tile kernel.
 bool small_tile_refill(const Product &P);
+// Whether a product's entry values are L.x itself (no d, one block, values in L's
+// value order or no L_map): the refill then reads L.x and skips the entry values.
+bool entry_values_are_lx(const Product &P, const double *Lx, const double *dvec);
 // Copies `n` descriptors, setting `prod`.
 void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStream_t s);
 // The larger rows of one product from their output-major term lists (needs
