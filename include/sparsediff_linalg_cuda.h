@@ -9,7 +9,9 @@
  *     unless a comment says otherwise);
  *   - the batched refill engine and the learned row scheduler.
  * Every function is extern "C" with plain pointers and sizes. Streams are passed
- * as void* (a cudaStream_t); NULL means the library's own stream. */
+ * as void* (a cudaStream_t); NULL means the library's own stream. The library
+ * works on one device per process: the device current when it is first used
+ * (one process per GPU, as torch.distributed and torchrun arrange it). */
 #ifndef SPARSEDIFF_LINALG_CUDA_H
 #define SPARSEDIFF_LINALG_CUDA_H
 
