@@ -1,11 +1,11 @@
-// Value refill of a COO coalescing plan (and of the matrix sums built on it), as a
-// gather in output order: at plan time every triplet's output position is found
-// (binary search of its column in its output row) and the triplets are sorted by
-// it with the stable radix sort, so each output's triplets sit together in
-// ascending triplet order; a refill is then one thread per output summing its
-// triplets' values (times their factors, when given) from +0.0 in that order --
-// upstream's memset + accumulator order, bit for bit -- with the triplet-to-output
-// permutation read in order and the values gathered once each.
+// COO coalescing (and the matrix sums built on it): the plan sorts the triplets
+// once, stably, by column and then by row, so they sit in (row, column, triplet)
+// order; the first triplet of each distinct (row, column) opens an output, which
+// gives the coalesced CSR structure and, in the same order, the triplet-to-output
+// permutation. A value refill is then a gather in output order: one thread per
+// output summing its triplets' values (times their factors, when given) from +0.0
+// in ascending triplet order -- upstream's memset + accumulator order, bit for bit
+// -- with the permutation read in order and the values gathered once each.
 #include <algorithm>
 
 #include "sdl_device.cuh"
@@ -13,7 +13,6 @@
 
 namespace sdl {
 
-void sum_positions(const int *rows, const int *cols, int n, const int *Cp, const int *Ci, int *map, cudaStream_t s);
 void radix_sort_pairs(unsigned *keys, uint2 *vals, unsigned *keys_tmp, uint2 *vals_tmp, int n, int key_bits,
                       cudaStream_t s);
 
@@ -23,36 +22,6 @@ int grid_coal(long long n, int per_block)
 {
     long long g = (n + per_block - 1) / per_block;
     return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 32));
-}
-
-__global__ void k_coal_keys(const int *__restrict__ map, int n, unsigned *__restrict__ keys, uint2 *__restrict__ vals)
-{
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
-    {
-        keys[t] = (unsigned)map[t];
-        vals[t] = make_uint2((unsigned)t, 0u);
-    }
-}
-
-// perm[q] = triplet of sorted slot q; ostart[o] = first slot of output o.
-__global__ void k_coal_starts(const unsigned *__restrict__ keys, const uint2 *__restrict__ vals, int n, int nout,
-                              int *__restrict__ perm, int *__restrict__ ostart, int *__restrict__ err)
-{
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    {
-        perm[q] = (int)vals[q].x;
-        const unsigned k = keys[q];
-        if (k >= (unsigned)nout)
-        {
-            atomicOr(err, 1);
-            continue;
-        }
-        if (q == 0 || keys[q - 1] != k) ostart[k] = (int)q;
-        if (q == 0 && k != 0) atomicOr(err, 1); // output 0 has no triplet
-        if (q > 0 && keys[q - 1] != k && k != keys[q - 1] + 1) atomicOr(err, 1); // an output without triplets
-        if (q == n - 1 && k != (unsigned)nout - 1) atomicOr(err, 1);             // the last outputs without triplets
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) ostart[nout] = n;
 }
 
 // A thread per output, four outputs (one grid stride apart) at a time: the first
@@ -102,31 +71,100 @@ __global__ void k_coal_fill(const int *__restrict__ ostart, const int *__restric
     }
 }
 
+// Structure and refill plan of a coalescing in one sort: the triplets are stably
+// radix-sorted by column, then by row, so they end up in (row, column, triplet)
+// order; the first triplet of every distinct (row, column) opens an output, in
+// CSR order; k_coal_fill refills from it.
+__global__ void k_cs_init(const int *__restrict__ rows, const int *__restrict__ cols, int n,
+                          unsigned *__restrict__ keys, uint2 *__restrict__ vals)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    {
+        keys[t] = (unsigned)cols[t];
+        vals[t] = make_uint2((unsigned)t, (unsigned)rows[t]);
+    }
+}
+
+// Column-sorted {column | triplet, row} -> row keys with {triplet, column}.
+__global__ void k_cs_rekey(const unsigned *__restrict__ keys1, const uint2 *__restrict__ vals1, int n,
+                           unsigned *__restrict__ keys2, uint2 *__restrict__ vals2)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    {
+        const uint2 v = vals1[q];
+        keys2[q] = v.y;
+        vals2[q] = make_uint2(v.x, keys1[q]);
+    }
+}
+
+__global__ void k_cs_flags(const unsigned *__restrict__ row, const uint2 *__restrict__ vals, int n, int *__restrict__ flag)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        flag[q] = (q == 0 || row[q] != row[q - 1] || vals[q].y != vals[q - 1].y) ? 1 : 0;
+}
+
+__global__ void k_cs_emit(const unsigned *__restrict__ row, const uint2 *__restrict__ vals, const int *__restrict__ flag,
+                          const int *__restrict__ oid, int n, int *__restrict__ perm, int *__restrict__ ostart,
+                          int *__restrict__ Ci, int *__restrict__ rowcnt)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    {
+        perm[q] = (int)vals[q].x;
+        if (flag[q])
+        {
+            const int o = oid[q];
+            ostart[o] = (int)q;
+            Ci[o] = (int)vals[q].y;
+            atomicAdd(&rowcnt[row[q]], 1);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) ostart[oid[n]] = n;
+}
+
 } // namespace
 
-void coalesce_order_build(const int *rows, const int *cols, int n, const int *Cp, const int *Ci, int nout,
+int coalesce_sorted_build(const int *rows, const int *cols, int n, int m, int ncols, DevBuf<int> &Cp, DevBuf<int> &Ci,
                           DevBuf<int> &perm, DevBuf<int> &ostart, cudaStream_t s)
 {
+    Cp.reset((size_t)m + 1);
     perm.reset((size_t)std::max(1, n));
-    ostart.reset((size_t)nout + 1);
     if (n == 0)
     {
-        SDL_CUDA(cudaMemsetAsync(ostart.get(), 0, ((size_t)nout + 1) * sizeof(int), s));
-        return;
+        SDL_CUDA(cudaMemsetAsync(Cp.get(), 0, Cp.bytes(), s));
+        Ci.reset(1);
+        ostart.reset(1);
+        SDL_CUDA(cudaMemsetAsync(ostart.get(), 0, sizeof(int), s));
+        SDL_CUDA(cudaStreamSynchronize(s));
+        return 0;
     }
-    DevBuf<int> map((size_t)n);
-    sum_positions(rows, cols, n, Cp, Ci, map.get(), s);
-    if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "coalesce plan: a triplet's column is missing from its row");
-    DevBuf<unsigned> keys((size_t)n), keys_tmp((size_t)n);
-    DevBuf<uint2> vals((size_t)n), vals_tmp((size_t)n);
-    SDL_LAUNCH(k_coal_keys, grid_coal(n, 256), 256, 0, s, map.get(), n, keys.get(), vals.get());
-    int bits = 1;
-    while (bits < 32 && ((long long)1 << bits) < (long long)nout) ++bits;
-    radix_sort_pairs(keys.get(), vals.get(), keys_tmp.get(), vals_tmp.get(), n, bits, s);
-    SDL_LAUNCH(k_coal_starts, grid_coal(n, 256), 256, 0, s, keys.get(), vals.get(), n, nout, perm.get(), ostart.get(),
-               runtime().d_error);
-    if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "coalesce plan: inconsistent output order");
+    auto bits_of = [](int v) {
+        int b = 1;
+        while (b < 31 && ((long long)1 << b) < (long long)v) ++b;
+        return b;
+    };
+    DevBuf<unsigned> ka((size_t)n), kb((size_t)n);
+    DevBuf<uint2> va((size_t)n), vb((size_t)n);
+    const int g = grid_coal(n, 256);
+    SDL_LAUNCH(k_cs_init, g, 256, 0, s, rows, cols, n, ka.get(), va.get());
+    radix_sort_pairs(ka.get(), va.get(), kb.get(), vb.get(), n, bits_of(ncols), s);
+    SDL_LAUNCH(k_cs_rekey, g, 256, 0, s, ka.get(), va.get(), n, kb.get(), vb.get());
+    radix_sort_pairs(kb.get(), vb.get(), ka.get(), va.get(), n, bits_of(m), s);
+    DevBuf<int> flag((size_t)n), oid((size_t)n + 1);
+    SDL_LAUNCH(k_cs_flags, g, 256, 0, s, kb.get(), vb.get(), n, flag.get());
+    const int nout = exclusive_scan_i32_checked(flag.get(), oid.get(), n, s);
+    Ci.reset((size_t)std::max(1, nout));
+    ostart.reset((size_t)nout + 1);
+    DevBuf<int> rowcnt((size_t)m + 1);
+    SDL_CUDA(cudaMemsetAsync(rowcnt.get(), 0, rowcnt.bytes(), s));
+    SDL_LAUNCH(k_cs_emit, g, 256, 0, s, kb.get(), vb.get(), flag.get(), oid.get(), n, perm.get(), ostart.get(),
+               Ci.get(), rowcnt.get());
+    const int total = exclusive_scan_i32_checked(rowcnt.get(), Cp.get(), m, s);
+    if (total != nout) fail(SDL_ERR_INTERNAL, "coalesce plan: row counts disagree with the outputs");
+    SDL_CUDA(cudaStreamSynchronize(s));
+    return nout;
 }
+
+
 
 void coalesce_order_fill(const int *ostart, const int *perm, const double *x, const double *f, int nout, double *C,
                          cudaStream_t s)

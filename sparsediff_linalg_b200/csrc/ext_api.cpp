@@ -25,15 +25,13 @@ struct sdl_transpose
 // (coalesce.cu), which sums in the same order.
 struct sdl_coalesce
 {
-    int m = 0, n = 0, nnz_in = 0;
-    TransposePlan G;
-    DevBuf<int> Ap, Ai;
-    Product P;
+    int m = 0, n = 0, nnz_in = 0, nout = 0;
+    DevBuf<int> Cp, Ci;       // the coalesced CSR structure
     DevBuf<int> perm, ostart; // triplets in output order; first slot of every output
 };
 
 namespace sdl {
-void coalesce_order_build(const int *rows, const int *cols, int n, const int *Cp, const int *Ci, int nout,
+int coalesce_sorted_build(const int *rows, const int *cols, int n, int m, int ncols, DevBuf<int> &Cp, DevBuf<int> &Ci,
                           DevBuf<int> &perm, DevBuf<int> &ostart, cudaStream_t s);
 void coalesce_order_fill(const int *ostart, const int *perm, const double *x, const double *f, int nout, double *C,
                          cudaStream_t s);
@@ -240,26 +238,7 @@ extern "C" sdl_status sdl_coalesce_create(const int *rows, const int *cols, int 
         c->m = m;
         c->n = n;
         c->nnz_in = nnz_in;
-        transpose_build(nullptr, rows, nnz_in, m, nnz_in, c->G, s);
-        c->Ap.reset((size_t)nnz_in + 1);
-        fill_iota(c->Ap.get(), nnz_in + 1, s);
-        c->Ai.reset(std::max(1, nnz_in));
-        if (nnz_in)
-            SDL_CUDA(cudaMemcpyAsync(c->Ai.get(), cols, (size_t)nnz_in * sizeof(int),
-                                     cudaMemcpyDeviceToDevice, s));
-        ProductDesc d;
-        d.Lp = c->G.Tp.get();
-        d.Li = c->G.Ti.get();
-        d.L_m = m;
-        d.L_nnz = nnz_in;
-        d.blocks = 1;
-        d.Ap = c->Ap.get();
-        d.Ai = c->Ai.get();
-        d.A_m = nnz_in;
-        d.A_n = n;
-        d.A_nnz = nnz_in;
-        product_symbolic(d, TuneConfig{}, c->P, s);
-        coalesce_order_build(rows, cols, nnz_in, c->P.Cp.get(), c->P.Ci.get(), c->P.nnz, c->perm, c->ostart, s);
+        c->nout = coalesce_sorted_build(rows, cols, nnz_in, m, n, c->Cp, c->Ci, c->perm, c->ostart, s);
         *out = c.release();
     });
 }
@@ -269,9 +248,9 @@ extern "C" sdl_status sdl_coalesce_info(const sdl_coalesce *C, int *nnz_out, con
 {
     return guard_status("sdl_coalesce_info", [&]() {
         if (!C) fail(SDL_ERR_INVALID, "NULL plan");
-        if (nnz_out) *nnz_out = C->P.nnz;
-        if (Cp) *Cp = C->P.Cp.get();
-        if (Ci) *Ci = C->P.Ci.get();
+        if (nnz_out) *nnz_out = C->nout;
+        if (Cp) *Cp = C->Cp.get();
+        if (Ci) *Ci = C->Ci.get();
     });
 }
 
@@ -280,7 +259,7 @@ extern "C" sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, 
 {
     return guard_status("sdl_coalesce_fill", [&]() {
         if (!C) fail(SDL_ERR_INVALID, "NULL plan");
-        coalesce_order_fill(C->ostart.get(), C->perm.get(), x, nullptr, C->P.nnz, Cx, pick_stream(stream));
+        coalesce_order_fill(C->ostart.get(), C->perm.get(), x, nullptr, C->nout, Cx, pick_stream(stream));
     });
 }
 
@@ -291,6 +270,6 @@ namespace sdl {
 // over its duplicates in ascending t, from +0.0 (d null: x[t]).
 void coalesce_fill_scaled(const sdl_coalesce *C, const double *x, const double *d, double *Cx, cudaStream_t s)
 {
-    coalesce_order_fill(C->ostart.get(), C->perm.get(), x, d, C->P.nnz, Cx, s);
+    coalesce_order_fill(C->ostart.get(), C->perm.get(), x, d, C->nout, Cx, s);
 }
 } // namespace sdl
