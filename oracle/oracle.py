@@ -229,29 +229,47 @@ def blocks_csr(blocks, Sp, Si, Sx, S_n):
     (src/permuted_dense/permuted_dense_linalg.c:313-430): output columns are the
     union of the patterns of S's rows col_perm_k, ascending; every output is summed
     over the compact CSC of S[col_perm_k, :] in its order (row r of the block
-    ascending), from +0.0, one rounding per product and per sum. Returns
+    ascending, then S's entry order), from +0.0, one rounding per product and per
+    sum. The compact CSC is built once per distinct col_perm; the sums run one
+    term depth at a time over all columns (a column has at most one term at each
+    depth, so every cell still sees its terms in order). Returns
     [(col_perm_C, C_k)] per block (numpy, float64). Test infrastructure only."""
+    Sp = np.asarray(Sp, np.int64)
+    Si = np.asarray(Si, np.int64)
+    Sx = np.asarray(Sx, np.float64)
+    plans = {}
+
+    def plan(cperm):
+        key = np.asarray(cperm, np.int64).tobytes()
+        if key in plans:
+            return plans[key]
+        cp = np.asarray(cperm, np.int64)
+        lens = Sp[cp + 1] - Sp[cp] if len(cp) else np.zeros(0, np.int64)
+        tot = int(lens.sum())
+        r = np.repeat(np.arange(len(cp), dtype=np.int64), lens)
+        first = np.repeat(Sp[cp] - np.concatenate([[0], np.cumsum(lens)[:-1]]), lens) if tot else r
+        q = first + np.arange(tot, dtype=np.int64)        # S entries, rows r ascending
+        c = Si[q]
+        o = np.argsort(c, kind="stable")                  # compact CSC order
+        r, q, c = r[o], q[o], c[o]
+        cols, start = np.unique(c, return_index=True)
+        loc = np.searchsorted(cols, c)
+        depth = np.arange(tot, dtype=np.int64) - start[loc] if tot else np.zeros(0, np.int64)
+        levels = []
+        for t in range(int(depth.max()) + 1 if tot else 0):
+            s = depth == t
+            levels.append((loc[s], r[s], q[s]))
+        plans[key] = (cols.astype(np.int32), levels)
+        return plans[key]
+
     out = []
     for X, cperm in blocks:
         X = np.asarray(X, np.float64)
-        ents = []  # (column of S, local row r, value) in upstream's order
-        for r, row in enumerate(cperm):
-            for q in range(Sp[row], Sp[row + 1]):
-                ents.append((int(Si[q]), r, float(Sx[q])))
-        cols = sorted({c for c, _, _ in ents})
-        loc = {c: k for k, c in enumerate(cols)}
-        per = [[] for _ in cols]
-        for c, r, v in ents:  # r ascending, then q: upstream's compact order
-            per[loc[c]].append((r, v))
+        cols, levels = plan(cperm)
         C = np.zeros((X.shape[0], len(cols)))
-        if cols:
-            depth = max(len(e) for e in per)
-            for t in range(depth):  # one term of every column at a time: sequential sums
-                idx = [k for k in range(len(cols)) if len(per[k]) > t]
-                rr = np.array([per[k][t][0] for k in idx])
-                vv = np.array([per[k][t][1] for k in idx])
-                C[:, idx] = C[:, idx] + X[:, rr] * vv[None, :]
-        out.append((np.array(cols, np.int32), C))
+        for loc, r, q in levels:
+            C[:, loc] = C[:, loc] + X[:, r] * Sx[q][None, :]
+        out.append((cols, C))
     return out
 
 

@@ -206,3 +206,118 @@ def test_port_kron_blocks_vs_explicit(orc):
             rows_p.append(len(rows_i))
     Ep, Ei, Ex = orc.gustavson(rows_p, rows_i, rows_x, p_blocks * mL, 1, d, A[0], A[1], A[2], A[3], A[4])
     assert np.array_equal(Cp, Ep) and np.array_equal(Ci, Ei) and np.array_equal(Cx, Ex)
+
+
+# ---------------------------------------------------------------- parallel drivers
+def test_parallel_spgemm_and_btda_equal_one_call(orc):
+    """Row-range pieces on a thread pool concatenate to the one-call result, bit
+    for bit (incl. empty rows and rows of very different weight)."""
+    from oracle import parallel
+    rng = np.random.default_rng(77)
+    lens = rng.integers(0, 30, 400)
+    lens[::50] = 0
+    lens[7] = 300
+    A = wl.variable_rowlen_csr(400, 500, lens, rng)
+    B = wl.small_random_csr(500, 300, 0.02, rng)
+    want = orc.spgemm(A, B)
+    got = parallel.spgemm(A, B, threads=3)
+    assert parallel.compare_csr(got, want)["bit_identical"]
+    A2 = wl.small_random_csr(500, 200, 0.03, rng)
+    d = rng.uniform(0.1, 10, 500)
+    want = orc.btda(A2, B, d)
+    got = parallel.btda(A2, B, d, threads=4)
+    r = parallel.compare_csr(got, want)
+    assert r["structure_equal"] and r["bit_identical"] and r["max_rel_err"] == 0.0
+
+
+def test_parallel_coalesce_equals_one_call(orc):
+    from oracle import parallel
+    rng = np.random.default_rng(78)
+    m, n, N = 300, 200, 20000
+    rows = rng.integers(0, m, N).astype(np.int32)
+    rows[rows == 5] = 6                                     # an empty output row
+    cols = rng.integers(0, n, N).astype(np.int32)
+    x = rng.standard_normal(N)
+    x[::11] = -0.0
+    want = orc.coalesce(rows, cols, x, m, n)
+    got = parallel.coalesce(rows, cols, x, m, n, threads=5)
+    assert parallel.compare_csr(got, want)["bit_identical"]
+
+
+def test_compare_csr_reports_errors(orc):
+    from oracle import parallel
+    p = np.array([0, 2, 3], np.int32)
+    i = np.array([0, 3, 1], np.int32)
+    x = np.array([1.0, -2.0, 0.5])
+    r = parallel.compare_csr((p, i, x), (p, i, x.copy()))
+    assert r["bit_identical"] and r["max_rel_err"] == 0.0
+    y = x.copy()
+    y[1] *= 1 + 2e-13
+    r = parallel.compare_csr((p, i, y), (p, i, x))
+    assert r["structure_equal"] and not r["bit_identical"] and 1e-13 < r["max_rel_err"] < 1e-12
+    assert r["within_tol"]
+    r = parallel.compare_csr((p, np.array([0, 2, 1], np.int32), x), (p, i, x))
+    assert not r["structure_equal"]
+
+
+def _blocks_csr_by_loops(blocks, Sp, Si, Sx):
+    """The definition, term by term: per block, output columns the union of S's rows
+    in col_perm (ascending); each cell summed from +0.0 over rows r ascending."""
+    out = []
+    for X, cperm in blocks:
+        ents = [(int(Si[q]), r, float(Sx[q])) for r, row in enumerate(cperm)
+                for q in range(Sp[row], Sp[row + 1])]
+        cols = sorted({c for c, _, _ in ents})
+        loc = {c: k for k, c in enumerate(cols)}
+        C = np.zeros((X.shape[0], len(cols)))
+        for i in range(X.shape[0]):
+            for c, r, v in ents:
+                C[i, loc[c]] = C[i, loc[c]] + X[i, r] * v
+        out.append((np.array(cols, np.int32), C))
+    return out
+
+
+def test_blocks_csr_oracle_matches_definition(orc):
+    rng = np.random.default_rng(79)
+    S = wl.small_random_csr(40, 60, 0.1, rng)
+    blocks = [(rng.standard_normal((5, 12)), np.sort(rng.choice(40, 12, replace=False)).astype(np.int32))
+              for _ in range(3)]
+    blocks.append((rng.standard_normal((3, 12)), blocks[0][1]))   # a repeated col_perm
+    blocks.append((rng.standard_normal((2, 1)), np.array([7], np.int32)))
+    want = _blocks_csr_by_loops(blocks, S[0], S[1], S[2])
+    got = orc.blocks_csr(blocks, S[0], S[1], S[2], 60)
+    for (gc, gv_), (wc, wv) in zip(got, want):
+        assert np.array_equal(gc, wc)
+        assert np.array_equal(gv_.view(np.int64), wv.view(np.int64))
+
+
+@need_ref
+def test_blocks_csr_oracle_matches_upstream_pd(orc):
+    """One permuted_dense block times a sparse matrix by the upstream library
+    (BA_matrices_* with B permuted_dense, src/permuted_dense/permuted_dense_linalg.c:313-430)
+    against the oracle's dense-block product, bit for bit."""
+    from sparsediff_linalg_b200._lib import CSR_p, matrix_p
+    ref = orc.reference()
+    rng = np.random.default_rng(80)
+    A = wl.small_random_csr(90, 400, 0.04, rng)            # S: 90 x 400
+    rp = np.sort(rng.choice(150, size=21, replace=False)).astype(np.int32)
+    cp = np.sort(rng.choice(90, size=33, replace=False)).astype(np.int32)
+    X = rng.standard_normal((21, 33))
+    c = ref.new_CSR_matrix(90, 400, len(A[1]))
+    s = c.contents
+    np.ctypeslib.as_array(s.p, shape=(91,))[:] = A[0]
+    np.ctypeslib.as_array(s.i, shape=(max(1, len(A[1])),))[:len(A[1])] = A[1]
+    np.ctypeslib.as_array(s.x, shape=(max(1, len(A[1])),))[:len(A[1])] = A[2]
+    Ar = ref.new_sparse_matrix(c)
+    Br = ref.new_permuted_dense(150, 90, 21, 33, rp.ctypes.data, cp.ctypes.data, X.ctypes.data)
+    Cr = ref.BA_matrices_alloc(Br, Ar)
+    ref.BA_matrices_fill_values(Br, Ar, Cr)
+    to_csr = C.CFUNCTYPE(CSR_p, matrix_p)
+    wp, wi, wx, wm, wn = csr_from_ptr(to_csr(Cr.contents.to_csr)(Cr))
+    (cols, Ck), = orc.blocks_csr([(X, cp)], A[0], A[1], A[2], 400)
+    for k, r in enumerate(rp):
+        assert np.array_equal(wi[wp[r]:wp[r + 1]], cols)
+        assert np.array_equal(wx[wp[r]:wp[r + 1]].view(np.int64), Ck[k].view(np.int64))
+    ref.free_matrix(Cr)
+    ref.free_matrix(Br)
+    ref.free_matrix(Ar)
