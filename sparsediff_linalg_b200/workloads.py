@@ -234,3 +234,26 @@ def skewed_device(seed=0, m=1_000_000, n=1_000_000, alpha=1.5, target=20_000_000
     A, sa = one()
     B, sb = one()
     return A, B, (sa, sb)
+
+
+def coalesce_device(seed=5, m=1_000_000, n=1_000_000, unique=35_000_000, dups=15_000_000, device="cuda"):
+    """The coalescing configuration generated on the GPU (torch, seeded): `unique`
+    distinct (row, col) pairs drawn uniformly over m x n, plus `dups` repeats drawn
+    uniformly from those pairs, shuffled; N(0, 1) values. Returns (rows, cols, x, m, n)
+    with int32 / float64 device tensors."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    total = m * n
+    keys = torch.unique(torch.randint(0, total, (int(unique * 1.01) + 16,), generator=g, device=device))
+    while keys.numel() < unique:
+        extra = torch.randint(0, total, (unique - keys.numel() + 1000,), generator=g, device=device)
+        keys = torch.unique(torch.cat([keys, extra]))
+    keys = keys[torch.randperm(keys.numel(), generator=g, device=device)[:unique]]
+    rep = keys[torch.randint(0, unique, (dups,), generator=g, device=device)]
+    allk = torch.cat([keys, rep])
+    allk = allk[torch.randperm(allk.numel(), generator=g, device=device)]
+    rows = (allk // n).to(torch.int32)
+    cols = (allk % n).to(torch.int32)
+    x = torch.randn(allk.numel(), generator=g, device=device, dtype=torch.float64)
+    return rows, cols, x, m, n
