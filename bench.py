@@ -63,6 +63,13 @@ def parse():
     ap.add_argument("--dense-blocks", type=int, default=64,
                     help="blocks of the stacked_pd x CSC case (64 is the configuration; fewer for profiling)")
     ap.add_argument("--learned-matrices", type=int, default=200)
+    ap.add_argument("--learned-runs", type=int, default=5,
+                    help="new-pattern builds per path in the skewed case (median and spread reported)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the CPU leg's comparison of every sub-result with the oracle")
+    ap.add_argument("--stub", action="store_true",
+                    help="no GPU: exercise the rank launcher, barrier and max-over-ranks reduction "
+                         "on gloo with a placeholder timed region (for CPU tests of the launcher)")
     return ap.parse_args()
 
 
@@ -74,12 +81,20 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def algorithmic_bytes_refill(nnzA, mA, nnzL, nL, len_d, nnzC, mC):
-    """Bytes a refill must move at least once (int32 = 4 B, FP64 = 8 B):
-    A (x, i, p), L = CSC of B (row indices, CSR positions of the entries and B's
-    values read through them, column offsets), d, C (read C.i, write C.x) and C.p."""
-    return (12 * nnzA + 4 * (mA + 1) + 16 * nnzL + 4 * (nL + 1) + 8 * len_d
-            + 12 * nnzC + 4 * (mC + 1))
+def algorithmic_bytes_refill(nnzA, mA, nnzL, nL, len_d, nnzC):
+    """Bytes a refill must move at least once (int32 = 4 B, FP64 = 8 B): A (x, i,
+    p), L = CSC of B (row indices, values, column offsets), d, and C (read C.i,
+    write C.x): 12 nnz(A) + 4 (m_A + 1) + 12 nnz(L) + 4 (n_L + 1) + 8 len(d) +
+    12 nnz(C)."""
+    return (12 * nnzA + 4 * (mA + 1) + 12 * nnzL + 4 * (nL + 1) + 8 * len_d + 12 * nnzC)
+
+
+def design_bytes_refill(nnzL, terms):
+    """Bytes this design moves beyond the algorithmic ones, per refill: the CSR
+    position of every L entry (B's values are read through it, 4 B), the entry
+    values V (written and read, 16 B per entry), the entry records (8 B per entry)
+    and the compiled schedule (one 4-byte word per term)."""
+    return 4 * nnzL + 16 * nnzL + 8 * nnzL + 4 * terms
 
 
 class Clocks:
@@ -137,25 +152,74 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but the launcher started {world} rank(s)")
     return world, rank, local
 
 
-def make_barrier(world):
+def launch_ranks(args):
+    """--gpus N without a torchrun environment: start N ranks of this script, one
+    process per GPU, under torch.distributed.run on 127.0.0.1, and return their
+    exit status. A hard limit well above the process group's own timeout ends a
+    launch whose ranks wait on one another."""
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def make_barrier(world, backend="nccl"):
     import torch
     import torch.distributed as dist
     if world <= 1:
         return (lambda: None), (lambda v: v)
     import datetime
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    dev = "cuda" if backend == "nccl" else "cpu"
 
     def barrier():
         dist.barrier()
 
     def allmax(v):
-        t = torch.tensor([float(v)], device="cuda")
+        t = torch.tensor([float(v)], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
     return barrier, allmax
+
+
+def allsum(v):
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t)
+    return float(t.item())
+
+
+def run_stub(args, world, rank):
+    """The launcher and the rank plumbing without a GPU (gloo): every rank takes the
+    same barrier / timed region / max-over-ranks steps as the GPU arm; rank 0 prints
+    one JSON line whose n_gpus is the number of ranks that ran."""
+    barrier, allmax = make_barrier(world, backend="gloo")
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        time.sleep(0.001 * (1 + rank))
+    t = allmax((time.perf_counter() - t0) / args.steps)
+    seen = int(allmax(rank)) + 1
+    barrier()
+    if rank == 0:
+        print(json.dumps({"metric": "stub", "value": round(world / t, 3), "unit": "steps/s", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3),
+                          "stub": True, "ranks_seen": seen}), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
 
 
 # ---------------------------------------------------------------- reference arm
@@ -237,14 +301,14 @@ def run_reference(args, world, rank):
             times.append(t_step)
     t_step = times[0]
     nnzC = int(nnzC_est)
-    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], nnzC, B[4])
+    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], nnzC)
     gbs = B_alg / t_step / 1e9
     line = {
         "impl": "reference", "metric": "btda_refill_hbm_gbs", "value": round(gbs, 3), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t_step * 1e3, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD_NAME, "nnz_C": nnzC},
+        "config": bench_config(nnzC),
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": 1, "kind": "reference",
                          "sample": f"{args.steps} upstream BTDA_matrices_fill_values refills "
                                    f"(A, B, d changed each time) on one host core"},
@@ -256,17 +320,45 @@ def run_reference(args, world, rank):
     return 0
 
 
+# ---------------------------------------------------------------- parity (CPU leg)
+def parity_of(got, want_fn, target):
+    """Compare a GPU result (p, i, x host arrays) with the oracle's (computed by
+    want_fn on the host cores): structure_equal, bit_identical, max_rel_err."""
+    from oracle import parallel
+    t0 = time.perf_counter()
+    want = want_fn()
+    cpu_s = time.perf_counter() - t0
+    r = parallel.compare_csr(got, want)
+    r.update(oracle=target, oracle_s=round(cpu_s, 2), threads=parallel.threads_default())
+    return r
+
+
+def _h(t, n=None):
+    a = t.cpu().numpy()
+    return a if n is None else a[:n]
+
+
+L2_NOTE = ("device arm: L2 flushed between timed steps (256 MiB write); "
+           "host arm: upstream's CPU refill, no device cache involved")
+
+
+def bench_config(nnz_C):
+    """The workload keys both arms print (the same on the device and host arms)."""
+    return {"workload": WORKLOAD_NAME, "nnz_C": int(nnz_C), "l2": L2_NOTE}
+
+
 # ---------------------------------------------------------------- b200 arm
 def run_b200(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
     barrier, allmax = make_barrier(world)
-    from sparsediff_linalg_b200 import lib
+    from sparsediff_linalg_b200 import lib, nvtx
     from sparsediff_linalg_b200.device import btda_product, Product
     L = lib()
     assert L.sdl_device_available() == 1, "CUDA library cannot use the device"
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
+    check = rank == 0 and world == 1 and not args.no_cpu_baseline and not args.no_parity
 
     A, B, d, A2x, B2x, d2 = workload()
     T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
@@ -276,16 +368,17 @@ def run_b200(args, world, rank, local):
     split = args.split_rows and world > 1
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    if split:
-        # rows r0..r1 of C on this rank (balanced by terms, the same ranges on every
-        # rank); A, B and d are read whole, C stays row-partitioned
-        from sparsediff_linalg_b200.device import btda_product_rows
-        from sparsediff_linalg_b200.sharding import btda_row_weights, row_ranges
-        r0, r1 = row_ranges(btda_row_weights(A[0], B[0], B[1], B[4]), world)[rank]
-        P, Tr = btda_product_rows(Ap, Ai, A[4], Bp, Bi, B[4], r0, r1)
-    else:
-        P, Tr = btda_product(Ap, Ai, A[4], Bp, Bi, B[4])
-    torch.cuda.synchronize()
+    with nvtx.range("bench: headline symbolic"):
+        if split:
+            # rows r0..r1 of C on this rank (balanced by terms, the same ranges on every
+            # rank); A, B and d are read whole, C stays row-partitioned
+            from sparsediff_linalg_b200.device import btda_product_rows
+            from sparsediff_linalg_b200.sharding import btda_row_weights, row_ranges
+            r0, r1 = row_ranges(btda_row_weights(A[0], B[0], B[1], B[4]), world)[rank]
+            P, Tr = btda_product_rows(Ap, Ai, A[4], Bp, Bi, B[4], r0, r1)
+        else:
+            P, Tr = btda_product(Ap, Ai, A[4], Bp, Bi, B[4])
+        torch.cuda.synchronize()
     symbolic_ms = (time.perf_counter() - t0) * 1e3
     # the product's plan picked by the autotuner on this pattern (timed refills
     # below run with it); it reports the as-given plan's refill time beside its own
@@ -300,11 +393,9 @@ def run_b200(args, world, rank, local):
     Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev)
     nnz_C = P.nnz
     if split:
-        import torch.distributed as dist
-        t = torch.tensor([P.nnz], dtype=torch.int64, device=dev)
-        dist.all_reduce(t)
-        nnz_C = int(t.item())
-    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], nnz_C, B[4])
+        nnz_C = int(round(allsum(P.nnz)))
+    B_alg = algorithmic_bytes_refill(len(A[1]), A[3], len(B[1]), B[4], A[3], nnz_C)
+    B_design = design_bytes_refill(len(B[1]), P.terms)
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     for w in range(args.warmup):
@@ -319,13 +410,14 @@ def run_b200(args, world, rank, local):
     launches0 = L.sdl_kernel_launch_count()
     barrier()
     torch.cuda.synchronize()
-    for k in range(args.steps):
-        ax, bx, dd = sets[k % 2]
-        flush.zero_()
-        evs[k][0].record(stream)
-        P.fill(bx, dd, ax, Cx, stream=stream)
-        evs[k][1].record(stream)
-    torch.cuda.synchronize()
+    with nvtx.range("bench: headline timed refills"):
+        for k in range(args.steps):
+            ax, bx, dd = sets[k % 2]
+            flush.zero_()
+            evs[k][0].record(stream)
+            P.fill(bx, dd, ax, Cx, stream=stream)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
     barrier()
     launches = L.sdl_kernel_launch_count() - launches0
     clocks = clk.stop()
@@ -341,6 +433,15 @@ def run_b200(args, world, rank, local):
     tj = ROOT / "profiles" / "btda_refill_traffic.json"
     if tj.exists():
         traffic = json.loads(tj.read_text()).get("dram_bytes_per_launch")
+    headline_parity = None
+    if check:
+        from oracle import parallel
+        last = (args.steps - 1) % 2
+        vA = (A[0], A[1], (A[2], A2x)[last], A[3], A[4])
+        vB = (B[0], B[1], (B[2], B2x)[last], B[3], B[4])
+        headline_parity = parity_of((_h(P.Cp), _h(P.Ci), _h(Cx, P.nnz)),
+                                    lambda: parallel.btda(vA, vB, (d, d2)[last]),
+                                    "oracle port (oracle/sdl_oracle.c), B^T D A with the last timed step's values")
 
     # ---- SpGEMM 2000x2000, 5 per row (launch-bound case): symbolic + numeric times
     from sparsediff_linalg_b200 import workloads as wl
@@ -361,24 +462,34 @@ def run_b200(args, world, rank, local):
     e1.record(stream)
     torch.cuda.synchronize()
     sp_num_us = e0.elapsed_time(e1) / 50 * 1e3
+    spgemm = {"symbolic_ms": round(sp_sym_ms, 3), "numeric_us": round(sp_num_us, 2), "nnz_C": SP.nnz}
+    if check:
+        from oracle import parallel
+        spgemm["parity"] = parity_of((_h(SP.Cp), _h(SP.Ci), _h(SCx, SP.nnz)), lambda: parallel.spgemm(SA, SB),
+                                     "oracle port (oracle/sdl_oracle.c)")
 
     batched = None
     if not args.no_batched:
-        batched = run_batched(args, dev)
+        with nvtx.range("bench: batched_512"):
+            batched = run_batched(args, dev, world, rank, barrier, allmax, check)
     learned = None
-    if not args.no_learned:
-        learned = run_learned(args, dev)
+    if not args.no_learned and world == 1:
+        with nvtx.range("bench: learned_skewed"):
+            learned = run_learned(args, dev, check)
     conversions = None
     if not args.no_conversions and world == 1:
-        conversions = run_conversions(args, dev, peaks()[0])
+        with nvtx.range("bench: conversions"):
+            conversions = run_conversions(args, dev, peaks()[0], check)
     dense = None
     if not args.no_dense and world == 1:
-        dense = run_dense(args, dev, peaks()[0])
+        with nvtx.range("bench: stacked_pd"):
+            dense = run_dense(args, dev, peaks()[0], check)
 
     # ---- e2e through the upstream C ABI with host buffers
     e2e = None
     if not args.no_e2e and not split:
-        e2e = run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world)
+        with nvtx.range("bench: e2e"):
+            e2e = run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world, check)
 
     line = {
         "metric": "btda_refill_hbm_gbs", "value": round(value, 3), "unit": "GB/s",
@@ -386,22 +497,28 @@ def run_b200(args, world, rank, local):
         "ms_per_step": round(mean_ms_max, 5), "higher_is_better": True,
         "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD_NAME, "nnz_C": nnz_C, "terms": P.terms,
-                   "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": (f"one product split by output rows over {world} GPUs" if split else
-                                   f"{world} independent products (one per GPU)") if world > 1 else "1 GPU"},
+        "config": bench_config(nnz_C),
+        "parallelism": (f"one product split by output rows over {world} GPUs" if split else
+                        f"{world} independent products (one per GPU)") if world > 1 else "1 GPU",
+        "terms": P.terms,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_kind": f"{peak_kind} (copy bandwidth)",
                      "algorithmic_bytes": B_alg,
-                     "kernel": "numeric refill (all row-class launches of one step)"},
+                     "algorithmic_formula": "12 nnz(A) + 4 (m_A + 1) + 12 nnz(L) + 4 (n_L + 1) + 8 len(d) + 12 nnz(C)",
+                     "design_bytes": B_design,
+                     "design_bytes_note": "moved beyond the algorithmic bytes: CSR positions of L (4 B/entry), "
+                                          "entry values V written + read (16 B/entry), entry records (8 B/entry), "
+                                          "schedule words (4 B/term)",
+                     "kernel": "numeric refill (all launches of one step)"},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "symbolic_ms": round(symbolic_ms, 3),
         "autotune": tune,
-        "spgemm_2000": {"symbolic_ms": round(sp_sym_ms, 3), "numeric_us": round(sp_num_us, 2),
-                        "nnz_C": SP.nnz},
+        "spgemm_2000": spgemm,
     }
+    if headline_parity is not None:
+        line["parity"] = headline_parity
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the same product by the upstream library on one host core (alloc, then fills)
         try:
@@ -430,13 +547,11 @@ def run_b200(args, world, rank, local):
     return 0
 
 
-def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world):
+def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world, check=False):
     """The metric through BTDA_matrices_fill_values on sparse matrix handles with
     host value buffers (upstream API, what SparseDiffEngine calls)."""
     import torch
-    from sparsediff_linalg_b200 import lib
     from sparsediff_linalg_b200.matrices import SparseMatrix
-    L = lib()
     Am = SparseMatrix.from_csr(*A)
     Bm = SparseMatrix.from_csr(*B)
     Cm = Am.BTA_alloc_with(Bm)
@@ -458,23 +573,48 @@ def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world):
     t = allmax(t)
     h2d = 8 * (len(A[1]) + len(B[1]) + A[3])
     d2h = 8 * Cm.nnz
-    return {"value": round(world * B_alg / t / 1e9, 3), "unit": "GB/s",
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": round(t * 1e3, 4),
-            "api": "BTDA_matrices_fill_values (host value arrays from the library's constructors, "
-                   "page-locked in place on their first transfer; d a caller-owned host array)"}
+    out = {"value": round(world * B_alg / t / 1e9, 3), "unit": "GB/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "ms_per_step": round(t * 1e3, 4),
+           "api": "BTDA_matrices_fill_values (host value arrays from the library's constructors, "
+                  "page-locked in place on their first transfer; d a caller-owned host array)"}
+    if check:
+        from oracle import parallel
+        last = (args.steps - 1) % 2
+        ax, bx, dd = vals[last]
+        out["parity"] = parity_of(Cm.csr()[:3], lambda: parallel.btda((A[0], A[1], ax, A[3], A[4]),
+                                                                        (B[0], B[1], bx, B[3], B[4]), dd),
+                                  "oracle port (oracle/sdl_oracle.c), host C after the last e2e step")
+    return out
 
 
-def run_batched(args, dev, refills=20):
+def batch_weights(inst):
+    """Terms of every B^T D A instance (its refill cost): sum over rows k of
+    nnz(B row k) * nnz(A row k), from the device row offsets."""
+    w = []
+    for k in inst:
+        la = (k["Ap"][1:] - k["Ap"][:-1]).long()
+        lb = (k["Bp"][1:] - k["Bp"][:-1]).long()
+        w.append(int((la * lb).sum()))
+    return w
+
+
+def run_batched(args, dev, world=1, rank=0, barrier=lambda: None, allmax=lambda v: v, check=False,
+                refills=20):
     """512 uneven B^T D A instances (rows log-uniform 1k..64k, cols = rows / 2, 4..16
     nnz per row), fixed patterns, `refills` value refills: batched (grouped
     persistent launches per refill, replayed from a CUDA graph) vs plain (one
-    refill per product). Inputs total several GB, far above L2, so no flush is needed."""
+    refill per product). Inputs total several GB, far above L2, so no flush is needed.
+    With N ranks the products are partitioned by their term counts (LPT, no
+    communication) and every rank refills its share; the time is the max over ranks."""
     import torch
     from sparsediff_linalg_b200 import workloads as wl
     from sparsediff_linalg_b200.device import Batch, btda_product
+    from sparsediff_linalg_b200.sharding import shard_products
     t0 = time.perf_counter()
-    inst = wl.batched_device(seed=3, count=512)
+    inst_all = wl.batched_device(seed=3, count=512)
+    mine = shard_products(batch_weights(inst_all), world)[rank] if world > 1 else list(range(len(inst_all)))
+    inst = [inst_all[i] for i in mine]
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     prods, outs = [], []
@@ -483,8 +623,7 @@ def run_batched(args, dev, refills=20):
         P, T = btda_product(k["Ap"], k["Ai"], k["n"], k["Bp"], k["Bi"], k["n"])
         prods.append((P, T))
         outs.append(torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev))
-        B_alg += algorithmic_bytes_refill(k["Ai"].numel(), k["m"], k["Bi"].numel(), k["n"], k["m"],
-                                          P.nnz, k["n"])
+        B_alg += algorithmic_bytes_refill(k["Ai"].numel(), k["m"], k["Bi"].numel(), k["n"], k["m"], P.nnz)
     torch.cuda.synchronize()
     sym_s = time.perf_counter() - t0
     Bt = Batch([p for p, _ in prods])
@@ -508,6 +647,7 @@ def run_batched(args, dev, refills=20):
 
     def timed(fn):
         evs = []
+        barrier()
         for r in range(refills):
             bind(r % 2)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -517,7 +657,7 @@ def run_batched(args, dev, refills=20):
                 e1.record(s)
             evs.append((e0, e1))
         s.synchronize()
-        return sum(a.elapsed_time(b) for a, b in evs) / refills
+        return allmax(sum(a.elapsed_time(b) for a, b in evs) / refills)
 
     for w in range(3):
         bind(w % 2)
@@ -528,15 +668,52 @@ def run_batched(args, dev, refills=20):
     ms_batched = timed(lambda st: Bt.refill(stream=st))
     ms_plain = timed(lambda st: Bt.refill_unbatched(stream=st))
     terms = sum(p.terms for p, _ in prods)
-    return {"instances": len(inst), "refills": refills, "tiles": Bt.tiles, "groups": Bt.groups,
-            "rows": int(sum(k["m"] for k in inst)),
-            "nnz_A": int(sum(k["Ai"].numel() for k in inst)), "terms": int(terms),
-            "nnz_C": int(sum(p.nnz for p, _ in prods)), "algorithmic_bytes": int(B_alg),
-            "batched_ms_per_refill": round(ms_batched, 4), "plain_ms_per_refill": round(ms_plain, 4),
-            "batched_gbs": round(B_alg / (ms_batched * 1e-3) / 1e9, 2),
-            "plain_gbs": round(B_alg / (ms_plain * 1e-3) / 1e9, 2),
-            "speedup_vs_plain": round(ms_plain / ms_batched, 3),
-            "generate_s": round(gen_s, 2), "symbolic_s": round(sym_s, 2)}
+    B_all = B_alg
+    if world > 1:
+        B_all = int(round(allsum(B_alg)))
+        terms = int(round(allsum(terms)))
+    out = {"instances": len(inst_all), "refills": refills, "tiles": Bt.tiles, "groups": Bt.groups,
+           "rows": int(sum(k["m"] for k in inst)),
+           "nnz_A": int(sum(k["Ai"].numel() for k in inst)), "terms": int(terms),
+           "nnz_C": int(sum(p.nnz for p, _ in prods)), "algorithmic_bytes": int(B_all),
+           "batched_ms_per_refill": round(ms_batched, 4), "plain_ms_per_refill": round(ms_plain, 4),
+           "batched_gbs": round(B_all / (ms_batched * 1e-3) / 1e9, 2),
+           "plain_gbs": round(B_all / (ms_plain * 1e-3) / 1e9, 2),
+           "speedup_vs_plain": round(ms_plain / ms_batched, 3),
+           "generate_s": round(gen_s, 2), "symbolic_s": round(sym_s, 2)}
+    if world > 1:
+        out["ranks"] = world
+        out["partition"] = "products by term count (LPT), no collective on the data path; time = max over ranks"
+        out["products_this_rank"] = len(inst)
+    if check:
+        # the batched path once more with the second value set, every product
+        # against the oracle
+        from oracle import parallel
+        bind(1)
+        with torch.cuda.stream(s):
+            Bt.refill(stream=s)
+        s.synchronize()
+        t0 = time.perf_counter()
+
+        def one(i):
+            k, (P, _) = inst[i], prods[i]
+            ax, bx, d = (v.cpu().numpy() for v in vals[i][1])
+            got = (_h(P.Cp), _h(P.Ci), _h(outs[i], P.nnz))
+            want = parallel.oracle.btda((_h(k["Ap"]), _h(k["Ai"]), ax, k["m"], k["n"]),
+                                        (_h(k["Bp"]), _h(k["Bi"]), bx, k["m"], k["n"]), d)
+            return parallel.compare_csr(got, want)
+
+        res = parallel.map_threads(one, range(len(inst)))
+        bad = [i for i, r in enumerate(res) if not (r["structure_equal"] and r["bit_identical"])]
+        errs = [r["max_rel_err"] for r in res]
+        out["parity"] = {"structure_equal": all(r["structure_equal"] for r in res),
+                         "bit_identical": not bad,
+                         "max_rel_err": None if any(e is None for e in errs) else max(errs, default=0.0),
+                         "products_checked": len(res), "products_differing": bad[:20],
+                         "oracle": "oracle port (oracle/sdl_oracle.c), every product, batched refill output",
+                         "oracle_s": round(time.perf_counter() - t0, 2),
+                         "threads": parallel.threads_default()}
+    return out
 
 
 def _event_ms(fn, stream, steps, flush=None):
@@ -556,7 +733,7 @@ def _event_ms(fn, stream, steps, flush=None):
     return sum(a.elapsed_time(b) for a, b in evs) / steps
 
 
-def run_conversions(args, dev, peak):
+def run_conversions(args, dev, peak, check=False):
     """CSR -> CSC of a 1M x 1M matrix with 10 distinct uniform columns per row, and
     coalescing of 50M COO triplets over 1M x 1M (35M distinct pairs plus 15M repeats,
     shuffled) into CSR with duplicates summed in input order. Structure (once per
@@ -597,6 +774,11 @@ def run_conversions(args, dev, peak):
         "conversion_ms": round(struct_ms, 3),
         "conversion_gbs": round(b_full / (struct_ms * 1e-3) / 1e9, 1),
         "algorithmic_bytes_fill": b_fill, "algorithmic_bytes_conversion": b_full}
+    if check:
+        from oracle import oracle
+        out["csr_to_csc_1M"]["parity"] = parity_of(
+            (_h(T.Tp), _h(T.Ti), _h(Tx)), lambda: oracle.transpose(A[0], A[1], A[2], m, n),
+            "oracle port (oracle/sdl_oracle.c), whole matrix")
     if not args.no_cpu_baseline:
         try:
             r = reference_csr_to_csc_times(A, 3)
@@ -606,12 +788,9 @@ def run_conversions(args, dev, peak):
             out["csr_to_csc_1M"]["upstream_cpu"] = {"unavailable": str(e)[:200]}
     del T, Ap, Ai, Ax, Tx, A
     torch.cuda.empty_cache()
-    # ---- 4c: COO coalescing
-    rows, cols, x, m, n = wl.coalesce_big(seed=5)
-    N = len(rows)
-    R = torch.as_tensor(rows, device=dev)
-    Cc = torch.as_tensor(cols, device=dev)
-    X = torch.as_tensor(x, device=dev)
+    # ---- 4c: COO coalescing (the triplets are drawn on the GPU)
+    R, Cc, X, m, n = wl.coalesce_device(seed=5, device=dev)
+    N = R.numel()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     CO = Coalesce(R, Cc, m, n, stream=s)
@@ -632,9 +811,28 @@ def run_conversions(args, dev, peak):
         "fill_frac_of_hbm": round(b_fill / (fill_ms * 1e-3) / 1e9 / peak, 4),
         "coalesce_gbs": round(b_full / ((struct_ms) * 1e-3) / 1e9, 1),
         "algorithmic_bytes_fill": b_fill, "algorithmic_bytes_coalesce": b_full}
+    if check:
+        from oracle import parallel
+        hr, hc, hx = _h(R), _h(Cc), _h(X)
+        out["coo_coalesce_50M"]["parity"] = parity_of(
+            (_h(CO.Cp), _h(CO.Ci), _h(Cx, CO.nnz)), lambda: parallel.coalesce(hr, hc, hx, m, n),
+            "oracle port (oracle/sdl_oracle.c; equal to upstream row_reduce of the one-triplet-per-row "
+            "CSR), all 50M triplets")
     del CO, R, Cc, X, Cx
     torch.cuda.empty_cache()
     return out
+
+
+def stacked_pd_S(rng, S_n, n0, per_col):
+    """S (n0 x S_n CSR) with `per_col` distinct uniform rows in every column: drawn as
+    the rows of S^T and transposed with numpy (a stable sort by column)."""
+    from sparsediff_linalg_b200 import workloads as wl
+    St = wl.fixed_rowlen_csr(S_n, n0, per_col, rng)
+    rows_of = np.repeat(np.arange(S_n, dtype=np.int64), np.diff(St[0]))   # column of S
+    order = np.argsort(St[1], kind="stable")
+    Sp = np.zeros(n0 + 1, np.int32)
+    Sp[1:] = np.cumsum(np.bincount(St[1], minlength=n0))
+    return Sp, rows_of[order].astype(np.int32), St[2][order]
 
 
 def reference_ba_spd_csr_times(m, blocks_rows, cperm, X, S, reps):
@@ -654,15 +852,13 @@ def reference_ba_spd_csr_times(m, blocks_rows, cperm, X, S, reps):
     return out
 
 
-def run_dense(args, dev, peak):
+def run_dense(args, dev, peak, check=False):
     """stacked_pd x CSC: 64 permuted-dense blocks of 64 x 256 (N(0,1)) whose 4096
     rows are a random permutation, col_perm 0..255, times S 256 x 100000 with 6
     distinct uniform rows per column (upstream BA_spd_csr_*): 64 output blocks of
     64 x 100000, 3.28 GB of FP64 -- bound by writing C. Algorithmic bytes:
     8 sum(m0 n0) + 12 nnz(S) + 4 (n_S + 1) + 8 nnz(C) + 4 sum(n0_C)."""
     import torch
-    from oracle import oracle
-    from sparsediff_linalg_b200 import workloads as wl
     from sparsediff_linalg_b200.device import BlocksCsr
     rng = np.random.default_rng(6)
     nb, m0, n0, S_n = args.dense_blocks, 64, 256, 100_000
@@ -670,8 +866,7 @@ def run_dense(args, dev, peak):
     blocks_rows = np.concatenate([np.sort(rows[k * m0:(k + 1) * m0]) for k in range(nb)]).astype(np.int32)
     cperm = np.arange(n0, dtype=np.int32)
     X = rng.standard_normal((nb, m0, n0))
-    St = wl.fixed_rowlen_csr(S_n, n0, 6, rng)  # S's columns as rows of S^T
-    Sp, Si, Sx = oracle.transpose(St[0], St[1], St[2], S_n, n0)
+    Sp, Si, Sx = stacked_pd_S(rng, S_n, n0, 6)
     S = (Sp, Si, Sx, n0, S_n)
     t0 = time.perf_counter()
     P = BlocksCsr([m0] * nb, [n0] * nb, [cperm] * nb, Sp, Si, n0, S_n)
@@ -694,6 +889,27 @@ def run_dense(args, dev, peak):
            "fill_gbs": round(B_alg / (ms * 1e-3) / 1e9, 1),
            "fill_frac_of_hbm": round(B_alg / (ms * 1e-3) / 1e9 / peak, 4), "algorithmic_bytes": int(B_alg),
            "l2": "flushed before each timed fill (256 MiB write); C (3.28 GB) exceeds L2"}
+    if check:
+        from oracle import oracle, parallel
+        got = Cv.cpu().numpy()
+        offs = np.concatenate([[0], np.cumsum([b[1] * b[2] for b in P.blocks])])
+        t0 = time.perf_counter()
+
+        def one(k):
+            src, mk, n0c, perm = P.blocks[k]
+            (cols, Cw), = oracle.blocks_csr([(X[src], cperm)], Sp, Si, Sx, S_n)
+            Cg = got[offs[k]:offs[k + 1]].reshape(mk, n0c)
+            ok = src == k and np.array_equal(perm, cols)
+            bits = ok and np.array_equal(Cg.view(np.int64), Cw.view(np.int64))
+            err = float(np.max(np.abs(Cg - Cw) / np.maximum(np.abs(Cw), 1e-300))) if ok and not bits else 0.0
+            return ok, bits, err
+
+        res = parallel.map_threads(one, range(P.out_blocks))
+        out["parity"] = {"structure_equal": all(r[0] for r in res), "bit_identical": all(r[1] for r in res),
+                         "max_rel_err": max((r[2] for r in res), default=0.0), "blocks_checked": len(res),
+                         "oracle": "oracle restatement of BA_pd_csr (oracle/oracle.py blocks_csr), every block",
+                         "oracle_s": round(time.perf_counter() - t0, 2), "threads": parallel.threads_default()}
+        del got
     if not args.no_cpu_baseline:
         try:
             r = reference_ba_spd_csr_times(nb * m0, blocks_rows, cperm, X, S, 1)
@@ -703,7 +919,7 @@ def run_dense(args, dev, peak):
             out["upstream_cpu"] = {"unavailable": str(e)[:200]}
     del P, Bv, Sx_d, Cv
     torch.cuda.empty_cache()
-    out["ata_dmma"] = run_dense_ata(args, dev, X, blocks_rows, cperm)
+    out["ata_dmma"] = run_dense_ata(args, dev, X, blocks_rows, cperm, check)
     return out
 
 
@@ -722,7 +938,7 @@ def reference_atda_spd_times(m, n, blocks_rows, cperm, X, d, reps):
     return out
 
 
-def run_dense_ata(args, dev, X, blocks_rows, cperm):
+def run_dense_ata(args, dev, X, blocks_rows, cperm, check=False):
     """A^T diag(d) A of the same stacked_pd (64 blocks of 64 x 256, col_perm 0..255):
     64 partials of 256 x 256 on the FP64 tensor cores (mma.sync m8n8k4), summed in
     block order into one 256 x 256 block. 2 * 64 * 64 * 256 * 256 flops."""
@@ -745,6 +961,23 @@ def run_dense_ata(args, dev, X, blocks_rows, cperm):
     out = {"workload": "A^T diag(d) A, A the stacked_pd above (64 blocks of 64 x 256), FP64 tensor cores",
            "out_blocks": P.out_blocks, "fill_us": round(ms * 1e3, 2),
            "fp64_tflops": round(flops / (ms * 1e-3) / 1e12, 2), "flops": int(flops)}
+    if check:
+        from oracle import oracle
+        t0 = time.perf_counter()
+        want = oracle.blocks_ata([(X[k], blocks_rows[k * m0:(k + 1) * m0], cperm) for k in range(nb)], d, n0)
+        got = Cv.cpu().numpy()
+        ok, worst, off = len(want) == P.out_blocks, 0.0, 0
+        for (rows_g, cols_g), (rows_o, cols_o, Cw, Ca) in zip(P.blocks, want):
+            ok = ok and np.array_equal(rows_g, rows_o) and np.array_equal(cols_g, cols_o)
+            Cg = got[off:off + Cw.size].reshape(Cw.shape)
+            off += Cw.size
+            worst = max(worst, float(np.max(np.abs(Cg - Cw) / (Ca + 1e-300))))
+        out["parity"] = {"structure_equal": bool(ok), "max_err_over_sum_abs_terms": worst,
+                         "within_tol": bool(ok and worst <= 1e-12),
+                         "oracle": "numpy A^T diag(d) A per block + upstream's coalescing order "
+                                   "(oracle/oracle.py blocks_ata); upstream uses dgemm, so values agree "
+                                   "within rounding, bounded by 1e-12 of the sum of |terms|",
+                         "oracle_s": round(time.perf_counter() - t0, 2)}
     if not args.no_cpu_baseline:
         try:
             r = reference_atda_spd_times(m, n0, blocks_rows, cperm, X, d, 3)
@@ -755,7 +988,7 @@ def run_dense_ata(args, dev, X, blocks_rows, cperm):
     return out
 
 
-def run_learned(args, dev):
+def run_learned(args, dev, check=False):
     """Skewed SpGEMM C = A B, A and B 1M x 1M with Zipf(1.5) row lengths (~20M nnz
     each, rows capped at 50k): the plain exact symbolic pass + refill against the
     learned one (scratch sized by the network, exact fallback) + refill. The
@@ -804,7 +1037,15 @@ def run_learned(args, dev):
     same = bool(torch.equal(plain_cp, learned.Cp) and torch.equal(plain_ci, learned.Ci) and
                 torch.equal(cx_plain.view(torch.int64), cx_learned.view(torch.int64)))
     st = learned.stats
-    return {"workload": "C = A B, A and B 1M x 1M, Zipf(1.5) row lengths scaled to ~20M nnz, cap 50k",
+    parity = None
+    if check:
+        from oracle import parallel
+        hA = (_h(Ap), _h(Ai), _h(Ax), m, m)
+        hB = (_h(Bp), _h(Bi), _h(Bx), m, m)
+        parity = parity_of((_h(learned.Cp), _h(learned.Ci), _h(cx_learned, learned.nnz)),
+                           lambda: parallel.spgemm(hA, hB),
+                           "oracle port (oracle/sdl_oracle.c), whole product, learned path output")
+    res = {"workload": "C = A B, A and B 1M x 1M, Zipf(1.5) row lengths scaled to ~20M nnz, cap 50k",
             "nnz_A": int(Ai.numel()), "nnz_B": int(Bi.numel()), "terms": int(learned.terms),
             "nnz_C": int(learned.nnz), "zipf_scale": [round(x, 6) for x in scales],
             "plain": {"symbolic_ms": round(ps, 2), "numeric_ms": round(pn, 3),
@@ -815,6 +1056,9 @@ def run_learned(args, dev):
                         "capacity_over_nnz": round(st["capacity"] / max(1, learned.nnz), 4),
                         "term_bound_over_nnz": round(st["term_bound"] / max(1, learned.nnz), 4)},
             "identical_structure_and_values": same, "training": info, "generate_s": round(gen_s, 2)}
+    if parity is not None:
+        res["parity"] = parity
+    return res
 
 
 def cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg):
@@ -835,7 +1079,11 @@ def cpu_baseline(args, A, B, d, A2x, B2x, d2, B_alg):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args)
     world, rank, local = dist_setup(args)
+    if args.stub:
+        return run_stub(args, world, rank)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     return run_b200(args, world, rank, local)
