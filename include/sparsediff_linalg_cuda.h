@@ -131,6 +131,26 @@ sdl_status sdl_product_replan(sdl_product *P, int tile_budget, int tile_max_term
    row (terms) its tiles take. Any pointer may be NULL. */
 sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, int *tile_max_terms);
 
+/* No upstream counterpart (it generalises upstream's fixed plan-vs-accumulator
+   threshold GUSTAVSON_PLAN_MAX_RATIO, src/internal/gustavson.h:52, used at
+   src/sparse/sparse_matrix.c:270-277): the tuning table. sdl_product_autotune
+   records its choice under P's pattern key -- rows of C, columns of A, terms per
+   row, terms per output and the histogram of C's row lengths over power-of-two
+   classes -- in a table of the process; sdl_product_apply_tuned re-plans a product
+   with the configuration recorded for its key (structure unchanged; *found = 0 and
+   nothing changes when the key is absent). The table is saved to and loaded from a
+   text file (one entry per line), so a later process takes tuned plans without
+   timing candidates; loading adds to the table (an entry replaces one of the same
+   key) and rejects a malformed file as a whole. The pattern key is written into
+   buf (NUL-terminated; len bytes available). apply_tuned and pattern_key
+   synchronise the stream; apply_tuned allocates. */
+sdl_status sdl_product_apply_tuned(sdl_product *P, int *found, void *stream);
+sdl_status sdl_product_pattern_key(const sdl_product *P, char *buf, int len, void *stream);
+sdl_status sdl_tune_table_save(const char *path);
+sdl_status sdl_tune_table_load(const char *path, int *entries);
+sdl_status sdl_tune_table_clear(void);
+sdl_status sdl_tune_table_size(int *entries);
+
 /* No upstream counterpart. Same result as sdl_product_fill, bit for bit, for
    callers that cannot call cudaMalloc while they refill: device memory wholly
    owned by another allocator, a fixed device-memory budget that may not grow, or

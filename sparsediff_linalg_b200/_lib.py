@@ -103,6 +103,12 @@ EXTENSION_SIGNATURES = {
     "sdl_product_tuning": (C.c_int, [vp, c_int_p, c_int_p, c_int_p, c_int_p, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), c_int_p, C.POINTER(C.c_double)]),
     "sdl_product_refill_shape": (C.c_int, [vp, c_int_p, c_int_p]),
+    "sdl_product_apply_tuned": (C.c_int, [vp, c_int_p, vp]),
+    "sdl_product_pattern_key": (C.c_int, [vp, C.c_char_p, C.c_int, vp]),
+    "sdl_tune_table_save": (C.c_int, [C.c_char_p]),
+    "sdl_tune_table_load": (C.c_int, [C.c_char_p, c_int_p]),
+    "sdl_tune_table_clear": (C.c_int, []),
+    "sdl_tune_table_size": (C.c_int, [c_int_p]),
     "sdl_product_replan": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]),
     "sdl_product_destroy": (None, [vp]),
     "sdl_product_fill_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp]),

@@ -1,3 +1,4 @@
+#include <cstring>
 // Device-resident extension API (sparsediff_linalg_cuda.h): products, transposes
 // and duplicate coalescing whose operands and results stay in HBM.
 #include <memory>
@@ -102,7 +103,34 @@ extern "C" sdl_status sdl_product_autotune(sdl_product *P, int reps, void *strea
 {
     return guard_status("sdl_product_autotune", [&]() {
         if (!P) fail(SDL_ERR_INVALID, "NULL product");
-        P->tuned = product_autotune(P->P, reps, pick_stream(stream));
+        cudaStream_t s = pick_stream(stream);
+        P->tuned = product_autotune(P->P, reps, s);
+        tune_table_record(product_pattern_key(P->P, s), P->P.cfg, P->tuned.refill_us);
+    });
+}
+
+extern "C" sdl_status sdl_product_apply_tuned(sdl_product *P, int *found, void *stream)
+{
+    return guard_status("sdl_product_apply_tuned", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        if (found) *found = 0;
+        cudaStream_t s = pick_stream(stream);
+        TuneConfig c;
+        if (!tune_table_lookup(product_pattern_key(P->P, s), c)) return;
+        product_replan(P->P, c, s);
+        P->tuned = TuneResult{};
+        P->tuned.best = c;
+        if (found) *found = 1;
+    });
+}
+
+extern "C" sdl_status sdl_product_pattern_key(const sdl_product *P, char *buf, int len, void *stream)
+{
+    return guard_status("sdl_product_pattern_key", [&]() {
+        if (!P || !buf || len <= 0) fail(SDL_ERR_INVALID, "NULL argument");
+        const std::string k = product_pattern_key(P->P, pick_stream(stream));
+        if ((int)k.size() >= len) fail(SDL_ERR_INVALID, "key buffer too short");
+        std::memcpy(buf, k.c_str(), k.size() + 1);
     });
 }
 

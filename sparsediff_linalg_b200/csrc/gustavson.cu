@@ -24,6 +24,8 @@
 #include <chrono>
 #include <cstddef>
 #include <climits>
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 
@@ -2386,6 +2388,55 @@ TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
     R.refill_us = best_us;
     R.tune_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     return R;
+}
+
+
+// ------------------------------------------------------------------ pattern key
+// Statistics of a product's pattern that the tuning table is keyed on: rows of C,
+// columns of A, terms per row, terms per output, and the histogram of row lengths
+// of C over power-of-two classes. Patterns with equal keys share a tuned plan.
+namespace {
+__global__ void k_rowlen_hist(const int *__restrict__ Cp, int m, unsigned long long *__restrict__ hist)
+{
+    __shared__ unsigned long long h[33];
+    for (int q = threadIdx.x; q < 33; q += blockDim.x) h[q] = 0;
+    __syncthreads();
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m; r += (long long)gridDim.x * blockDim.x)
+    {
+        const int len = Cp[r + 1] - Cp[r];
+        atomicAdd(&h[len > 0 ? 32 - __clz(len) : 0], 1ULL);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 33; q += blockDim.x)
+        if (h[q]) atomicAdd(&hist[q], h[q]);
+}
+} // namespace
+
+std::string product_pattern_key(const Product &P, cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    unsigned long long hist[33] = {0};
+    if (P.m_out > 0)
+    {
+        DevBuf<unsigned long long> dh(33);
+        SDL_CUDA(cudaMemsetAsync(dh.get(), 0, dh.bytes(), s));
+        SDL_LAUNCH(k_rowlen_hist, grid_for(P.m_out, 256, rt.num_sms * 4), 256, 0, s, P.Cp.get(), P.m_out, dh.get());
+        SDL_CUDA(cudaMemcpyAsync(hist, dh.get(), sizeof(hist), cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaStreamSynchronize(s));
+    }
+    auto lg = [](double v) { return (int)std::floor(std::log2(v + 1.0)); };
+    const double rows = std::max(1, P.m_out);
+    char buf[96];
+    std::snprintf(buf, sizeof buf, "m%d.n%d.t%d.c%d.h", lg(P.m_out), lg(P.n),
+                  (int)std::lround(2.0 * std::log2((double)P.terms / rows + 1.0)),
+                  (int)std::min<long long>(64, std::llround(4.0 * (double)P.terms / std::max(1, P.nnz))));
+    std::string key(buf);
+    for (int b = 0; b < 33; ++b)
+    {
+        const int eighths = (int)std::lround(8.0 * (double)hist[b] / rows);
+        if (eighths > 0) key += std::to_string(b) + ":" + std::to_string(eighths) + ",";
+    }
+    return key;
 }
 
 } // namespace sdl

@@ -310,6 +310,14 @@ void product_replan(Product &P, const TuneConfig &c, cudaStream_t s);
 // refill CTAs per SM by refills with placeholder values (L2 flushed before each);
 // P ends up planned with the fastest, which is returned with its timings.
 TuneResult product_autotune(Product &P, int reps, cudaStream_t s);
+// Key of P's pattern for the tuning table: rows of C, columns of A, terms per row,
+// terms per output and the histogram of C's row lengths over power-of-two classes
+// (each class's share of the rows in eighths). Synchronises the stream.
+std::string product_pattern_key(const Product &P, cudaStream_t s);
+// The process's tuning table (tune_table.cpp): the configuration recorded for a
+// pattern key (record replaces an earlier one), and its lookup.
+void tune_table_record(const std::string &key, const TuneConfig &c, double refill_us);
+bool tune_table_lookup(const std::string &key, TuneConfig &c);
 // Symbolic phase: fills P.Cp, P.Ci, P.nnz and the numeric schedule.
 void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P,
                       cudaStream_t s, bool keep_row_terms = false);

@@ -88,6 +88,20 @@ class Product:
                                        refill_ctas_per_sm, _stream(stream)))
         self._init_from_handle(self.handle)
 
+    def apply_tuned(self, stream=None):
+        """Re-plan with the tuning table's configuration for this pattern (True if
+        the table had one)."""
+        found = C.c_int()
+        check(lib().sdl_product_apply_tuned(self.handle, C.byref(found), _stream(stream)))
+        if found.value:
+            self._init_from_handle(self.handle)
+        return bool(found.value)
+
+    def pattern_key(self, stream=None):
+        buf = C.create_string_buffer(512)
+        check(lib().sdl_product_pattern_key(self.handle, buf, 512, _stream(stream)))
+        return buf.value.decode()
+
     def refill_shape(self):
         th, tm = C.c_int(), C.c_int()
         check(lib().sdl_product_refill_shape(self.handle, C.byref(th), C.byref(tm)))
@@ -379,3 +393,23 @@ class KeyGrouping:
 
 def group_by_key(keys, nkeys):
     return KeyGrouping(keys, nkeys)
+
+
+def tune_table_save(path):
+    check(lib().sdl_tune_table_save(str(path).encode()))
+
+
+def tune_table_load(path):
+    n = C.c_int()
+    check(lib().sdl_tune_table_load(str(path).encode(), C.byref(n)))
+    return n.value
+
+
+def tune_table_clear():
+    check(lib().sdl_tune_table_clear())
+
+
+def tune_table_size():
+    n = C.c_int()
+    check(lib().sdl_tune_table_size(C.byref(n)))
+    return n.value
