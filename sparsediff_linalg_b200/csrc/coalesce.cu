@@ -173,4 +173,176 @@ void coalesce_order_fill(const int *ostart, const int *perm, const double *x, co
     SDL_LAUNCH(k_coal_fill, grid_coal(nout, 256), 256, 0, s, ostart, perm, x, f, nout, C);
 }
 
+// ------------------------------------------------------------------ bucketed refill
+// For large inputs the one-pass refill gathers every triplet value at random from
+// an array far larger than L2, so DRAM moves whole sectors for 8 useful bytes. The
+// bucketed refill splits it into two streaming-friendly passes:
+//  1. the values are read in input order, a chunk of CO_CHUNK triplets per CTA,
+//     and written into output-range buckets (bucket b holds the triplets of outputs
+//     [b * span, (b + 1) * span)), each chunk's triplets of one bucket as one
+//     contiguous run, after the chunk's runs of that bucket from earlier chunks --
+//     so every bucket holds its triplets in input order;
+//  2. the one-pass refill, reading from the buckets instead of the input: an
+//     output's triplets now lie in one bucket of a few MB, which stays in L2 while
+//     the outputs of that range are summed.
+// The sums are the same sums in the same order (ascending triplet per output,
+// from +0.0), so the result is bit-identical to the one-pass refill.
+namespace {
+constexpr int CO_CHUNK = 4096;
+constexpr int CO_THREADS = 256;
+constexpr int CO_MAX_BUCKETS = 512;
+
+// Output index of every triplet (inverse of the output-order permutation).
+__global__ void k_cb_owner(const int *__restrict__ ostart, const int *__restrict__ perm, int nout,
+                           int *__restrict__ owner)
+{
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < nout; o += (long long)gridDim.x * blockDim.x)
+        for (int q = ostart[o]; q < ostart[o + 1]; ++q) owner[perm[q]] = (int)o;
+}
+
+// Per chunk: its triplets stably ordered by bucket (bitonic sort of bucket << 12 |
+// index in shared memory), the order (lperm), each bucket's first position in it
+// (cbound, nb + 1 per chunk), each bucket's count (count, bucket-major for the
+// scan over chunks) and every triplet's rank inside its bucket's run (rank).
+__global__ void __launch_bounds__(CO_THREADS) k_cb_chunks(const int *__restrict__ owner, int n, int span, int nb,
+                                                         unsigned short *__restrict__ lperm, int *__restrict__ cbound,
+                                                         int *__restrict__ count, int nchunks,
+                                                         unsigned short *__restrict__ rank)
+{
+    __shared__ unsigned key[CO_CHUNK];
+    __shared__ int bstart[CO_MAX_BUCKETS + 1];
+    const int c = blockIdx.x;
+    const long long t0 = (long long)c * CO_CHUNK;
+    const int cnt = (int)(n - t0 < CO_CHUNK ? n - t0 : CO_CHUNK);
+    for (int i = threadIdx.x; i < CO_CHUNK; i += CO_THREADS)
+        key[i] = i < cnt ? ((unsigned)(owner[t0 + i] / span) << 12) | (unsigned)i : 0xffffffffu;
+    for (int b = threadIdx.x; b <= nb; b += CO_THREADS) bstart[b] = cnt;
+    __syncthreads();
+    for (int k = 2; k <= CO_CHUNK; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1)
+        {
+            for (int i = threadIdx.x; i < CO_CHUNK; i += CO_THREADS)
+            {
+                const int l = i ^ j;
+                if (l > i)
+                {
+                    const unsigned a = key[i], b = key[l];
+                    if (((i & k) == 0) == (a > b))
+                    {
+                        key[i] = b;
+                        key[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // first position of every bucket present in the chunk; absent buckets take the
+    // start of the next present one (filled backwards below)
+    for (int i = threadIdx.x; i < cnt; i += CO_THREADS)
+    {
+        const int b = (int)(key[i] >> 12);
+        if (i == 0 || (int)(key[i - 1] >> 12) != b) bstart[b] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (int b = nb - 1; b >= 0; --b) bstart[b] = min(bstart[b], bstart[b + 1]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < cnt; i += CO_THREADS)
+    {
+        const int b = (int)(key[i] >> 12), li = (int)(key[i] & 0xfffu);
+        lperm[t0 + i] = (unsigned short)li;
+        rank[t0 + li] = (unsigned short)(i - bstart[b]);
+    }
+    for (int b = threadIdx.x; b <= nb; b += CO_THREADS)
+    {
+        cbound[(long long)c * (nb + 1) + b] = bstart[b];
+        if (b < nb) count[(long long)b * nchunks + c] = bstart[b + 1] - bstart[b];
+    }
+}
+
+// Bucket position of the triplet in every output-order slot.
+__global__ void k_cb_perm2(const int *__restrict__ perm, const int *__restrict__ owner,
+                           const unsigned short *__restrict__ rank, const long long *__restrict__ dst, int n, int span,
+                           int nchunks, int *__restrict__ perm2)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    {
+        const int t = perm[q];
+        const int b = owner[t] / span, c = t / CO_CHUNK;
+        perm2[q] = (int)(dst[(long long)b * nchunks + c] + rank[t]);
+    }
+}
+
+// Pass 1: a CTA per chunk; the chunk's values (times their factors) are staged in
+// shared memory, then every warp writes the runs of its share of the buckets.
+__global__ void __launch_bounds__(CO_THREADS) k_cb_scatter(const double *__restrict__ x, const double *__restrict__ f,
+                                                          int n, int nb, const unsigned short *__restrict__ lperm,
+                                                          const int *__restrict__ cbound,
+                                                          const long long *__restrict__ dst, int nchunks,
+                                                          double *__restrict__ buf)
+{
+    __shared__ double xs[CO_CHUNK];
+    __shared__ int bs[CO_MAX_BUCKETS + 1];
+    const int c = blockIdx.x;
+    const long long t0 = (long long)c * CO_CHUNK;
+    const int cnt = (int)(n - t0 < CO_CHUNK ? n - t0 : CO_CHUNK);
+    for (int i = threadIdx.x; i < cnt; i += CO_THREADS)
+        xs[i] = f ? __dmul_rn(__ldcs(f + t0 + i), __ldcs(x + t0 + i)) : __ldcs(x + t0 + i);
+    for (int b = threadIdx.x; b <= nb; b += CO_THREADS) bs[b] = __ldcs(cbound + (long long)c * (nb + 1) + b);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = warp; b < nb; b += CO_THREADS / 32)
+    {
+        const int i0 = bs[b], i1 = bs[b + 1];
+        if (i0 == i1) continue;
+        double *out = buf + dst[(long long)b * nchunks + c];
+        for (int i = i0 + lane; i < i1; i += 32) out[i - i0] = xs[__ldcs(lperm + t0 + i)];
+    }
+}
+} // namespace
+
+void coalesce_bucket_build(const int *ostart, const int *perm, int n, int nout, CoalesceBuckets &B, cudaStream_t s)
+{
+    B = CoalesceBuckets{};
+    if (n < COALESCE_BUCKET_MIN || nout <= 0) return;
+    Runtime &rt = runtime();
+    int span = 1 << 17;
+    while ((long long)(nout + span - 1) / span > CO_MAX_BUCKETS) span <<= 1;
+    const int nb = (nout + span - 1) / span;
+    const int nchunks = (int)(((long long)n + CO_CHUNK - 1) / CO_CHUNK);
+    DevBuf<int> owner((size_t)n);
+    SDL_LAUNCH(k_cb_owner, grid_coal(nout, 256), 256, 0, s, ostart, perm, nout, owner.get());
+    B.lperm.reset((size_t)n);
+    B.cbound.reset((size_t)nchunks * (nb + 1));
+    DevBuf<int> count((size_t)nb * nchunks);
+    DevBuf<long long> count64((size_t)nb * nchunks);
+    DevBuf<unsigned short> rank((size_t)n);
+    SDL_LAUNCH(k_cb_chunks, nchunks, CO_THREADS, 0, s, owner.get(), n, span, nb, B.lperm.get(), B.cbound.get(),
+               count.get(), nchunks, rank.get());
+    // run offsets: bucket-major exclusive scan of the per-chunk counts
+    widen_i32(count.get(), count64.get(), (long long)nb * nchunks, s);
+    B.dst.reset((size_t)nb * nchunks + 1);
+    const long long total = exclusive_scan_i64(count64.get(), B.dst.get(), (long long)nb * nchunks, s);
+    if (total != n) fail(SDL_ERR_INTERNAL, "coalesce buckets: runs do not cover the triplets");
+    B.perm2.reset((size_t)n);
+    SDL_LAUNCH(k_cb_perm2, grid_coal(n, 256), 256, 0, s, perm, owner.get(), rank.get(), B.dst.get(), n, span,
+               nchunks, B.perm2.get());
+    B.buf.reset((size_t)n);
+    B.nb = nb;
+    B.nchunks = nchunks;
+    B.n = n;
+    SDL_CUDA(cudaStreamSynchronize(s));
+    (void)rt;
+}
+
+void coalesce_bucket_fill(const CoalesceBuckets &B, const int *ostart, const double *x, const double *f, int nout,
+                          double *C, cudaStream_t s)
+{
+    SDL_LAUNCH(k_cb_scatter, B.nchunks, CO_THREADS, 0, s, x, f, B.n, B.nb, B.lperm.get(), B.cbound.get(), B.dst.get(),
+               B.nchunks, B.buf.get());
+    SDL_LAUNCH(k_coal_fill, grid_coal(nout, 256), 256, 0, s, ostart, B.perm2.get(), B.buf.get(), nullptr, nout, C);
+}
+
 } // namespace sdl

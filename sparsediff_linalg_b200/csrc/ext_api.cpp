@@ -29,9 +29,11 @@ struct sdl_coalesce
     int m = 0, n = 0, nnz_in = 0, nout = 0;
     DevBuf<int> Cp, Ci;       // the coalesced CSR structure
     DevBuf<int> perm, ostart; // triplets in output order; first slot of every output
+    CoalesceBuckets buckets;  // bucketed refill plan (large inputs)
 };
 
 namespace sdl {
+void coalesce_fill_scaled(const sdl_coalesce *C, const double *x, const double *d, double *Cx, cudaStream_t s);
 int coalesce_sorted_build(const int *rows, const int *cols, int n, int m, int ncols, DevBuf<int> &Cp, DevBuf<int> &Ci,
                           DevBuf<int> &perm, DevBuf<int> &ostart, cudaStream_t s);
 void coalesce_order_fill(const int *ostart, const int *perm, const double *x, const double *f, int nout, double *C,
@@ -267,6 +269,7 @@ extern "C" sdl_status sdl_coalesce_create(const int *rows, const int *cols, int 
         c->n = n;
         c->nnz_in = nnz_in;
         c->nout = coalesce_sorted_build(rows, cols, nnz_in, m, n, c->Cp, c->Ci, c->perm, c->ostart, s);
+        coalesce_bucket_build(c->ostart.get(), c->perm.get(), nnz_in, c->nout, c->buckets, s);
         *out = c.release();
     });
 }
@@ -287,7 +290,7 @@ extern "C" sdl_status sdl_coalesce_fill(const sdl_coalesce *C, const double *x, 
 {
     return guard_status("sdl_coalesce_fill", [&]() {
         if (!C) fail(SDL_ERR_INVALID, "NULL plan");
-        coalesce_order_fill(C->ostart.get(), C->perm.get(), x, nullptr, C->nout, Cx, pick_stream(stream));
+        coalesce_fill_scaled(C, x, nullptr, Cx, pick_stream(stream));
     });
 }
 
@@ -298,6 +301,9 @@ namespace sdl {
 // over its duplicates in ascending t, from +0.0 (d null: x[t]).
 void coalesce_fill_scaled(const sdl_coalesce *C, const double *x, const double *d, double *Cx, cudaStream_t s)
 {
-    coalesce_order_fill(C->ostart.get(), C->perm.get(), x, d, C->nout, Cx, s);
+    if (C->buckets.active())
+        coalesce_bucket_fill(C->buckets, C->ostart.get(), x, d, C->nout, Cx, s);
+    else
+        coalesce_order_fill(C->ostart.get(), C->perm.get(), x, d, C->nout, Cx, s);
 }
 } // namespace sdl

@@ -146,9 +146,35 @@ struct TransposePlan
 };
 void transpose_build(const int *d_p, const int *d_idx, int rows, int cols, int nnz,
                      TransposePlan &out, cudaStream_t s);
-// Tx[q] = x[src[q]].
+// Tx[q] = x[src[q]] for q < n, where x holds (at least) n values and src is a
+// permutation of [0, n) (every caller gathers through a transpose's or grouping's
+// source map); x may be pulled into L2 whole before the gather.
 void gather_values(const int *d_src, const double *d_x, double *d_out, int n,
                    cudaStream_t s);
+
+// ---------------------------------------------------------------- coalescing
+// Bucketed refill plan of a coalescing (coalesce.cu): for inputs of at least
+// COALESCE_BUCKET_MIN triplets the refill first writes the values, chunk by chunk,
+// into output-range buckets (lperm: each chunk's triplets in bucket order; cbound:
+// each bucket's first position in a chunk's order, nb + 1 per chunk; dst: start of
+// every (bucket, chunk) run in buf, bucket-major), then sums every output from its
+// bucket (perm2: the buf position of every output-order slot). buf is the plan's
+// refill scratch.
+constexpr int COALESCE_BUCKET_MIN = 1 << 22;
+struct CoalesceBuckets
+{
+    int n = 0, nb = 0, nchunks = 0;
+    DevBuf<unsigned short> lperm;
+    DevBuf<int> cbound, perm2;
+    DevBuf<long long> dst;
+    DevBuf<double> buf;
+    bool active() const { return nb > 0; }
+};
+void coalesce_bucket_build(const int *ostart, const int *perm, int n, int nout, CoalesceBuckets &B, cudaStream_t s);
+void coalesce_bucket_fill(const CoalesceBuckets &B, const int *ostart, const double *x, const double *f, int nout,
+                          double *C, cudaStream_t s);
+// dst[k] = src[k] (int -> long long), k < n.
+void widen_i32(const int *d_src, long long *d_dst, long long n, cudaStream_t s);
 
 // ---------------------------------------------------------------- Gustavson
 // Row classes of the row-wise product. Thresholds are tunable (autotuner).

@@ -269,6 +269,32 @@ def test_coalesce_bit_exact(sdl, orc, m, n, N):
     assert_same(got, orc.coalesce(rows, cols, x2, m, n))
 
 
+@pytest.mark.parametrize("m,n,N,neg_zero", [(2000, 2000, 5_000_000, True),     # ~3.7M outputs, many buckets
+                                             (300, 300, 4_500_000, False),       # 90k outputs, ~50 terms each
+                                             (100_000, 100_000, 4_194_304, True)])  # exactly the threshold
+def test_coalesce_bucketed_refill_bit_exact(sdl, orc, m, n, N, neg_zero):
+    """Inputs of at least 4Mi triplets take the bucketed refill (values first written
+    into output-range buckets, then summed per output from L2): the same bits as
+    the oracle, on the first fill and on a refill with new values."""
+    from oracle import parallel
+    rng = np.random.default_rng(N % 1000 + m)
+    rows = rng.integers(0, m, N).astype(np.int32)
+    cols = rng.integers(0, n, N).astype(np.int32)
+    x = rng.standard_normal(N)
+    if neg_zero:
+        x[::7] = -0.0
+    H = HostCOO(rows, cols, x, m, n)
+    Cm = sdl.COO_coalesce_alloc(H.ref)
+    assert Cm, sdl.sdl_last_error()
+    for rnd in range(2):
+        sdl.COO_coalesce_fill_values(H.ref, Cm)
+        got = csr_from_ptr(Cm)
+        want = parallel.coalesce(rows, cols, H.x.copy(), m, n)
+        assert_same(got, want)
+        H.x[...] = rng.standard_normal(N)
+    sdl.free_CSR_matrix(Cm)
+
+
 def test_fills_make_no_device_allocation(sdl):
     rng = np.random.default_rng(3)
     A = wl.small_random_csr(500, 400, 0.02, rng)

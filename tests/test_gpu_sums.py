@@ -97,6 +97,32 @@ def test_sum_two_and_scaled_match_upstream(libs):
             lib.free(*hs[name][::-1])
 
 
+def test_large_scaled_sum_matches_upstream(libs):
+    """A sum of two sparse operands with 4.5M entries together: its coalescing plan
+    takes the bucketed refill (factors applied while the values are bucketed)."""
+    mine, ref = libs
+    rng = np.random.default_rng(701)
+    m, n = 3000, 3000
+    specs = [sparse_spec(rng, m, n, 0.25), sparse_spec(rng, m, n, 0.25)]
+    hs = {}
+    for name, lib in (("mine", mine), ("ref", ref)):
+        A, B = lib.make(specs[0]), lib.make(specs[1])
+        S = lib.L.new_sparse_matrix_alloc(m, n, A.contents.nnz + B.contents.nnz)
+        lib.L.sum_matrices_alloc(A, B, S)
+        lib.L.sum_matrices_fill_values(A, B, S)
+        hs[name] = (A, B, S)
+    assert hs["mine"][0].contents.nnz + hs["mine"][1].contents.nnz >= 4_194_304
+    same(hs["mine"][2], hs["ref"][2], "large sum")
+    d1 = np.ascontiguousarray(rng.uniform(-2, 2, m))
+    d2 = np.ascontiguousarray(rng.uniform(-2, 2, m))
+    for name, lib in (("mine", mine), ("ref", ref)):
+        A, B, S = hs[name]
+        lib.L.sum_scaled_matrices_fill_values(A, B, S, d1.ctypes.data, d2.ctypes.data)
+    same(hs["mine"][2], hs["ref"][2], "large scaled sum")
+    for name, lib in (("mine", mine), ("ref", ref)):
+        lib.free(*hs[name][::-1])
+
+
 def test_sum_4_and_sum_n_match_upstream(libs):
     mine, ref = libs
     rng = np.random.default_rng(701)
