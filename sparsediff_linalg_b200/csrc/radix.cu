@@ -10,6 +10,9 @@
 // the tile is reordered by digit in shared memory before it is written out.
 #include <algorithm>
 
+#include <mutex>
+#include <unordered_set>
+
 #include "sdl_device.cuh"
 #include "sdl_internal.h"
 
@@ -125,12 +128,20 @@ void radix_sort_pairs(unsigned *keys, uint2 *vals, unsigned *keys_tmp, uint2 *va
                       cudaStream_t s)
 {
     if (n <= 1) return;
-    static bool attr_set = false; // set once, outside any capture
-    if (!attr_set)
     {
-        SDL_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)RS_SCATTER_SMEM));
-        attr_set = true;
+        // the kernel attribute is per device: set it once for each device the
+        // process sorts on (plans may be built from several host threads)
+        static std::mutex mu;
+        static std::unordered_set<int> done;
+        int dev = 0;
+        SDL_CUDA(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu);
+        if (!done.count(dev))
+        {
+            SDL_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)RS_SCATTER_SMEM));
+            done.insert(dev);
+        }
     }
     const int ntiles = (int)(((long long)n + RS_TILE - 1) / RS_TILE);
     if ((long long)ntiles * 256 > INT_MAX) fail(SDL_ERR_OVERFLOW, "radix sort: too many tiles");

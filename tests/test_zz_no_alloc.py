@@ -17,10 +17,10 @@ from sparsediff_linalg_b200 import workloads as wl
 pytestmark = pytest.mark.gpu
 
 
-def _operands(rng):
+def _operands(rng, nA=30000):
     """B^T D A whose output rows span the tile rows, the shared-accumulator rows and
     rows with more than 8192 outputs (the ones that use the scratch)."""
-    m, nA = 6000, 30000
+    m = 6000
     col_lens = [0, 1, 3, 8, 30, 100, 400, 1500, 3000, 6000] + [4] * 100
     ent = []
     for c, ln in enumerate(col_lens):
@@ -64,6 +64,37 @@ def test_noalloc_refill_matches_regular_fill(sdl):
         g = got.cpu().numpy().view(np.int64)
         assert np.array_equal(w, g), f"call {call}: values differ from sdl_product_fill"
     assert sdl.sdl_device_alloc_count() == allocs, "the refills must not allocate"
+
+
+def test_noalloc_products_of_different_widths_alternate(sdl):
+    """Two products whose A differ in width, refilled alternately through the shared
+    scratch: each call finds its rows' map slices as it needs them, whatever the
+    call before it left in the array."""
+    import torch
+    from sparsediff_linalg_b200.device import btda_product
+
+    rng = np.random.default_rng(2025)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
+    cases = []
+    for nA in (30000, 12000):
+        A, B = _operands(rng, nA)
+        P, Tr = btda_product(T(A[0]), T(A[1]), A[4], T(B[0]), T(B[1]), B[4])
+        assert np.diff(P.Cp.cpu().numpy()).max() > 8192
+        cases.append((A, B, P, Tr))
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream or 1)
+    for call in range(4):
+        A, B, P, _ = cases[call % 2]
+        ax = T(rng.standard_normal(len(A[1])))
+        bx = T(rng.standard_normal(len(B[1])))
+        d = T(rng.uniform(0.1, 10.0, A[3]))
+        want = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+        got = torch.full((P.nnz,), float("nan"), dtype=torch.float64, device="cuda")
+        P.fill(bx, d, ax, want)
+        st = sdl.sdl_product_fill_noalloc(P.handle, C.c_void_p(bx.data_ptr()), C.c_void_p(d.data_ptr()),
+                                          C.c_void_p(ax.data_ptr()), C.c_void_p(got.data_ptr()), stream)
+        assert st == 0, sdl.sdl_last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(want.cpu().numpy().view(np.int64), got.cpu().numpy().view(np.int64)), f"call {call}"
 
 
 def test_noalloc_rejects_products_beyond_the_scratch(sdl):
