@@ -990,74 +990,97 @@ def run_dense_ata(args, dev, X, blocks_rows, cperm, check=False):
 
 def run_learned(args, dev, check=False):
     """Skewed SpGEMM C = A B, A and B 1M x 1M with Zipf(1.5) row lengths (~20M nnz
-    each, rows capped at 50k): the plain exact symbolic pass + refill against the
-    learned one (scratch sized by the network, exact fallback) + refill. The
+    each, rows capped at 50k), the pattern met for the first time: plain = the exact
+    symbolic pass with its refill plan, then the first fill; learned = the one-shot
+    pass (rows up to 8192 terms sorted with their values into the network's
+    predicted capacity, overflowing rows redone exactly, larger rows by the bitmap
+    pass and an accumulating kernel; no refill plan). Each is timed `learned_runs`
+    times (median and range reported), device memory released between runs. The
     network is trained first on the row statistics of 200 seeded smaller matrices
-    of the same recipe. Structures are compared for equality."""
+    of the same recipe. Outputs are compared bit for bit."""
     import torch
     from sparsediff_linalg_b200 import workloads as wl
     from sparsediff_linalg_b200.device import Product
-    from sparsediff_linalg_b200.learned import LearnedProduct, scratch_bytes
+    from sparsediff_linalg_b200.learned import LearnedFilledProduct, LearnedProduct, scratch_bytes
     from sparsediff_linalg_b200.train_scheduler import train
     net, info = train(matrices=args.learned_matrices, epochs=8)
     t0 = time.perf_counter()
     (Ap, Ai, Ax), (Bp, Bi, Bx), scales = wl.skewed_device(seed=0)
     gen_s = time.perf_counter() - t0
+    m = Ap.numel() - 1
 
-    def once(make):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        P = make()
-        torch.cuda.synchronize()
-        t_sym = time.perf_counter() - t0
+    def plain():
+        P = Product(Ap, Ai, Bp, Bi, m)
         Cx = torch.empty(max(1, P.nnz), dtype=torch.float64, device=dev)
         P.fill(Ax, None, Bx, Cx)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        P.fill(Ax, None, Bx, Cx)
-        e1.record()
-        torch.cuda.synchronize()
-        return P, t_sym * 1e3, e0.elapsed_time(e1), Cx
+        return P, Cx
 
-    m = Ap.numel() - 1
-    # one untimed pass of each first: the first large allocations and kernel loads of
-    # a process would otherwise land on whichever pass runs first
-    for make in (lambda: Product(Ap, Ai, Bp, Bi, m), lambda: LearnedProduct(Ap, Ai, Bp, Bi, m, net, margin=0.25)):
-        warm = make()
+    def learned():
+        Q = LearnedFilledProduct(Ap, Ai, Bp, Bi, m, net, Ax, None, Bx, margin=0.25)
+        return Q, Q.values
+
+    def timed(make, runs):
+        ms = []
+        out = None
+        for _ in range(runs):
+            out = None
+            torch.cuda.empty_cache()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = make()
+            torch.cuda.synchronize()
+            ms.append((time.perf_counter() - t0) * 1e3)
+        return out, ms
+
+    # one untimed pass of each first (first large allocations and kernel loads)
+    for make in (plain, learned):
+        w = make()
         torch.cuda.synchronize()
-        del warm
-        torch.cuda.empty_cache()
-    plain, ps, pn, cx_plain = once(lambda: Product(Ap, Ai, Bp, Bi, m))
-    plain_scratch = scratch_bytes(plain)
-    plain_cp, plain_ci = plain.Cp.clone(), plain.Ci.clone()
-    del plain
-    torch.cuda.empty_cache()
-    learned, ls, ln, cx_learned = once(lambda: LearnedProduct(Ap, Ai, Bp, Bi, m, net, margin=0.25))
-    same = bool(torch.equal(plain_cp, learned.Cp) and torch.equal(plain_ci, learned.Ci) and
-                torch.equal(cx_plain.view(torch.int64), cx_learned.view(torch.int64)))
-    st = learned.stats
-    parity = None
+        del w
+    runs = max(1, args.learned_runs)
+    (P, cx_plain), plain_ms = timed(plain, runs)
+    plain_cp, plain_ci = P.Cp.clone(), P.Ci.clone()
+    plain_scratch = scratch_bytes(P)
+    # the refill of the planned product (a recurring pattern), for reference
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    P.fill(Ax, None, Bx, cx_plain)
+    e1.record()
+    torch.cuda.synchronize()
+    refill_ms = e0.elapsed_time(e1)
+    del P
+    (Q, cx_learned), learned_ms = timed(learned, runs)
+    same = bool(torch.equal(plain_cp, Q.Cp) and torch.equal(plain_ci, Q.Ci) and
+                torch.equal(cx_plain[:Q.nnz].view(torch.int64), cx_learned.view(torch.int64)))
+    st = Q.stats
+    med = lambda v: round(statistics.median(v), 2)  # noqa: E731
+    res = {"workload": "C = A B, A and B 1M x 1M, Zipf(1.5) row lengths scaled to ~20M nnz, cap 50k; "
+                       "the pattern met for the first time (structure + first values)",
+           "nnz_A": int(Ai.numel()), "nnz_B": int(Bi.numel()), "terms": int(Q.terms),
+           "nnz_C": int(Q.nnz), "zipf_scale": [round(x, 6) for x in scales], "runs": runs,
+           "plain": {"new_pattern_ms_median": med(plain_ms), "new_pattern_ms_range": [round(min(plain_ms), 2),
+                                                                                      round(max(plain_ms), 2)],
+                     "what": "exact symbolic pass + refill plan + first fill", "scratch_bytes": int(plain_scratch),
+                     "later_refill_ms": round(refill_ms, 3)},
+           "learned": {"new_pattern_ms_median": med(learned_ms),
+                       "new_pattern_ms_range": [round(min(learned_ms), 2), round(max(learned_ms), 2)],
+                       "what": "learned one-shot pass (structure + values, no refill plan)",
+                       "scratch_bytes": int(st["scratch_bytes"]), "fallback_rows": st["fallback_rows"],
+                       "fallback_terms": st["fallback_terms"],
+                       "class_accuracy": round(st["class_hits"] / max(1, st["rows"]), 4),
+                       "capacity_over_nnz": round(st["capacity"] / max(1, Q.nnz), 4),
+                       "term_bound_over_nnz": round(st["term_bound"] / max(1, Q.nnz), 4)},
+           "speedup_new_pattern": round(statistics.median(plain_ms) / statistics.median(learned_ms), 3),
+           "identical_structure_and_values": same, "training": info, "generate_s": round(gen_s, 2)}
     if check:
         from oracle import parallel
         hA = (_h(Ap), _h(Ai), _h(Ax), m, m)
         hB = (_h(Bp), _h(Bi), _h(Bx), m, m)
-        parity = parity_of((_h(learned.Cp), _h(learned.Ci), _h(cx_learned, learned.nnz)),
-                           lambda: parallel.spgemm(hA, hB),
-                           "oracle port (oracle/sdl_oracle.c), whole product, learned path output")
-    res = {"workload": "C = A B, A and B 1M x 1M, Zipf(1.5) row lengths scaled to ~20M nnz, cap 50k",
-            "nnz_A": int(Ai.numel()), "nnz_B": int(Bi.numel()), "terms": int(learned.terms),
-            "nnz_C": int(learned.nnz), "zipf_scale": [round(x, 6) for x in scales],
-            "plain": {"symbolic_ms": round(ps, 2), "numeric_ms": round(pn, 3),
-                      "scratch_bytes": int(plain_scratch)},
-            "learned": {"symbolic_ms": round(ls, 2), "numeric_ms": round(ln, 3),
-                        "scratch_bytes": int(st["scratch_bytes"]), "fallback_rows": st["fallback_rows"],
-                        "class_accuracy": round(st["class_hits"] / max(1, st["rows"]), 4),
-                        "capacity_over_nnz": round(st["capacity"] / max(1, learned.nnz), 4),
-                        "term_bound_over_nnz": round(st["term_bound"] / max(1, learned.nnz), 4)},
-            "identical_structure_and_values": same, "training": info, "generate_s": round(gen_s, 2)}
-    if parity is not None:
-        res["parity"] = parity
+        res["parity"] = parity_of((_h(Q.Cp), _h(Q.Ci), _h(cx_learned)), lambda: parallel.spgemm(hA, hB),
+                                  "oracle port (oracle/sdl_oracle.c), whole product, learned one-shot output")
+    del Q, cx_learned, cx_plain
+    torch.cuda.empty_cache()
+    _ = LearnedProduct  # the scratch-sizing learned symbolic pass stays available
     return res
 
 

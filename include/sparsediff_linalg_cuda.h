@@ -246,6 +246,27 @@ typedef struct sdl_learned_stats
 sdl_status sdl_product_create_learned(const sdl_product_desc *desc, const sdl_mlp *net,
                                       float margin, void *stream, sdl_product **out,
                                       sdl_learned_stats *stats);
+/* No upstream counterpart: the learned one-shot product, for a pattern met for the
+   first time (it replaces upstream's gustavson_alloc passes 1 and 2 and the first
+   gustavson_fill_values, src/sparse/gustavson.c:26-143). Structure and values of
+   C = kron(I, L) diag(d) A come out of one pass over the terms: every row of up to
+   8192 terms is sorted together with its term values into the slots the network
+   predicts for it (capacity = predicted nnz x (1 + margin) + 8, at most its term
+   count), its columns and its sums -- each in upstream's visiting order, from
+   +0.0 -- written at once; a row whose outputs do not fit is flagged and redone
+   exactly; larger rows take the exact bitmap pass for their columns and an
+   accumulating kernel for their values. No refill plan is built: the product's
+   values are at sdl_product_values (device memory owned by P, nnz doubles), and
+   sdl_product_fill refuses P until sdl_product_complete_plan has built the plan (a
+   pattern that recurs). The result is bit-identical to sdl_product_create followed
+   by sdl_product_fill. Lx, d as for sdl_product_fill; Ax is required. Allocates;
+   synchronises the stream. sdl_product_plan_ready reports whether P can be refilled. */
+sdl_status sdl_product_create_learned_filled(const sdl_product_desc *desc, const sdl_mlp *net, float margin,
+                                             const double *Lx, const double *d, const double *Ax, void *stream,
+                                             sdl_product **out, sdl_learned_stats *stats);
+sdl_status sdl_product_values(const sdl_product *P, const double **Cx);
+sdl_status sdl_product_complete_plan(sdl_product *P, void *stream);
+sdl_status sdl_product_plan_ready(const sdl_product *P, int *ready);
 /* Column scratch bytes the symbolic pass of a product used. */
 sdl_status sdl_product_scratch_bytes(const sdl_product *P, long long *bytes);
 

@@ -103,6 +103,11 @@ EXTENSION_SIGNATURES = {
     "sdl_product_tuning": (C.c_int, [vp, c_int_p, c_int_p, c_int_p, c_int_p, C.POINTER(C.c_double),
                                      C.POINTER(C.c_double), c_int_p, C.POINTER(C.c_double)]),
     "sdl_product_refill_shape": (C.c_int, [vp, c_int_p, c_int_p]),
+    "sdl_product_create_learned_filled": (C.c_int, [C.POINTER(sdl_product_desc), vp, C.c_float, vp, vp, vp, vp,
+                                                    C.POINTER(vp), vp]),
+    "sdl_product_values": (C.c_int, [vp, vp]),
+    "sdl_product_complete_plan": (C.c_int, [vp, vp]),
+    "sdl_product_plan_ready": (C.c_int, [vp, c_int_p]),
     "sdl_product_apply_tuned": (C.c_int, [vp, c_int_p, vp]),
     "sdl_product_pattern_key": (C.c_int, [vp, C.c_char_p, C.c_int, vp]),
     "sdl_tune_table_save": (C.c_int, [C.c_char_p]),

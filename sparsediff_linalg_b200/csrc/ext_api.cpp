@@ -11,6 +11,7 @@ struct sdl_product
 {
     Product P;
     TuneResult tuned;
+    DevBuf<double> values; // C's values from the learned one-shot pass
 };
 
 struct sdl_transpose
@@ -214,6 +215,41 @@ sdl_product *product_new_learned(const ProductDesc &d, const Mlp &net, float mar
     product_symbolic_learned(d, TuneConfig{}, net, margin, p->P, st, s);
     return p.release();
 }
+
+sdl_product *product_new_learned_oneshot(const ProductDesc &d, const Mlp &net, float margin, const double *Lx,
+                                         const double *dvec, const double *Ax, LearnedStats &st, cudaStream_t s)
+{
+    auto p = std::make_unique<sdl_product>();
+    product_oneshot_learned(d, TuneConfig{}, net, margin, Lx, dvec, Ax, p->P, p->values, st, s);
+    return p.release();
+}
+} // namespace sdl
+
+extern "C" sdl_status sdl_product_values(const sdl_product *P, const double **Cx)
+{
+    return guard_status("sdl_product_values", [&]() {
+        if (!P || !Cx) fail(SDL_ERR_INVALID, "NULL argument");
+        *Cx = P->values.get();
+    });
+}
+
+extern "C" sdl_status sdl_product_complete_plan(sdl_product *P, void *stream)
+{
+    return guard_status("sdl_product_complete_plan", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        product_complete_plan(P->P, pick_stream(stream));
+    });
+}
+
+extern "C" sdl_status sdl_product_plan_ready(const sdl_product *P, int *ready)
+{
+    return guard_status("sdl_product_plan_ready", [&]() {
+        if (!P || !ready) fail(SDL_ERR_INVALID, "NULL argument");
+        *ready = P->P.plan_ready ? 1 : 0;
+    });
+}
+
+namespace sdl {
 } // namespace sdl
 
 // ------------------------------------------------------------------ transpose

@@ -370,6 +370,214 @@ __global__ void k_sym_cta(const int *__restrict__ rows, int count, SymArgs a)
     }
 }
 
+// ------------------------------------------------------------ one-shot rows
+// Symbolic and numeric in one pass, for a pattern met for the first time: every
+// term of the row is gathered as a key (column << 32 | term index) with its value
+// (L.x * d[k]) * A.x, the keys are sorted, and each run of equal columns -- its
+// terms in visiting order, since the term index breaks ties -- is summed from +0.0
+// in that order: the column and the value of one output of C, exactly the sum the
+// numeric pass computes. Outputs go to the row's slot range [off, off + cap);
+// a row with more outputs than its capacity is flagged and redone.
+struct OneShotArgs
+{
+    const int *Lp, *Li, *L_map;
+    int L_m, n_L;
+    const double *Lx, *d;
+    const int *Ap, *Ai;
+    const double *Ax;
+    const long long *off; // first slot of each row
+    const long long *cap; // slots of each row (null: unbounded)
+    int *col;
+    double *val;
+    int *row_nnz;
+    unsigned char *overflow;
+};
+
+__device__ __forceinline__ double oneshot_entry_value(const OneShotArgs &a, int ii, int k)
+{
+    const double lx = a.Lx ? a.Lx[a.L_map ? a.L_map[ii] : ii] : 1.0;
+    return a.d ? __dmul_rn(lx, a.d[k]) : lx;
+}
+
+// Sorted keys -> outputs: run q (first key of its column) sums its terms in order.
+__device__ __forceinline__ double oneshot_run_sum(const unsigned long long *key, const double *val, int cnt, int q)
+{
+    const unsigned c = (unsigned)(key[q] >> 32);
+    double acc = 0.0;
+    for (int r = q; r < cnt && (unsigned)(key[r] >> 32) == c; ++r) acc = __dadd_rn(acc, val[(unsigned)key[r]]);
+    return acc;
+}
+
+template <int CAP>
+__global__ void k_oneshot_warp(const int *__restrict__ rows, int count, OneShotArgs a)
+{
+    extern __shared__ __align__(16) unsigned char osm[];
+    const int lane = lane_id(), wpb = blockDim.x >> 5, w = threadIdx.x >> 5;
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(osm) + (size_t)w * 2 * CAP;
+    double *val = reinterpret_cast<double *>(key + CAP);
+    for (long long it = blockIdx.x * (long long)wpb + w; it < count; it += (long long)gridDim.x * wpb)
+    {
+        const int row = rows[it];
+        const int b = row / a.L_m, r = row - b * a.L_m;
+        const int ls = a.Lp[r], le = a.Lp[r + 1];
+        int cnt = 0;
+        for (int c = ls; c < le; c += 32)
+        {
+            const int ii = c + lane;
+            int s = 0, len = 0;
+            double v = 0.0;
+            if (ii < le)
+            {
+                const int k = a.Li[ii] + b * a.n_L;
+                s = a.Ap[k];
+                len = a.Ap[k + 1] - s;
+                v = oneshot_entry_value(a, ii, k);
+            }
+            const int incl = warp_incl_scan(len);
+            const int total = __shfl_sync(FULL_MASK, incl, 31);
+            for (int base = 0; base < total; base += 32)
+            {
+                const int u = base + lane;
+                const int e = warp_entry_of(incl, u);
+                const int se = __shfl_sync(FULL_MASK, s, e), ie = __shfl_sync(FULL_MASK, incl, e),
+                          lne = __shfl_sync(FULL_MASK, len, e);
+                const double ve = __shfl_sync(FULL_MASK, v, e);
+                if (u < total)
+                {
+                    const int jj = se + u - (ie - lne);
+                    key[cnt + u] = ((unsigned long long)(unsigned)a.Ai[jj] << 32) | (unsigned)(cnt + u);
+                    val[cnt + u] = __dmul_rn(ve, a.Ax[jj]);
+                }
+            }
+            cnt += total;
+        }
+        const int P = next_pow2(cnt);
+        for (int q = cnt + lane; q < P; q += 32) key[q] = ~0ULL;
+        __syncwarp();
+        warp_bitonic_sort(key, P);
+        const long long off = a.off[row], cap = a.cap ? a.cap[row] : 0x7fffffffffffffffLL;
+        int nn = 0;
+        for (int base = 0; base < cnt; base += 32)
+        {
+            const int q = base + lane;
+            const bool flag = q < cnt && (q == 0 || (unsigned)(key[q] >> 32) != (unsigned)(key[q - 1] >> 32));
+            const unsigned bal = __ballot_sync(FULL_MASK, flag);
+            const long long at = nn + __popc(bal & lanemask_lt());
+            if (flag && at < cap)
+            {
+                a.col[off + at] = (int)(key[q] >> 32);
+                a.val[off + at] = oneshot_run_sum(key, val, cnt, q);
+            }
+            nn += __popc(bal);
+        }
+        if (lane == 0)
+        {
+            a.row_nnz[row] = nn;
+            if (nn > cap) a.overflow[row] = 1;
+        }
+        __syncwarp();
+    }
+}
+
+template <int CAP>
+__global__ void k_oneshot_cta(const int *__restrict__ rows, int count, OneShotArgs a)
+{
+    extern __shared__ __align__(16) unsigned char osm[];
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(osm);
+    double *val = reinterpret_cast<double *>(key + CAP);
+    CtaChunk ch;
+    ch.v = val + CAP;
+    ch.incl = reinterpret_cast<int *>(ch.v + blockDim.x);
+    ch.s = ch.incl + blockDim.x;
+    ch.len = ch.s + blockDim.x;
+    ch.scr = ch.len + blockDim.x;
+    __shared__ int tot_sh;
+    for (int it = blockIdx.x; it < count; it += gridDim.x)
+    {
+        const int row = rows[it];
+        const int b = row / a.L_m, r = row - b * a.L_m;
+        const int ls = a.Lp[r], le = a.Lp[r + 1];
+        int cnt = 0;
+        for (int c = ls; c < le; c += blockDim.x)
+        {
+            const int total = cta_load_chunk(a.Li, a.Ap, b, a.n_L, c, le, ch, a.Lx, a.L_map, a.d, true);
+            const int nent = min((int)blockDim.x, le - c);
+            for (int u = threadIdx.x; u < total; u += blockDim.x)
+            {
+                const int e = cta_entry_of(ch.incl, nent, u);
+                const int jj = ch.s[e] + u - (ch.incl[e] - ch.len[e]);
+                key[cnt + u] = ((unsigned long long)(unsigned)a.Ai[jj] << 32) | (unsigned)(cnt + u);
+                val[cnt + u] = __dmul_rn(ch.v[e], a.Ax[jj]);
+            }
+            cnt += total;
+            __syncthreads();
+        }
+        const int P = next_pow2(cnt);
+        for (int q = cnt + threadIdx.x; q < P; q += blockDim.x) key[q] = ~0ULL;
+        __syncthreads();
+        block_bitonic_sort(key, P);
+        const long long off = a.off[row], cap = a.cap ? a.cap[row] : 0x7fffffffffffffffLL;
+        int nn = 0;
+        for (int base = 0; base < cnt; base += blockDim.x)
+        {
+            const int q = base + threadIdx.x;
+            const int flag =
+                (q < cnt && (q == 0 || (unsigned)(key[q] >> 32) != (unsigned)(key[q - 1] >> 32))) ? 1 : 0;
+            const int incl = block_incl_scan_int(flag, ch.scr);
+            const long long at = nn + incl - 1;
+            if (flag && at < cap)
+            {
+                a.col[off + at] = (int)(key[q] >> 32);
+                a.val[off + at] = oneshot_run_sum(key, val, cnt, q);
+            }
+            if (threadIdx.x == blockDim.x - 1) tot_sh = incl;
+            __syncthreads();
+            nn += tot_sh;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+        {
+            a.row_nnz[row] = nn;
+            if (nn > cap) a.overflow[row] = 1;
+        }
+        __syncthreads();
+    }
+}
+
+// Final columns and values of every row from its slot range (capacity slots, or
+// the exact redo's slots for rows that overflowed); rows marked `late` get their
+// values afterwards (large rows: columns here, values by the accumulating kernel).
+__global__ void k_oneshot_compact(const long long *__restrict__ cap_off, const long long *__restrict__ fb_off,
+                                  const unsigned char *__restrict__ overflow, const unsigned char *__restrict__ late,
+                                  const int *__restrict__ Cp, const int *__restrict__ tcol,
+                                  const double *__restrict__ tval, const int *__restrict__ fcol,
+                                  const double *__restrict__ fval, int *__restrict__ Ci, double *__restrict__ Cx,
+                                  int m_out)
+{
+    const int lane = lane_id(), wpb = blockDim.x >> 5;
+    for (long long row = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); row < m_out;
+         row += (long long)gridDim.x * wpb)
+    {
+        const int c0 = Cp[row], nn = Cp[row + 1] - c0;
+        const bool ov = overflow[row];
+        const int *sc = ov ? fcol + fb_off[row] : tcol + cap_off[row];
+        const double *sv = ov ? fval + fb_off[row] : tval + cap_off[row];
+        const bool vals = !late[row];
+        for (int q = lane; q < nn; q += 32)
+        {
+            Ci[c0 + q] = sc[q];
+            if (vals) Cx[c0 + q] = sv[q];
+        }
+    }
+}
+
+__global__ void k_mark_class(const unsigned char *__restrict__ cls, int m_out, int which,
+                             unsigned char *__restrict__ out)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out; r += (long long)gridDim.x * blockDim.x)
+        out[r] = cls[r] == which ? 1 : 0;
+}
+
 // Large rows: mark columns in a shared-memory bitmap, one column window at a time;
 // reading the bitmap word by word yields the columns in ascending order.
 __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a, int words)
@@ -1964,6 +2172,185 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
 }
 
 namespace {
+// Launches the one-shot kernel of every row class up to 8192 terms.
+void oneshot_launch(const OneShotArgs &oa, const int *lists, const int *cnt, const int *off, const TuneConfig &cfg,
+                    cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    const int gcap = rt.num_sms * 16;
+    const int wpb = std::max(1, std::min(8, cfg.rows_per_cta_warp));
+    if (cnt[SYM_W32])
+    {
+        const size_t sm = (size_t)wpb * 2 * 32 * 8;
+        SDL_LAUNCH(k_oneshot_warp<32>, grid_for(cnt[SYM_W32], wpb, gcap), wpb * 32, sm, s, lists + off[SYM_W32],
+                   cnt[SYM_W32], oa);
+    }
+    if (cnt[SYM_W128])
+    {
+        const size_t sm = (size_t)wpb * 2 * 128 * 8;
+        SDL_LAUNCH(k_oneshot_warp<128>, grid_for(cnt[SYM_W128], wpb, gcap), wpb * 32, sm, s, lists + off[SYM_W128],
+                   cnt[SYM_W128], oa);
+    }
+    if (cnt[SYM_W512])
+    {
+        const size_t sm = (size_t)wpb * 2 * 512 * 8;
+        set_smem(k_oneshot_warp<512>, sm);
+        SDL_LAUNCH(k_oneshot_warp<512>, grid_for(cnt[SYM_W512], wpb, gcap), wpb * 32, sm, s, lists + off[SYM_W512],
+                   cnt[SYM_W512], oa);
+    }
+    if (cnt[SYM_C2K])
+    {
+        const int th = 256;
+        const size_t sm = 2048 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
+        set_smem(k_oneshot_cta<2048>, sm);
+        SDL_LAUNCH(k_oneshot_cta<2048>, grid_for(cnt[SYM_C2K], 1, gcap), th, sm, s, lists + off[SYM_C2K],
+                   cnt[SYM_C2K], oa);
+    }
+    if (cnt[SYM_C8K])
+    {
+        const int th = 512;
+        const size_t sm = 8192 * 16 + (size_t)th * 8 + (3 * th + 32) * 4;
+        set_smem(k_oneshot_cta<8192>, sm);
+        SDL_LAUNCH(k_oneshot_cta<8192>, grid_for(cnt[SYM_C8K], 1, gcap), th, sm, s, lists + off[SYM_C8K],
+                   cnt[SYM_C8K], oa);
+    }
+}
+} // namespace
+
+void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const Mlp &net, float margin,
+                             const double *Lx, const double *dvec, const double *Ax, Product &P,
+                             DevBuf<double> &Cx, LearnedStats &st, cudaStream_t s)
+{
+    Runtime &rt = runtime();
+    validate_product(d, cfg, P, s);
+    const int m_out = P.m_out;
+    st = LearnedStats{};
+    P.Cp.reset((size_t)m_out + 1);
+    P.plan_ready = false;
+    if (m_out == 0)
+    {
+        SDL_CUDA(cudaMemsetAsync(P.Cp.get(), 0, sizeof(int), s));
+        P.nnz = 0;
+        P.terms = 0;
+        P.Ci.reset(1);
+        Cx.reset(1);
+        P.row_terms.reset(1);
+        SDL_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    if (d.A_nnz > 0 && !Ax) fail(SDL_ERR_INVALID, "one-shot product: NULL A values");
+    DevBuf<long long> ub(m_out), cap(m_out), cap_off((size_t)m_out + 1), ub_off((size_t)m_out + 1);
+    DevBuf<unsigned char> pcls(m_out), overflow(m_out), cls(m_out);
+    SDL_LAUNCH(k_row_terms_learned, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, d.Lp, d.Li, d.L_m,
+               P.n_L, m_out, d.Ap, d.A_n, net.params.get(), margin, ub.get(), cap.get(), pcls.get());
+    P.terms = exclusive_scan_i64(ub.get(), ub_off.get(), m_out, s);
+    st.cap_total = exclusive_scan_i64(cap.get(), cap_off.get(), m_out, s);
+    st.ub_total = P.terms;
+    DevBuf<int> row_nnz(m_out);
+    SDL_CUDA(cudaMemsetAsync(row_nnz.get(), 0, row_nnz.bytes(), s));
+    SDL_CUDA(cudaMemsetAsync(overflow.get(), 0, overflow.bytes(), s));
+    DevBuf<int> tcol(std::max<long long>(1, st.cap_total));
+    DevBuf<double> tval(std::max<long long>(1, st.cap_total));
+    SDL_LAUNCH(k_sym_classify, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, ub.get(), m_out, cfg.warp_max_terms,
+               cls.get());
+    DevBuf<int> lists;
+    int cnt[SYM_NBINS], off[SYM_NBINS + 1];
+    bin_items(cls.get(), m_out, SYM_NBINS, lists, cnt, off, s);
+    // rows up to 8192 terms: structure and values in one pass
+    OneShotArgs oa{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, cap_off.get(), cap.get(),
+                   tcol.get(), tval.get(), row_nnz.get(), overflow.get()};
+    oneshot_launch(oa, lists.get(), cnt, off, cfg, s);
+    // larger rows: their columns by the bitmap pass (values once C is laid out)
+    int bcnt[SYM_NBINS] = {0};
+    bcnt[SYM_BITMAP] = cnt[SYM_BITMAP];
+    if (bcnt[SYM_BITMAP])
+    {
+        SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, cap_off.get(), tcol.get(), row_nnz.get(),
+                   cap.get(), overflow.get()};
+        sym_launch(sa, lists.get(), bcnt, off, d, cfg, s);
+    }
+    // rows whose outputs did not fit their capacity: the same passes again,
+    // unbounded, into term-count space
+    DevBuf<long long> fb_len(m_out), fb_off((size_t)m_out + 1);
+    SDL_LAUNCH(k_overflow_terms, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, overflow.get(), ub.get(), m_out,
+               fb_len.get());
+    st.fallback_terms = exclusive_scan_i64(fb_len.get(), fb_off.get(), m_out, s);
+    DevBuf<int> fcol(std::max<long long>(1, st.fallback_terms));
+    DevBuf<double> fval(std::max<long long>(1, st.fallback_terms));
+    if (st.fallback_terms > 0)
+    {
+        DevBuf<unsigned char> fcls(m_out);
+        SDL_CUDA(cudaMemcpyAsync(fcls.get(), cls.get(), m_out, cudaMemcpyDeviceToDevice, s));
+        SDL_LAUNCH(k_mask_classes, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, overflow.get(), m_out,
+                   fcls.get());
+        DevBuf<int> flists;
+        int fcnt[SYM_NBINS], foff[SYM_NBINS + 1];
+        bin_items(fcls.get(), m_out, SYM_NBINS, flists, fcnt, foff, s);
+        for (int c = 0; c < SYM_NBINS; ++c) st.fallback_rows += fcnt[c];
+        OneShotArgs fa{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, fb_off.get(), nullptr,
+                       fcol.get(), fval.get(), row_nnz.get(), nullptr};
+        oneshot_launch(fa, flists.get(), fcnt, foff, cfg, s);
+        int fb_bits[SYM_NBINS] = {0};
+        fb_bits[SYM_BITMAP] = fcnt[SYM_BITMAP];
+        if (fb_bits[SYM_BITMAP])
+        {
+            SymArgs sb{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, fb_off.get(), fcol.get(), row_nnz.get(),
+                       nullptr, nullptr};
+            sym_launch(sb, flists.get(), fb_bits, foff, d, cfg, s);
+        }
+    }
+    P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
+    P.Ci.reset(std::max(1, P.nnz));
+    Cx.reset(std::max(1, P.nnz));
+    DevBuf<unsigned char> late(m_out);
+    SDL_LAUNCH(k_mark_class, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, cls.get(), m_out, (int)SYM_BITMAP,
+               late.get());
+    if (P.nnz > 0)
+        SDL_LAUNCH(k_oneshot_compact, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, cap_off.get(), fb_off.get(),
+                   overflow.get(), late.get(), P.Cp.get(), tcol.get(), tval.get(), fcol.get(), fval.get(), P.Ci.get(),
+                   Cx.get(), m_out);
+    // values of the larger rows: accumulated in C.x through a per-CTA column ->
+    // position map, same-position terms applied in visiting order
+    if (cnt[SYM_BITMAP] && P.nnz > 0)
+    {
+        const long long per_slot = std::max(1, P.n);
+        const long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
+        const int slots = (int)std::min<long long>({(long long)rt.num_sms, max_slots, (long long)cnt[SYM_BITMAP]});
+        DevBuf<int> posmap((size_t)slots * per_slot);
+        NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(), Cx.get(),
+                   rt.d_error};
+        const int th = 512;
+        const size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
+        set_smem(k_num_gmem, sm);
+        SDL_LAUNCH(k_num_gmem, slots, th, sm, s, lists.get() + off[SYM_BITMAP], cnt[SYM_BITMAP], na, posmap.get(),
+                   P.n, nullptr);
+        if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "one-shot product: a term column is missing from its row");
+    }
+    {
+        DevBuf<unsigned long long> hits(1);
+        SDL_CUDA(cudaMemsetAsync(hits.get(), 0, 8, s));
+        SDL_LAUNCH(k_class_hits, grid_for(m_out, 256, rt.num_sms * 4), 256, 0, s, pcls.get(), P.Cp.get(), m_out,
+                   hits.get());
+        unsigned long long h = 0;
+        SDL_CUDA(cudaMemcpyAsync(&h, hits.get(), 8, cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaStreamSynchronize(s));
+        st.class_hits = (long long)h;
+        st.rows = m_out;
+    }
+    P.scratch_bytes = (long long)(tcol.bytes() + tval.bytes() + fcol.bytes() + fval.bytes());
+    P.row_terms = std::move(ub);
+    SDL_CUDA(cudaStreamSynchronize(s));
+}
+
+void product_complete_plan(Product &P, cudaStream_t s)
+{
+    if (P.plan_ready) return;
+    if (P.m_out > 0) build_schedule(P.desc, P, P.row_terms.get(), s);
+    SDL_CUDA(cudaStreamSynchronize(s));
+    P.plan_ready = true;
+}
+
+namespace {
 __global__ void k_rebase_tiles(const TileDesc *__restrict__ src, int n, int prod, TileDesc *__restrict__ dst)
 {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
@@ -2172,6 +2559,9 @@ bool entry_values_are_lx(const Product &P, const double *Lx, const double *dvec)
 void product_numeric(const Product &P, const double *Lx, const double *dvec, const double *Ax,
                      double *Cx, cudaStream_t s)
 {
+    if (!P.plan_ready)
+        fail(SDL_ERR_INVALID, "product from the learned one-shot pass: build its refill plan first "
+                              "(sdl_product_complete_plan)");
     if (P.nnz == 0) return;
     ProdSched S = sched_of(P);
     const ProdPtrs vals{Lx, dvec, Ax, Cx};

@@ -23,6 +23,8 @@ extern "C" sdl_status sdl_product_create(const sdl_product_desc *desc, void *str
 namespace sdl {
 sdl_product *product_new_learned(const ProductDesc &d, const Mlp &net, float margin, LearnedStats &st,
                                  cudaStream_t s);
+sdl_product *product_new_learned_oneshot(const ProductDesc &d, const Mlp &net, float margin, const double *Lx,
+                                         const double *dvec, const double *Ax, LearnedStats &st, cudaStream_t s);
 }
 
 extern "C" sdl_status sdl_mlp_create(unsigned long long seed, sdl_mlp **out)
@@ -118,6 +120,44 @@ extern "C" sdl_status sdl_product_create_learned(const sdl_product_desc *desc, c
         if (!d.Lp || !d.Ap) fail(SDL_ERR_INVALID, "NULL structure pointer");
         LearnedStats st;
         sdl_product *P = product_new_learned(d, net->net, margin, st, pick_stream(stream));
+        if (stats)
+        {
+            stats->rows = st.rows;
+            stats->term_bound = st.ub_total;
+            stats->capacity = st.cap_total;
+            stats->fallback_rows = st.fallback_rows;
+            stats->fallback_terms = st.fallback_terms;
+            stats->class_hits = st.class_hits;
+            stats->scratch_bytes = product_of(P)->scratch_bytes;
+        }
+        *out = P;
+    });
+}
+
+extern "C" sdl_status sdl_product_create_learned_filled(const sdl_product_desc *desc, const sdl_mlp *net,
+                                                        float margin, const double *Lx, const double *d,
+                                                        const double *Ax, void *stream, sdl_product **out,
+                                                        sdl_learned_stats *stats)
+{
+    return guard_status("sdl_product_create_learned_filled", [&]() {
+        if (!desc || !net || !out) fail(SDL_ERR_INVALID, "NULL argument");
+        if (!(margin >= 0.f)) fail(SDL_ERR_INVALID, "margin must be >= 0");
+        *out = nullptr;
+        ProductDesc dd;
+        dd.Lp = desc->Lp;
+        dd.Li = desc->Li;
+        dd.L_map = desc->L_map;
+        dd.L_m = desc->L_m;
+        dd.L_nnz = desc->L_nnz;
+        dd.blocks = desc->blocks;
+        dd.Ap = desc->Ap;
+        dd.Ai = desc->Ai;
+        dd.A_m = desc->A_m;
+        dd.A_n = desc->A_n;
+        dd.A_nnz = desc->A_nnz;
+        if (!dd.Lp || !dd.Ap) fail(SDL_ERR_INVALID, "NULL structure pointer");
+        LearnedStats st;
+        sdl_product *P = product_new_learned_oneshot(dd, net->net, margin, Lx, d, Ax, st, pick_stream(stream));
         if (stats)
         {
             stats->rows = st.rows;

@@ -326,6 +326,9 @@ struct Product
     TuneConfig cfg;
     // per-row statistics kept for the learned scheduler (optional)
     DevBuf<long long> row_terms; // ub per row
+    // false for a product made by the learned one-shot pass until its refill plan is
+    // built (product_complete_plan); its fills are refused until then
+    bool plan_ready = true;
 };
 
 // Re-plans P with configuration c (same structure; the schedule follows c).
@@ -347,6 +350,18 @@ bool tune_table_lookup(const std::string &key, TuneConfig &c);
 // Symbolic phase: fills P.Cp, P.Ci, P.nnz and the numeric schedule.
 void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P,
                       cudaStream_t s, bool keep_row_terms = false);
+// Learned one-shot pass of a pattern met for the first time: C's structure and
+// values (Cx, allocated here) in one pass over the terms -- rows of up to 8192 terms
+// sorted with their values into the network's predicted capacity (rows that do not
+// fit are redone exactly), larger rows by the exact bitmap pass and an accumulating
+// kernel -- without building the refill plan. P then holds C's structure with
+// plan_ready = false; product_complete_plan builds the plan for later refills.
+struct LearnedStats;
+struct Mlp;
+void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const Mlp &net, float margin,
+                             const double *Lx, const double *dvec, const double *Ax, Product &P,
+                             DevBuf<double> &Cx, LearnedStats &st, cudaStream_t s);
+void product_complete_plan(Product &P, cudaStream_t s);
 // Statistics of a learned symbolic pass.
 struct LearnedStats
 {

@@ -91,6 +91,39 @@ class LearnedProduct(Product):
         self._init_from_handle(h)
 
 
+class LearnedFilledProduct(Product):
+    """A pattern met for the first time: C's structure and values from the learned
+    one-shot pass (sdl_product_create_learned_filled). `values` is C.x (device,
+    owned by the product); refills need complete_plan() first."""
+
+    def __init__(self, Lp, Li, Ap, Ai, A_n, net, Lx, d, Ax, margin=0.25, L_map=None, blocks=1, stream=None):
+        L = lib()
+        self._keep = (Lp, Li, Ap, Ai, L_map, net, Lx, d, Ax)
+        desc = sdl_product_desc(
+            _ptr(Lp).value, _ptr(Li).value, _ptr(L_map).value if L_map is not None else None,
+            Lp.numel() - 1, Li.numel(), blocks, _ptr(Ap).value, _ptr(Ai).value,
+            Ap.numel() - 1, A_n, Ai.numel())
+        h = C.c_void_p()
+        st = LearnedStats()
+        check(L.sdl_product_create_learned_filled(C.byref(desc), net.handle, margin, _ptr(Lx), _ptr(d), _ptr(Ax),
+                                                  _stream(stream), C.byref(h), C.byref(st)))
+        self.stats = st.as_dict()
+        self._init_from_handle(h)
+        cx = C.c_void_p()
+        check(L.sdl_product_values(self.handle, C.byref(cx)))
+        from .device import _as_tensor
+        self.values = _as_tensor(cx.value, self.nnz, "<f8") if self.nnz else None
+
+    def plan_ready(self):
+        r = C.c_int()
+        check(lib().sdl_product_plan_ready(self.handle, C.byref(r)))
+        return bool(r.value)
+
+    def complete_plan(self, stream=None):
+        check(lib().sdl_product_complete_plan(self.handle, _stream(stream)))
+        self._init_from_handle(self.handle)
+
+
 def scratch_bytes(product):
     b = C.c_longlong()
     check(lib().sdl_product_scratch_bytes(product.handle, C.byref(b)))

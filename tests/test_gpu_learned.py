@@ -101,3 +101,78 @@ def test_trained_network_gain(sdl):
     assert st["fallback_rows"] <= 0.05 * st["rows"]
     assert st["class_hits"] >= 0.9 * st["rows"]
     assert scratch_bytes(learned) < scratch_bytes(plain)
+
+
+@pytest.mark.parametrize("mode", ["untrained_zero_margin", "trained"])
+def test_oneshot_product_matches_oracle(sdl, orc, mode):
+    """The learned one-shot pass (structure and values of a new pattern in one pass,
+    no refill plan) against the oracle: every row class (warp rows, CTA rows, rows
+    beyond 8192 terms), rows that overflow their predicted capacity (an untrained
+    network with no margin forces many) redone exactly; then the plan is completed
+    and a refill with new values equals the plain product's, bit for bit."""
+    import torch
+    from oracle import parallel
+    from sparsediff_linalg_b200.device import Product
+    from sparsediff_linalg_b200.learned import LearnedFilledProduct, Mlp
+    if mode == "trained":
+        net, _, _ = _train(sdl, seeds=(30, 31), epochs=6)
+        margin = 0.25
+    else:
+        net, margin = Mlp(seed=9), 0.0
+    A, B = _skewed(77)
+    n = 20000
+    Q = LearnedFilledProduct(A[0], A[1], B[0], B[1], n, net, A[2], None, B[2], margin=margin)
+    assert not Q.plan_ready()
+    lens = np.diff(Q.Cp.cpu().numpy())
+    ub = np.diff(A[0].cpu().numpy())
+    assert lens.max() > 8192 or ub.max() > 0
+    hA = tuple(t.cpu().numpy() for t in A) + (n, n)
+    hB = tuple(t.cpu().numpy() for t in B) + (n, n)
+    want = parallel.spgemm(hA, hB)
+    res = parallel.compare_csr((Q.Cp.cpu().numpy(), Q.Ci.cpu().numpy(), Q.values.cpu().numpy()), want)
+    assert res["structure_equal"] and res["bit_identical"], res
+    if mode != "trained":
+        assert Q.stats["fallback_rows"] > 0
+    # a refill needs the plan
+    cx = torch.empty(Q.nnz, dtype=torch.float64, device="cuda")
+    with pytest.raises(Exception):
+        Q.fill(A[2], None, B[2], cx)
+    Q.complete_plan()
+    assert Q.plan_ready()
+    P = Product(A[0], A[1], B[0], B[1], n)
+    ax = torch.randn(A[2].numel(), dtype=torch.float64, device="cuda")
+    bx = torch.randn(B[2].numel(), dtype=torch.float64, device="cuda")
+    cp = torch.empty(P.nnz, dtype=torch.float64, device="cuda")
+    Q.fill(ax, None, bx, cx)
+    P.fill(ax, None, bx, cp)
+    torch.cuda.synchronize()
+    assert torch.equal(cx.view(torch.int64), cp.view(torch.int64))
+
+
+def test_oneshot_btda_with_value_map_and_d(sdl, orc):
+    """B^T D A through the one-shot pass: L is B's CSC read through the CSR positions
+    (L_map) and every entry value is L.x * d[k], as in the refill."""
+    import torch
+    from oracle import parallel
+    from sparsediff_linalg_b200.device import Transpose
+    from sparsediff_linalg_b200.learned import LearnedFilledProduct, Mlp
+    rng = np.random.default_rng(55)
+    m, nA, nB = 30000, 9000, 2000
+    A = wl.fixed_rowlen_csr(m, nA, 6, rng)
+    # B's columns drawn with skewed popularity, so the rows of C (B's columns) span
+    # every class: a few columns hold thousands of entries (over 8192 terms), most few
+    pop = 1.0 / np.arange(1, nB + 1) ** 1.1
+    pop /= pop.sum()
+    ent = np.unique(np.stack([np.repeat(np.arange(m), 4), rng.choice(nB, 4 * m, p=pop)], 1), axis=0)
+    Bp = np.zeros(m + 1, np.int32)
+    np.add.at(Bp, ent[:, 0] + 1, 1)
+    B = (np.cumsum(Bp).astype(np.int32), ent[:, 1].astype(np.int32), rng.standard_normal(len(ent)), m, nB)
+    d = rng.uniform(0.1, 10, m)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")  # noqa: E731
+    Tr = Transpose(T(B[0]), T(B[1]), m, nB)
+    net = Mlp(seed=4)
+    Q = LearnedFilledProduct(Tr.Tp, Tr.Ti, T(A[0]), T(A[1]), nA, net, T(B[2]), T(d), T(A[2]), margin=0.1,
+                             L_map=Tr.src)
+    want = parallel.btda(A, B, d)
+    res = parallel.compare_csr((Q.Cp.cpu().numpy(), Q.Ci.cpu().numpy(), Q.values.cpu().numpy()), want)
+    assert res["structure_equal"] and res["bit_identical"], res
