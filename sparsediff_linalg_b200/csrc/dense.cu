@@ -12,7 +12,6 @@
 // build has none). The kernel is bound by the writes of C.
 #include <algorithm>
 #include <climits>
-#include <cstdint>
 #include <map>
 
 #include "capi_common.h"
@@ -118,196 +117,6 @@ __global__ void __launch_bounds__(BC_THREADS) k_blocks_csr(const BlkTile *__rest
         }
         __syncthreads();
     }
-}
-
-// ---- shared-memory-staged variant
-// Persistent CTAs (one per SM), each over a contiguous range of the tiles (tiles
-// are ordered by block, so a CTA meets one or two blocks). The transposed source
-// block (m0 x n0_B values, up to BCS_BT_MAX bytes) is bulk-copied into shared
-// memory once per block met (cp.async.bulk completing on an mbarrier), so every
-// term reads its block column from shared memory instead of L1/L2; each tile's
-// compact-CSC entries and column offsets are copied into shared memory one tile
-// ahead (cp.async), so the term loops never wait on global loads. Sums and their
-// order are those of k_blocks_csr: bit-identical.
-constexpr int BCS_THREADS = 512;
-constexpr int BCS_ENT = 2048;                   // entries of a tile staged ahead
-constexpr size_t BCS_BT_MAX = 144u << 10;       // largest staged source block (bytes)
-constexpr long long BCS_WAIT_LIMIT = 1LL << 26; // mbarrier polls before giving up
-
-struct BcsStage
-{
-    int cp[BC_COLS + 1];
-    int rows[BCS_ENT];
-    double vals[BCS_ENT];
-};
-
-__host__ __device__ constexpr size_t bcs_smem_bytes(long long bt_vals)
-{
-    return (size_t)bt_vals * 8 + sizeof(double) * BC_ROWS * (BC_COLS + 1) + 2 * sizeof(BcsStage) + 16;
-}
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void cp_async4(void *dst, const void *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src));
-}
-
-// Copies tile t's column offsets and (when they fit) entries into stage st.
-__device__ __forceinline__ void bcs_prefetch(BcsStage &st, const BlkTile &t, const BlkDesc &D,
-                                             const int *__restrict__ cp_all, const int *__restrict__ rows_all,
-                                             const double *__restrict__ vals_all)
-{
-    const int ncol = min(BC_COLS, D.n0_C - t.c0);
-    for (int i = threadIdx.x; i <= ncol; i += BCS_THREADS) cp_async4(&st.cp[i], cp_all + D.cp_off + t.c0 + i);
-    const int n = t.d1 - t.d0;
-    if (n <= BCS_ENT)
-        for (int i = threadIdx.x; i < n; i += BCS_THREADS)
-        {
-            cp_async4(&st.rows[i], rows_all + D.d_off + t.d0 + i);
-            cp_async8(&st.vals[i], vals_all + D.d_off + t.d0 + i);
-        }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-}
-
-__global__ void __launch_bounds__(BCS_THREADS, 1) k_blocks_csr_smem(const BlkTile *__restrict__ tiles, int ntiles,
-                                                                    const BlkDesc *__restrict__ descs,
-                                                                    const int *__restrict__ cp_all,
-                                                                    const int *__restrict__ rows_all,
-                                                                    const double *__restrict__ vals_all,
-                                                                    const double *__restrict__ BT_vals,
-                                                                    double *__restrict__ C_vals, long long bt_cap,
-                                                                    int *__restrict__ err)
-{
-    extern __shared__ __align__(128) unsigned char bcs_sm[];
-    double *bt = reinterpret_cast<double *>(bcs_sm);
-    double(*tile)[BC_COLS + 1] = reinterpret_cast<double(*)[BC_COLS + 1]>(bcs_sm + bt_cap * 8);
-    BcsStage *stage = reinterpret_cast<BcsStage *>(bcs_sm + bt_cap * 8 + sizeof(double) * BC_ROWS * (BC_COLS + 1));
-    __shared__ __align__(8) unsigned long long mbar;
-    __shared__ int abort_flag;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long t_begin = (long long)ntiles * blockIdx.x / gridDim.x;
-    const long long t_end = (long long)ntiles * (blockIdx.x + 1) / gridDim.x;
-    if (threadIdx.x == 0)
-    {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        abort_flag = 0;
-    }
-    __syncthreads();
-    if (t_begin >= t_end) return;
-    unsigned phase = 0;
-    int cur = -1;
-    {
-        const BlkTile t0 = tiles[t_begin];
-        bcs_prefetch(stage[0], t0, descs[t0.blk], cp_all, rows_all, vals_all);
-    }
-    for (long long tt = t_begin; tt < t_end; ++tt)
-    {
-        const int sb = (int)((tt - t_begin) & 1);
-        const BlkTile t = tiles[tt];
-        const BlkDesc D = descs[t.blk];
-        if (tt + 1 < t_end)
-        {
-            const BlkTile tn = tiles[tt + 1];
-            bcs_prefetch(stage[sb ^ 1], tn, descs[tn.blk], cp_all, rows_all, vals_all);
-        }
-        else
-            asm volatile("cp.async.commit_group;" ::: "memory"); // keeps the group count uniform
-        if (t.blk != cur)
-        {
-            // every thread is done with the previous block's columns (the barrier
-            // closing the last tile's write-back); stage this block's
-            const double *src = BT_vals + D.b_off;
-            const long long nval = (long long)D.m0 * D.n0_B;
-            const bool bulk = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && ((nval & 1) == 0) && nval > 0;
-            if (bulk)
-            {
-                if (threadIdx.x == 0)
-                {
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    const unsigned bytes = (unsigned)(nval * 8);
-                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&mbar)),
-                                 "r"(bytes)
-                                 : "memory");
-                    for (unsigned off = 0; off < bytes; off += 32768u)
-                    {
-                        const unsigned sz = min(32768u, bytes - off);
-                        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
-                                     "%2, [%3];" ::"r"(smem_u32(bcs_sm + off)),
-                                     "l"(reinterpret_cast<const unsigned char *>(src) + off), "r"(sz),
-                                     "r"(smem_u32(&mbar))
-                                     : "memory");
-                    }
-                }
-                // bounded wait for the copy (parity `phase`)
-                unsigned done = 0;
-                for (long long it = 0; it < BCS_WAIT_LIMIT && !done; ++it)
-                    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
-                                 "selp.u32 %0, 1, 0, p; }"
-                                 : "=r"(done)
-                                 : "r"(smem_u32(&mbar)), "r"(phase)
-                                 : "memory");
-                if (!done) abort_flag = 1;
-                phase ^= 1u;
-            }
-            else
-                for (long long i = threadIdx.x; i < nval; i += BCS_THREADS) bt[i] = src[i];
-            __syncthreads();
-            if (abort_flag)
-            {
-                if (threadIdx.x == 0) atomicOr(err, 16);
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                return;
-            }
-            cur = t.blk;
-        }
-        // this tile's stage is complete (the newest group, the next tile's, may
-        // still be in flight)
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
-        __syncthreads();
-        const BcsStage &st = stage[sb];
-        const bool staged = t.d1 - t.d0 <= BCS_ENT;
-        const int *grows = rows_all + D.d_off, *scp = st.cp;
-        const double *gvals = vals_all + D.d_off;
-        const int ncol = min(BC_COLS, D.n0_C - t.c0);
-        for (int i0 = 0; i0 < D.m0; i0 += BC_ROWS)
-        {
-            const int ia = i0 + lane, ib = i0 + 32 + lane;
-            for (int cl = warp; cl < BC_COLS; cl += BCS_THREADS / 32)
-            {
-                double a0 = 0.0, a1 = 0.0;
-                if (cl < ncol)
-                {
-                    const int d1 = scp[cl + 1];
-                    for (int d = scp[cl]; d < d1; ++d)
-                    {
-                        const int r = staged ? st.rows[d - t.d0] : grows[d];
-                        const double v = staged ? st.vals[d - t.d0] : gvals[d];
-                        const double *col = bt + (long long)r * D.m0;
-                        if (ia < D.m0) a0 = __dadd_rn(a0, __dmul_rn(col[ia], v));
-                        if (ib < D.m0) a1 = __dadd_rn(a1, __dmul_rn(col[ib], v));
-                    }
-                }
-                tile[lane][cl] = a0;
-                tile[32 + lane][cl] = a1;
-            }
-            __syncthreads();
-            const int nrow = min(BC_ROWS, D.m0 - i0);
-            double *C = C_vals + D.c_off + (long long)i0 * D.n0_C + t.c0;
-            for (int e = threadIdx.x; e < nrow * BC_COLS; e += BCS_THREADS)
-            {
-                const int ri = e / BC_COLS, cl = e % BC_COLS;
-                if (cl < ncol) __stcs(C + (long long)ri * D.n0_C + cl, tile[ri][cl]);
-            }
-            __syncthreads();
-        }
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 } // namespace
@@ -420,9 +229,7 @@ std::unique_ptr<BlocksCsrPlan> blocks_csr_build(int n_src, const int *m0, const 
             D.n0_B = n0[k];
             D.n0_C = n0C;
             const int blk = (int)descs.size();
-            for (int c0 = 0; c0 < n0C && m0[k] > 0; c0 += BC_COLS)
-                tiles.push_back(BlkTile{blk, c0, cc.cp[c0], cc.cp[std::min(n0C, c0 + BC_COLS)]});
-            P->bt_max = std::max(P->bt_max, bk);
+            for (int c0 = 0; c0 < n0C && m0[k] > 0; c0 += BC_COLS) tiles.push_back(BlkTile{blk, c0});
             descs.push_back(D);
             P->src.push_back(k);
             P->col_perm.push_back(cc.col_perm_C);
@@ -463,18 +270,6 @@ void blocks_csr_fill(const BlocksCsrPlan &P, const double *B_vals, const double 
     // transposed twice: outputs and sources are one to one here)
     const dim3 tg(std::max(1, P.tr_x), std::max(1, P.tr_y), (unsigned)P.src.size());
     SDL_LAUNCH(k_transpose_blocks, tg, dim3(32, 8), 0, s, P.desc.get(), (int)P.src.size(), B_vals, P.BT.get());
-    if ((size_t)P.bt_max * 8 <= BCS_BT_MAX && bcs_smem_bytes(P.bt_max) <= (size_t)rt.smem_optin)
-    {
-        // every source block fits in shared memory: the staged kernel
-        const long long cap = (P.bt_max + 15) / 16 * 16; // keeps the output tile 128-byte aligned
-        const size_t smem = bcs_smem_bytes(cap);
-        if (smem > 48 * 1024)
-            SDL_CUDA(cudaFuncSetAttribute(k_blocks_csr_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int grid = std::max(1, std::min(P.ntiles, rt.num_sms));
-        SDL_LAUNCH(k_blocks_csr_smem, grid, BCS_THREADS, smem, s, P.tiles.get(), P.ntiles, P.desc.get(), P.cp.get(),
-                   P.rows.get(), P.vals.get(), P.BT.get(), C_vals, cap, rt.d_error);
-        return;
-    }
     SDL_LAUNCH(k_blocks_csr, P.ntiles, BC_THREADS, 0, s, P.tiles.get(), P.desc.get(), P.cp.get(),
                P.rows.get(), P.vals.get(), P.BT.get(), C_vals);
 }

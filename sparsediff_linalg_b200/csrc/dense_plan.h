@@ -21,11 +21,10 @@ struct BlkDesc
     int m0, n0_B, n0_C, pad;
 };
 
-// One CTA's share: columns [c0, c0 + 32) of output block `blk`, whose compact-CSC
-// entries are [d0, d1) (relative to the block's d_off).
+// One CTA's share: columns [c0, c0 + 32) of output block `blk`.
 struct BlkTile
 {
-    int blk, c0, d0, d1;
+    int blk, c0;
 };
 
 struct BlocksCsrPlan
@@ -43,7 +42,6 @@ struct BlocksCsrPlan
     DevBuf<int> cp, rows, pos;
     DevBuf<double> vals; // S.x gathered in compact order (refill scratch)
     DevBuf<double> BT;   // the source blocks transposed (refill scratch)
-    long long bt_max = 0; // values of the largest source block
     int tr_x = 0, tr_y = 0; // transpose grid: 32 x 32 tiles of the largest block
     DevBuf<BlkDesc> desc;
     DevBuf<BlkTile> tiles;

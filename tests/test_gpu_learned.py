@@ -118,7 +118,12 @@ def test_oneshot_product_matches_oracle(sdl, orc, mode):
         net, _, _ = _train(sdl, seeds=(30, 31), epochs=6)
         margin = 0.25
     else:
+        # a network that predicts no outputs at all: every row gets the minimum
+        # capacity (8 slots) and every longer row overflows and is redone exactly
         net, margin = Mlp(seed=9), 0.0
+        p = np.zeros(mo.NPARAMS, np.float32)
+        p[-4] = -30.0                                   # bias of the row-nnz output
+        net.set_params(p)
     A, B = _skewed(77)
     n = 20000
     Q = LearnedFilledProduct(A[0], A[1], B[0], B[1], n, net, A[2], None, B[2], margin=margin)
