@@ -544,33 +544,6 @@ __global__ void k_oneshot_cta(const int *__restrict__ rows, int count, OneShotAr
     }
 }
 
-// Final columns and values of every row from its slot range (capacity slots, or
-// the exact redo's slots for rows that overflowed); rows marked `late` get their
-// values afterwards (large rows: columns here, values by the accumulating kernel).
-__global__ void k_oneshot_compact(const long long *__restrict__ cap_off, const long long *__restrict__ fb_off,
-                                  const unsigned char *__restrict__ overflow, const unsigned char *__restrict__ late,
-                                  const int *__restrict__ Cp, const int *__restrict__ tcol,
-                                  const double *__restrict__ tval, const int *__restrict__ fcol,
-                                  const double *__restrict__ fval, int *__restrict__ Ci, double *__restrict__ Cx,
-                                  int m_out)
-{
-    const int lane = lane_id(), wpb = blockDim.x >> 5;
-    for (long long row = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); row < m_out;
-         row += (long long)gridDim.x * wpb)
-    {
-        const int c0 = Cp[row], nn = Cp[row + 1] - c0;
-        const bool ov = overflow[row];
-        const int *sc = ov ? fcol + fb_off[row] : tcol + cap_off[row];
-        const double *sv = ov ? fval + fb_off[row] : tval + cap_off[row];
-        const bool vals = !late[row];
-        for (int q = lane; q < nn; q += 32)
-        {
-            Ci[c0 + q] = sc[q];
-            if (vals) Cx[c0 + q] = sv[q];
-        }
-    }
-}
-
 __global__ void k_mark_class(const unsigned char *__restrict__ cls, int m_out, int which,
                              unsigned char *__restrict__ out)
 {
@@ -647,19 +620,63 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
     }
 }
 
-__global__ void k_compact(const long long *__restrict__ ub_off, const int *__restrict__ row_nnz,
-                          const int *__restrict__ Cp, const int *__restrict__ tmp,
-                          int *__restrict__ Ci, int m_out)
+// Compaction of per-row slot ranges into C: row r's Cp[r + 1] - Cp[r] outputs are
+// copied from its slots (off0[r] in src0, or off1[r] in src1 for rows flagged in
+// sel) to C.i (and C.x when value sources are given, except for rows flagged in
+// late). A CTA takes COMPACT_ROWS consecutive rows and its threads stride over all
+// of their outputs (each output finds its row by a search over the CTA's row
+// offsets in shared memory), so rows of one or two outputs -- most rows of a skewed
+// product -- do not leave a warp idle.
+constexpr int COMPACT_ROWS = 256;
+__global__ void __launch_bounds__(256) k_compact_rows(const int *__restrict__ Cp, int m_out,
+                                                      const long long *__restrict__ off0,
+                                                      const long long *__restrict__ off1,
+                                                      const unsigned char *__restrict__ sel,
+                                                      const unsigned char *__restrict__ late,
+                                                      const int *__restrict__ src0c, const int *__restrict__ src1c,
+                                                      const double *__restrict__ src0v,
+                                                      const double *__restrict__ src1v, int *__restrict__ Ci,
+                                                      double *__restrict__ Cx)
 {
-    const int lane = lane_id(), wpb = blockDim.x >> 5;
-    for (long long row = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); row < m_out;
-         row += (long long)gridDim.x * wpb)
+    __shared__ int cp[COMPACT_ROWS + 1];
+    __shared__ long long so[COMPACT_ROWS];
+    __shared__ unsigned char fl[COMPACT_ROWS];
+    for (long long r0 = (long long)blockIdx.x * COMPACT_ROWS; r0 < m_out; r0 += (long long)gridDim.x * COMPACT_ROWS)
     {
-        int nn = row_nnz[row];
-        const int *src = tmp + ub_off[row];
-        int *dst = Ci + Cp[row];
-        for (int q = lane; q < nn; q += 32) dst[q] = src[q];
+        const int nr = (int)(m_out - r0 < COMPACT_ROWS ? m_out - r0 : COMPACT_ROWS);
+        for (int i = threadIdx.x; i <= nr; i += blockDim.x) cp[i] = Cp[r0 + i];
+        for (int i = threadIdx.x; i < nr; i += blockDim.x)
+        {
+            const bool alt = sel && sel[r0 + i];
+            so[i] = alt ? off1[r0 + i] : off0[r0 + i];
+            fl[i] = (unsigned char)((alt ? 1 : 0) | (late && late[r0 + i] ? 2 : 0));
+        }
+        __syncthreads();
+        const int q0 = cp[0], q1 = cp[nr];
+        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x)
+        {
+            int lo = 0, hi = nr; // last row i with cp[i] <= q
+            while (hi - lo > 1)
+            {
+                const int mid = (lo + hi) >> 1;
+                if (cp[mid] <= q)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const long long at = so[lo] + (q - cp[lo]);
+            const bool alt = fl[lo] & 1;
+            Ci[q] = alt ? src1c[at] : src0c[at];
+            if (Cx && !(fl[lo] & 2)) Cx[q] = alt ? src1v[at] : src0v[at];
+        }
+        __syncthreads();
     }
+}
+
+int compact_grid(int m_out)
+{
+    return (int)std::max<long long>(1, std::min<long long>(((long long)m_out + COMPACT_ROWS - 1) / COMPACT_ROWS,
+                                                           (long long)runtime().num_sms * 16));
 }
 
 // ------------------------------------------------------------ numeric kernels
@@ -1401,13 +1418,26 @@ __global__ void k_num_cta(const int *__restrict__ rows, int count, NumArgs a,
     }
 }
 
-constexpr int GMEM_CLAIM = 4096;
+constexpr int GMEM_CLAIM = 16384; // claim slots (a power of two)
+constexpr int GMEM_TPT = 8;        // terms per thread in one claim round
+constexpr int GMEM_THREADS = 512;
+
+__host__ __device__ constexpr size_t gmem_smem_bytes()
+{
+    return (size_t)GMEM_THREADS * 8 + GMEM_CLAIM * 4 + (3 * GMEM_THREADS + 32) * 4;
+}
 
 // Large rows: accumulate straight into C.x; a per-CTA global map column -> position
 // (only this row's columns are ever read, so it never needs clearing) and a hashed
-// claim table keep same-position terms in order.
-__global__ void k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
-                           int *__restrict__ posmap_all, int n, const ProdPtrs *__restrict__ vals)
+// claim table keep same-position terms in order. A claim round takes GMEM_TPT terms
+// per thread (GMEM_THREADS * GMEM_TPT consecutive terms): every pending term claims
+// its slot with its term index, the smallest index of a slot adds its product, and
+// the round repeats until no term is pending -- so the terms of one output are
+// added in ascending term order (upstream's visiting order), whichever threads
+// hold them.
+__global__ void __launch_bounds__(GMEM_THREADS) k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
+                                                          int *__restrict__ posmap_all, int n,
+                                                          const ProdPtrs *__restrict__ vals)
 {
     bind_values(a, vals);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1437,39 +1467,52 @@ __global__ void k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
         {
             int total = cta_load_chunk(a.Li, a.Ap, b, a.n_L, c, le, ch, a.Lx, a.L_map, a.d, true);
             int nent = min((int)blockDim.x, le - c);
-            for (int base = 0; base < total; base += blockDim.x)
+            for (int base = 0; base < total; base += blockDim.x * GMEM_TPT)
             {
-                int u = base + threadIdx.x;
-                bool pending = u < total;
-                int pos = 0;
-                double prod = 0.0;
-                if (pending)
+                int pos[GMEM_TPT];
+                double prod[GMEM_TPT];
+                unsigned pend = 0; // bit k: term k of this thread still to be added
+#pragma unroll
+                for (int k = 0; k < GMEM_TPT; ++k)
                 {
-                    int e = cta_entry_of(ch.incl, nent, u);
-                    int jj = ch.s[e] + u - (ch.incl[e] - ch.len[e]);
-                    int j = a.Ai[jj];
-                    prod = __dmul_rn(ch.v[e], a.Ax[jj]);
-                    pos = posmap[j];
-                    if (pos < 0 || pos >= nr)
+                    const int u = base + k * blockDim.x + threadIdx.x;
+                    pos[k] = 0;
+                    prod[k] = 0.0;
+                    if (u < total)
                     {
-                        atomicOr(a.err, 1);
-                        pending = false;
+                        int e = cta_entry_of(ch.incl, nent, u);
+                        int jj = ch.s[e] + u - (ch.incl[e] - ch.len[e]);
+                        int j = a.Ai[jj];
+                        prod[k] = __dmul_rn(ch.v[e], a.Ax[jj]);
+                        pos[k] = posmap[j];
+                        if (pos[k] < 0 || pos[k] >= nr)
+                            atomicOr(a.err, 1);
+                        else
+                            pend |= 1u << k;
                     }
                 }
-                int slot = pos & (GMEM_CLAIM - 1);
                 while (true)
                 {
-                    if (pending) atomicMin(&claim[slot], u);
+#pragma unroll
+                    for (int k = 0; k < GMEM_TPT; ++k)
+                        if (pend & (1u << k))
+                            atomicMin(&claim[pos[k] & (GMEM_CLAIM - 1)], base + k * (int)blockDim.x + (int)threadIdx.x);
                     __syncthreads();
-                    bool won = pending && claim[slot] == u;
-                    if (won) acc[pos] = __dadd_rn(acc[pos], prod);
+                    unsigned won = 0;
+#pragma unroll
+                    for (int k = 0; k < GMEM_TPT; ++k)
+                        if ((pend & (1u << k)) &&
+                            claim[pos[k] & (GMEM_CLAIM - 1)] == base + k * (int)blockDim.x + (int)threadIdx.x)
+                        {
+                            won |= 1u << k;
+                            acc[pos[k]] = __dadd_rn(acc[pos[k]], prod[k]);
+                        }
                     __syncthreads();
-                    if (won)
-                    {
-                        claim[slot] = INT_MAX;
-                        pending = false;
-                    }
-                    if (!__syncthreads_or(pending)) break;
+#pragma unroll
+                    for (int k = 0; k < GMEM_TPT; ++k)
+                        if (won & (1u << k)) claim[pos[k] & (GMEM_CLAIM - 1)] = INT_MAX;
+                    pend &= ~won;
+                    if (!__syncthreads_or(pend != 0)) break;
                 }
             }
             __syncthreads();
@@ -2018,22 +2061,6 @@ __global__ void k_overflow_terms(const unsigned char *__restrict__ overflow, con
         fb_len[r] = overflow[r] ? ub[r] : 0;
 }
 
-__global__ void k_compact_learned(const long long *__restrict__ cap_off, const long long *__restrict__ fb_off,
-                                  const unsigned char *__restrict__ overflow, const int *__restrict__ row_nnz,
-                                  const int *__restrict__ Cp, const int *__restrict__ tmp,
-                                  const int *__restrict__ fb, int *__restrict__ Ci, int m_out)
-{
-    const int lane = lane_id(), wpb = blockDim.x >> 5;
-    for (long long row = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); row < m_out;
-         row += (long long)gridDim.x * wpb)
-    {
-        int nn = row_nnz[row];
-        const int *src = overflow[row] ? fb + fb_off[row] : tmp + cap_off[row];
-        int *dst = Ci + Cp[row];
-        for (int q = lane; q < nn; q += 32) dst[q] = src[q];
-    }
-}
-
 __global__ void k_class_hits(const unsigned char *__restrict__ pcls, const int *__restrict__ Cp, int m_out,
                              unsigned long long *__restrict__ hits)
 {
@@ -2082,8 +2109,8 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
     if (P.nnz > 0)
-        SDL_LAUNCH(k_compact, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, ub_off.get(),
-                   row_nnz.get(), P.Cp.get(), tmp.get(), P.Ci.get(), m_out);
+        SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, ub_off.get(), nullptr, nullptr,
+                   nullptr, tmp.get(), nullptr, nullptr, nullptr, P.Ci.get(), nullptr);
     P.scratch_bytes = (long long)tmp.bytes();
     build_schedule(d, P, ub.get(), s);
     if (keep_row_terms) P.row_terms = std::move(ub);
@@ -2152,9 +2179,8 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
     if (P.nnz > 0)
-        SDL_LAUNCH(k_compact_learned, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, cap_off.get(),
-                   fb_off.get(), overflow.get(), row_nnz.get(), P.Cp.get(), tmp.get(), fb.get(), P.Ci.get(),
-                   m_out);
+        SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, cap_off.get(), fb_off.get(),
+                   overflow.get(), nullptr, tmp.get(), fb.get(), nullptr, nullptr, P.Ci.get(), nullptr);
     {
         DevBuf<unsigned long long> hits(1);
         SDL_CUDA(cudaMemsetAsync(hits.get(), 0, 8, s));
@@ -2306,9 +2332,8 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
     SDL_LAUNCH(k_mark_class, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, cls.get(), m_out, (int)SYM_BITMAP,
                late.get());
     if (P.nnz > 0)
-        SDL_LAUNCH(k_oneshot_compact, grid_for(m_out, 8, rt.num_sms * 16), 256, 0, s, cap_off.get(), fb_off.get(),
-                   overflow.get(), late.get(), P.Cp.get(), tcol.get(), tval.get(), fcol.get(), fval.get(), P.Ci.get(),
-                   Cx.get(), m_out);
+        SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, cap_off.get(), fb_off.get(),
+                   overflow.get(), late.get(), tcol.get(), fcol.get(), tval.get(), fval.get(), P.Ci.get(), Cx.get());
     // values of the larger rows: accumulated in C.x through a per-CTA column ->
     // position map, same-position terms applied in visiting order
     if (cnt[SYM_BITMAP] && P.nnz > 0)
@@ -2319,10 +2344,9 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
         DevBuf<int> posmap((size_t)slots * per_slot);
         NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(), Cx.get(),
                    rt.d_error};
-        const int th = 512;
-        const size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
+        const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
-        SDL_LAUNCH(k_num_gmem, slots, th, sm, s, lists.get() + off[SYM_BITMAP], cnt[SYM_BITMAP], na, posmap.get(),
+        SDL_LAUNCH(k_num_gmem, slots, GMEM_THREADS, sm, s, lists.get() + off[SYM_BITMAP], cnt[SYM_BITMAP], na, posmap.get(),
                    P.n, nullptr);
         if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "one-shot product: a term column is missing from its row");
     }
@@ -2503,8 +2527,8 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
     }
     if (cnt[NUM_GMEM])
     {
-        int th = 512;
-        size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
+        const int th = GMEM_THREADS;
+        const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
         SDL_LAUNCH(k_num_gmem, P.gmem_slots, th, sm, s, rows + off[NUM_GMEM], cnt[NUM_GMEM], na,
                    P.gmem_scratch.get(), P.n, vals);
@@ -2540,8 +2564,8 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
     }
     if (cnt[NUM_GMEM])
     {
-        int th = 512;
-        size_t sm = (size_t)th * 8 + GMEM_CLAIM * 4 + (3 * th + 32) * 4;
+        const int th = GMEM_THREADS;
+        const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
         SDL_LAUNCH(k_num_gmem, std::min(slots, cnt[NUM_GMEM]), th, sm, s, rows + off[NUM_GMEM],
                    cnt[NUM_GMEM], na, posmap, P.n, nullptr);
