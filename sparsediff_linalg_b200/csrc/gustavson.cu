@@ -653,21 +653,40 @@ __global__ void __launch_bounds__(256) k_compact_rows(const int *__restrict__ Cp
         }
         __syncthreads();
         const int q0 = cp[0], q1 = cp[nr];
-        for (int q = q0 + threadIdx.x; q < q1; q += blockDim.x)
+        constexpr int ILP = 4; // outputs per thread whose loads are in flight together
+        for (int qb = q0 + threadIdx.x; qb < q1; qb += ILP * blockDim.x)
         {
-            int lo = 0, hi = nr; // last row i with cp[i] <= q
-            while (hi - lo > 1)
+            int col[ILP], lo[ILP];
+            double val[ILP];
+#pragma unroll
+            for (int k = 0; k < ILP; ++k)
             {
-                const int mid = (lo + hi) >> 1;
-                if (cp[mid] <= q)
-                    lo = mid;
-                else
-                    hi = mid;
+                const int q = qb + k * blockDim.x;
+                lo[k] = -1;
+                if (q >= q1) continue;
+                int l = 0, hi = nr; // last row i with cp[i] <= q
+                while (hi - l > 1)
+                {
+                    const int mid = (l + hi) >> 1;
+                    if (cp[mid] <= q)
+                        l = mid;
+                    else
+                        hi = mid;
+                }
+                lo[k] = l;
+                const long long at = so[l] + (q - cp[l]);
+                const bool alt = fl[l] & 1;
+                col[k] = alt ? src1c[at] : src0c[at];
+                if (Cx && !(fl[l] & 2)) val[k] = alt ? src1v[at] : src0v[at];
             }
-            const long long at = so[lo] + (q - cp[lo]);
-            const bool alt = fl[lo] & 1;
-            Ci[q] = alt ? src1c[at] : src0c[at];
-            if (Cx && !(fl[lo] & 2)) Cx[q] = alt ? src1v[at] : src0v[at];
+#pragma unroll
+            for (int k = 0; k < ILP; ++k)
+            {
+                if (lo[k] < 0) continue;
+                const int q = qb + k * blockDim.x;
+                Ci[q] = col[k];
+                if (Cx && !(fl[lo[k]] & 2)) Cx[q] = val[k];
+            }
         }
         __syncthreads();
     }
@@ -1420,34 +1439,37 @@ __global__ void k_num_cta(const int *__restrict__ rows, int count, NumArgs a,
 
 constexpr int GMEM_CLAIM = 16384; // claim slots (a power of two)
 constexpr int GMEM_TPT = 8;        // terms per thread in one claim round
+constexpr int GMEM_EPT = 8;        // L entries per thread in one chunk
 constexpr int GMEM_THREADS = 512;
+constexpr int GMEM_CHUNK = GMEM_THREADS * GMEM_EPT;
 
 __host__ __device__ constexpr size_t gmem_smem_bytes()
 {
-    return (size_t)GMEM_THREADS * 8 + GMEM_CLAIM * 4 + (3 * GMEM_THREADS + 32) * 4;
+    // per chunk entry: value (8 B), inclusive term count, A row start and length
+    // (4 B each); the claim table; the scan scratch
+    return (size_t)GMEM_CHUNK * 20 + GMEM_CLAIM * 4 + 64 * 4;
 }
 
 // Large rows: accumulate straight into C.x; a per-CTA global map column -> position
 // (only this row's columns are ever read, so it never needs clearing) and a hashed
-// claim table keep same-position terms in order. A claim round takes GMEM_TPT terms
-// per thread (GMEM_THREADS * GMEM_TPT consecutive terms): every pending term claims
-// its slot with its term index, the smallest index of a slot adds its product, and
-// the round repeats until no term is pending -- so the terms of one output are
-// added in ascending term order (upstream's visiting order), whichever threads
-// hold them.
+// claim table keep same-position terms in order. The row's L entries are taken
+// GMEM_CHUNK at a time (GMEM_EPT consecutive entries per thread), and their terms
+// in claim rounds of GMEM_TPT terms per thread: every pending term claims its slot
+// with its term index, the smallest index of a slot adds its product, and the round
+// repeats until no term is pending -- so the terms of one output are added in
+// ascending term order (upstream's visiting order), whichever threads hold them.
 __global__ void __launch_bounds__(GMEM_THREADS) k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
                                                           int *__restrict__ posmap_all, int n,
                                                           const ProdPtrs *__restrict__ vals)
 {
     bind_values(a, vals);
     extern __shared__ __align__(16) unsigned char smraw[];
-    CtaChunk ch;
-    ch.v = (double *)smraw;
-    int *claim = (int *)(ch.v + blockDim.x);
-    ch.incl = claim + GMEM_CLAIM;
-    ch.s = ch.incl + blockDim.x;
-    ch.len = ch.s + blockDim.x;
-    ch.scr = ch.len + blockDim.x;
+    double *ev = (double *)smraw;                 // entry values
+    int *incl = (int *)(ev + GMEM_CHUNK);         // inclusive term counts
+    int *es = incl + GMEM_CHUNK;                  // A row starts
+    int *elen = es + GMEM_CHUNK;                  // A row lengths
+    int *claim = elen + GMEM_CHUNK;
+    int *scr = claim + GMEM_CLAIM;
     int *posmap = posmap_all + (long long)blockIdx.x * n;
     for (int it = blockIdx.x; it < count; it += gridDim.x)
     {
@@ -1463,10 +1485,43 @@ __global__ void __launch_bounds__(GMEM_THREADS) k_num_gmem(const int *__restrict
         for (int q = threadIdx.x; q < GMEM_CLAIM; q += blockDim.x) claim[q] = INT_MAX;
         __syncthreads();
         int ls = a.Lp[r], le = a.Lp[r + 1];
-        for (int c = ls; c < le; c += blockDim.x)
+        for (int c = ls; c < le; c += GMEM_CHUNK)
         {
-            int total = cta_load_chunk(a.Li, a.Ap, b, a.n_L, c, le, ch, a.Lx, a.L_map, a.d, true);
-            int nent = min((int)blockDim.x, le - c);
+            // this thread's GMEM_EPT consecutive entries, their term counts scanned
+            const int e0 = threadIdx.x * GMEM_EPT;
+            int mine = 0;
+            int lens[GMEM_EPT];
+#pragma unroll
+            for (int k = 0; k < GMEM_EPT; ++k)
+            {
+                const int ii = c + e0 + k;
+                int st = 0, ln = 0;
+                double v = 0.0;
+                if (ii < le)
+                {
+                    const int kk = a.Li[ii] + b * a.n_L;
+                    st = a.Ap[kk];
+                    ln = a.Ap[kk + 1] - st;
+                    const double lx = a.Lx ? a.Lx[a.L_map ? a.L_map[ii] : ii] : 1.0;
+                    v = a.d ? __dmul_rn(lx, a.d[kk]) : lx;
+                }
+                es[e0 + k] = st;
+                elen[e0 + k] = ln;
+                ev[e0 + k] = v;
+                lens[k] = ln;
+                mine += ln;
+            }
+            const int before = block_incl_scan_int(mine, scr) - mine; // ends with a barrier
+            int run = before;
+#pragma unroll
+            for (int k = 0; k < GMEM_EPT; ++k)
+            {
+                run += lens[k];
+                incl[e0 + k] = run;
+            }
+            __syncthreads();
+            const int total = incl[GMEM_CHUNK - 1];
+            const int nent = min(GMEM_CHUNK, le - c);
             for (int base = 0; base < total; base += blockDim.x * GMEM_TPT)
             {
                 int pos[GMEM_TPT];
@@ -1480,10 +1535,10 @@ __global__ void __launch_bounds__(GMEM_THREADS) k_num_gmem(const int *__restrict
                     prod[k] = 0.0;
                     if (u < total)
                     {
-                        int e = cta_entry_of(ch.incl, nent, u);
-                        int jj = ch.s[e] + u - (ch.incl[e] - ch.len[e]);
+                        int e = cta_entry_of(incl, nent, u);
+                        int jj = es[e] + u - (incl[e] - elen[e]);
                         int j = a.Ai[jj];
-                        prod[k] = __dmul_rn(ch.v[e], a.Ax[jj]);
+                        prod[k] = __dmul_rn(ev[e], a.Ax[jj]);
                         pos[k] = posmap[j];
                         if (pos[k] < 0 || pos[k] >= nr)
                             atomicOr(a.err, 1);
