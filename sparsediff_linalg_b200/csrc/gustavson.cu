@@ -554,6 +554,24 @@ __global__ void k_oneshot_cta(const int *__restrict__ rows, int count, OneShotAr
 constexpr int OSH_THREADS = 512;
 constexpr int OSH_TPT = 4;
 constexpr int OSH_CLAIM = 4096;
+constexpr int OSH_EPT = 2; // L entries per thread in one chunk
+constexpr int OSH_CHUNK = OSH_THREADS * OSH_EPT;
+
+// Entry of term u for a warp whose lanes hold 32 consecutive terms u0 + lane: lane 0
+// searches u0's entry e0, every lane loads the inclusive count of entry e0 + lane,
+// and a lane's entry is e0 + the number of those counts <= its u (entries hold at
+// least one term unless their A row is empty; when the warp's terms span more than
+// 32 entries the lane searches on its own). Every lane of the warp must call it.
+__device__ __forceinline__ int warp_chunk_entry(const int *incl, int nent, int u0, int u)
+{
+    int e0 = 0;
+    if (lane_id() == 0) e0 = cta_entry_of(incl, nent, u0);
+    e0 = __shfl_sync(FULL_MASK, e0, 0);
+    const int mine = e0 + lane_id() < nent ? incl[e0 + lane_id()] : INT_MAX;
+    const int last = __shfl_sync(FULL_MASK, mine, 31);
+    const int k = warp_entry_of(mine, u); // valid for u below the 32nd candidate's count
+    return u < last ? e0 + k : cta_entry_of(incl, nent, u);
+}
 
 // Byte offset of the chunk arrays (their doubles first): after the bitmap, the
 // prefix per 4 words and the claims, rounded up to 16 bytes.
@@ -565,7 +583,43 @@ __host__ __device__ constexpr size_t osh_chunk_offset(int words)
 __host__ __device__ constexpr size_t osh_smem_bytes(int words)
 {
     // bitmap, prefix per 4 words, claims, chunk arrays (value, incl, start, length), scan scratch
-    return osh_chunk_offset(words) + (size_t)OSH_THREADS * 8 + (size_t)(3 * OSH_THREADS + 32) * 4;
+    return osh_chunk_offset(words) + (size_t)OSH_CHUNK * 20 + 64 * 4;
+}
+
+// Loads OSH_CHUNK L entries of row (b, r) from c (OSH_EPT consecutive per thread):
+// their A row starts and lengths, values (when asked) and inclusive term counts.
+// Returns the chunk's term count; ends with a barrier.
+__device__ __forceinline__ int osh_load_chunk(const OneShotArgs &a, int b, int c, int le, double *ev, int *incl,
+                                              int *es, int *elen, int *scr, bool want_v)
+{
+    const int e0 = threadIdx.x * OSH_EPT;
+    int lens[OSH_EPT], mine = 0;
+#pragma unroll
+    for (int k = 0; k < OSH_EPT; ++k)
+    {
+        const int ii = c + e0 + k;
+        int st = 0, ln = 0;
+        if (ii < le)
+        {
+            const int kk = a.Li[ii] + b * a.n_L;
+            st = a.Ap[kk];
+            ln = a.Ap[kk + 1] - st;
+            if (want_v) ev[e0 + k] = oneshot_entry_value(a, ii, kk);
+        }
+        es[e0 + k] = st;
+        elen[e0 + k] = ln;
+        lens[k] = ln;
+        mine += ln;
+    }
+    int run = block_incl_scan_int(mine, scr) - mine;
+#pragma unroll
+    for (int k = 0; k < OSH_EPT; ++k)
+    {
+        run += lens[k];
+        incl[e0 + k] = run;
+    }
+    __syncthreads();
+    return incl[OSH_CHUNK - 1];
 }
 
 __device__ __forceinline__ int osh_rank(const unsigned *bm, const int *pre, int j)
@@ -584,12 +638,11 @@ __global__ void __launch_bounds__(OSH_THREADS, 1) k_oneshot_heavy(const int *__r
     const int ngroups = words / 4;
     int *pre = reinterpret_cast<int *>(bm + words);
     int *claim = pre + ngroups + 1;
-    CtaChunk ch;
-    ch.v = reinterpret_cast<double *>(osm + osh_chunk_offset(words));
-    ch.incl = reinterpret_cast<int *>(ch.v + blockDim.x);
-    ch.s = ch.incl + blockDim.x;
-    ch.len = ch.s + blockDim.x;
-    ch.scr = ch.len + blockDim.x;
+    double *ev = reinterpret_cast<double *>(osm + osh_chunk_offset(words));
+    int *incl_c = reinterpret_cast<int *>(ev + OSH_CHUNK);
+    int *es = incl_c + OSH_CHUNK;
+    int *elen = es + OSH_CHUNK;
+    int *scr = elen + OSH_CHUNK;
     __shared__ int nn_sh;
     for (int it = blockIdx.x; it < count; it += gridDim.x)
     {
@@ -600,15 +653,19 @@ __global__ void __launch_bounds__(OSH_THREADS, 1) k_oneshot_heavy(const int *__r
         for (int q = threadIdx.x; q < OSH_CLAIM; q += blockDim.x) claim[q] = INT_MAX;
         __syncthreads();
         // sweep 1: the row's columns
-        for (int c = ls; c < le; c += blockDim.x)
+        for (int c = ls; c < le; c += OSH_CHUNK)
         {
-            const int total = cta_load_chunk(a.Li, a.Ap, b, a.n_L, c, le, ch, nullptr, nullptr, nullptr, false);
-            const int nent = min((int)blockDim.x, le - c);
-            for (int u = threadIdx.x; u < total; u += blockDim.x)
+            const int total = osh_load_chunk(a, b, c, le, ev, incl_c, es, elen, scr, false);
+            const int nent = min(OSH_CHUNK, le - c);
+            for (int ub = (threadIdx.x & ~31); ub < total; ub += blockDim.x)
             {
-                const int e = cta_entry_of(ch.incl, nent, u);
-                const int j = a.Ai[ch.s[e] + u - (ch.incl[e] - ch.len[e])];
-                atomicOr(&bm[j >> 5], 1u << (j & 31));
+                const int u = ub + lane_id();
+                const int e = warp_chunk_entry(incl_c, nent, ub, u);
+                if (u < total)
+                {
+                    const int j = a.Ai[es[e] + u - (incl_c[e] - elen[e])];
+                    atomicOr(&bm[j >> 5], 1u << (j & 31));
+                }
             }
             __syncthreads();
         }
@@ -618,7 +675,7 @@ __global__ void __launch_bounds__(OSH_THREADS, 1) k_oneshot_heavy(const int *__r
         int mine = 0;
         for (int g = g0; g < g1; ++g)
             mine += __popc(bm[4 * g]) + __popc(bm[4 * g + 1]) + __popc(bm[4 * g + 2]) + __popc(bm[4 * g + 3]);
-        const int incl = block_incl_scan_int(mine, ch.scr);
+        const int incl = block_incl_scan_int(mine, scr);
         int run = incl - mine;
         for (int g = g0; g < g1; ++g)
         {
@@ -659,10 +716,10 @@ __global__ void __launch_bounds__(OSH_THREADS, 1) k_oneshot_heavy(const int *__r
         __syncthreads();
         // sweep 2: every term's product added at its rank, same-output terms in order
         double *acc = a.val + off;
-        for (int c = ls; c < le; c += blockDim.x)
+        for (int c = ls; c < le; c += OSH_CHUNK)
         {
-            const int total = cta_load_chunk(a.Li, a.Ap, b, a.n_L, c, le, ch, a.Lx, a.L_map, a.d, true);
-            const int nent = min((int)blockDim.x, le - c);
+            const int total = osh_load_chunk(a, b, c, le, ev, incl_c, es, elen, scr, true);
+            const int nent = min(OSH_CHUNK, le - c);
             for (int base = 0; base < total; base += blockDim.x * OSH_TPT)
             {
                 int pos[OSH_TPT];
@@ -671,15 +728,17 @@ __global__ void __launch_bounds__(OSH_THREADS, 1) k_oneshot_heavy(const int *__r
 #pragma unroll
                 for (int k = 0; k < OSH_TPT; ++k)
                 {
-                    const int u = base + k * blockDim.x + threadIdx.x;
+                    const int ub = base + k * blockDim.x + (threadIdx.x & ~31);
+                    const int u = ub + lane_id();
                     pos[k] = 0;
                     prod[k] = 0.0;
+                    if (ub >= total) continue; // uniform over the warp
+                    const int e = warp_chunk_entry(incl_c, nent, ub, u);
                     if (u < total)
                     {
-                        const int e = cta_entry_of(ch.incl, nent, u);
-                        const int jj = ch.s[e] + u - (ch.incl[e] - ch.len[e]);
+                        const int jj = es[e] + u - (incl_c[e] - elen[e]);
                         pos[k] = osh_rank(bm, pre, a.Ai[jj]);
-                        prod[k] = __dmul_rn(ch.v[e], a.Ax[jj]);
+                        prod[k] = __dmul_rn(ev[e], a.Ax[jj]);
                         if ((unsigned)pos[k] < (unsigned)nn)
                             pend |= 1u << k;
                         else
