@@ -544,236 +544,6 @@ __global__ void k_oneshot_cta(const int *__restrict__ rows, int count, OneShotAr
     }
 }
 
-// One-shot of a large row (more than 8192 terms), structure and values in one
-// kernel: a first sweep over the row's terms marks its columns in a shared-memory
-// bitmap of all n columns; prefix counts per 128 columns turn the bitmap into a
-// rank structure, so a column's output position is its rank among the marked
-// columns (the outputs are the marked columns in ascending order). The columns are
-// written, the row's values cleared, and a second sweep adds every term's product
-// at its rank, in claim rounds that keep same-output terms in visiting order.
-constexpr int OSH_THREADS = 512;
-constexpr int OSH_TPT = 4;
-constexpr int OSH_CLAIM = 4096;
-constexpr int OSH_EPT = 2; // L entries per thread in one chunk
-constexpr int OSH_CHUNK = OSH_THREADS * OSH_EPT;
-
-// Entry of term u for a warp whose lanes hold 32 consecutive terms u0 + lane: lane 0
-// searches u0's entry e0, every lane loads the inclusive count of entry e0 + lane,
-// and a lane's entry is e0 + the number of those counts <= its u (entries hold at
-// least one term unless their A row is empty; when the warp's terms span more than
-// 32 entries the lane searches on its own). Every lane of the warp must call it.
-__device__ __forceinline__ int warp_chunk_entry(const int *incl, int nent, int u0, int u)
-{
-    int e0 = 0;
-    if (lane_id() == 0) e0 = cta_entry_of(incl, nent, u0);
-    e0 = __shfl_sync(FULL_MASK, e0, 0);
-    const int mine = e0 + lane_id() < nent ? incl[e0 + lane_id()] : INT_MAX;
-    const int last = __shfl_sync(FULL_MASK, mine, 31);
-    const int k = warp_entry_of(mine, u); // valid for u below the 32nd candidate's count
-    return u < last ? e0 + k : cta_entry_of(incl, nent, u);
-}
-
-// Byte offset of the chunk arrays (their doubles first): after the bitmap, the
-// prefix per 4 words and the claims, rounded up to 16 bytes.
-__host__ __device__ constexpr size_t osh_chunk_offset(int words)
-{
-    return ((size_t)words * 4 + (size_t)(words / 4 + 1) * 4 + OSH_CLAIM * 4 + 15) / 16 * 16;
-}
-
-__host__ __device__ constexpr size_t osh_smem_bytes(int words)
-{
-    // bitmap, prefix per 4 words, claims, chunk arrays (value, incl, start, length), scan scratch
-    return osh_chunk_offset(words) + (size_t)OSH_CHUNK * 20 + 64 * 4;
-}
-
-// Loads OSH_CHUNK L entries of row (b, r) from c (OSH_EPT consecutive per thread):
-// their A row starts and lengths, values (when asked) and inclusive term counts.
-// Returns the chunk's term count; ends with a barrier.
-__device__ __forceinline__ int osh_load_chunk(const OneShotArgs &a, int b, int c, int le, double *ev, int *incl,
-                                              int *es, int *elen, int *scr, bool want_v)
-{
-    const int e0 = threadIdx.x * OSH_EPT;
-    int lens[OSH_EPT], mine = 0;
-#pragma unroll
-    for (int k = 0; k < OSH_EPT; ++k)
-    {
-        const int ii = c + e0 + k;
-        int st = 0, ln = 0;
-        if (ii < le)
-        {
-            const int kk = a.Li[ii] + b * a.n_L;
-            st = a.Ap[kk];
-            ln = a.Ap[kk + 1] - st;
-            if (want_v) ev[e0 + k] = oneshot_entry_value(a, ii, kk);
-        }
-        es[e0 + k] = st;
-        elen[e0 + k] = ln;
-        lens[k] = ln;
-        mine += ln;
-    }
-    int run = block_incl_scan_int(mine, scr) - mine;
-#pragma unroll
-    for (int k = 0; k < OSH_EPT; ++k)
-    {
-        run += lens[k];
-        incl[e0 + k] = run;
-    }
-    __syncthreads();
-    return incl[OSH_CHUNK - 1];
-}
-
-__device__ __forceinline__ int osh_rank(const unsigned *bm, const int *pre, int j)
-{
-    const int w = j >> 5, g = w >> 2;
-    int r = pre[g];
-    for (int q = g << 2; q < w; ++q) r += __popc(bm[q]);
-    return r + __popc(bm[w] & ((1u << (j & 31)) - 1u));
-}
-
-__global__ void __launch_bounds__(OSH_THREADS, 1) k_oneshot_heavy(const int *__restrict__ rows, int count,
-                                                                   OneShotArgs a, int words, int *__restrict__ err)
-{
-    extern __shared__ __align__(16) unsigned char osm[];
-    unsigned *bm = reinterpret_cast<unsigned *>(osm);
-    const int ngroups = words / 4;
-    int *pre = reinterpret_cast<int *>(bm + words);
-    int *claim = pre + ngroups + 1;
-    double *ev = reinterpret_cast<double *>(osm + osh_chunk_offset(words));
-    int *incl_c = reinterpret_cast<int *>(ev + OSH_CHUNK);
-    int *es = incl_c + OSH_CHUNK;
-    int *elen = es + OSH_CHUNK;
-    int *scr = elen + OSH_CHUNK;
-    __shared__ int nn_sh;
-    for (int it = blockIdx.x; it < count; it += gridDim.x)
-    {
-        const int row = rows[it];
-        const int b = row / a.L_m, r = row - b * a.L_m;
-        const int ls = a.Lp[r], le = a.Lp[r + 1];
-        for (int q = threadIdx.x; q < words; q += blockDim.x) bm[q] = 0u;
-        for (int q = threadIdx.x; q < OSH_CLAIM; q += blockDim.x) claim[q] = INT_MAX;
-        __syncthreads();
-        // sweep 1: the row's columns
-        for (int c = ls; c < le; c += OSH_CHUNK)
-        {
-            const int total = osh_load_chunk(a, b, c, le, ev, incl_c, es, elen, scr, false);
-            const int nent = min(OSH_CHUNK, le - c);
-            for (int ub = (threadIdx.x & ~31); ub < total; ub += blockDim.x)
-            {
-                const int u = ub + lane_id();
-                const int e = warp_chunk_entry(incl_c, nent, ub, u);
-                if (u < total)
-                {
-                    const int j = a.Ai[es[e] + u - (incl_c[e] - elen[e])];
-                    atomicOr(&bm[j >> 5], 1u << (j & 31));
-                }
-            }
-            __syncthreads();
-        }
-        // prefix counts: each thread sums a contiguous run of groups
-        const int gpt = (ngroups + blockDim.x - 1) / blockDim.x;
-        const int g0 = min(ngroups, (int)threadIdx.x * gpt), g1 = min(ngroups, g0 + gpt);
-        int mine = 0;
-        for (int g = g0; g < g1; ++g)
-            mine += __popc(bm[4 * g]) + __popc(bm[4 * g + 1]) + __popc(bm[4 * g + 2]) + __popc(bm[4 * g + 3]);
-        const int incl = block_incl_scan_int(mine, scr);
-        int run = incl - mine;
-        for (int g = g0; g < g1; ++g)
-        {
-            pre[g] = run;
-            run += __popc(bm[4 * g]) + __popc(bm[4 * g + 1]) + __popc(bm[4 * g + 2]) + __popc(bm[4 * g + 3]);
-        }
-        if (threadIdx.x == blockDim.x - 1)
-        {
-            pre[ngroups] = incl;
-            nn_sh = incl;
-        }
-        __syncthreads();
-        const int nn = nn_sh;
-        const long long off = a.off[row], cap = a.cap ? a.cap[row] : 0x7fffffffffffffffLL;
-        if (threadIdx.x == 0)
-        {
-            a.row_nnz[row] = nn;
-            if (nn > cap) a.overflow[row] = 1;
-        }
-        if (nn > cap) continue; // redone with room for every term (uniform over the CTA)
-        // the columns in ascending order, and the values cleared
-        for (int g = g0; g < g1; ++g)
-        {
-            int at = pre[g];
-            for (int q = 4 * g; q < 4 * g + 4; ++q)
-            {
-                unsigned word = bm[q];
-                while (word)
-                {
-                    const int bit = __ffs(word) - 1;
-                    a.col[off + at] = q * 32 + bit;
-                    a.val[off + at] = 0.0;
-                    ++at;
-                    word &= word - 1;
-                }
-            }
-        }
-        __syncthreads();
-        // sweep 2: every term's product added at its rank, same-output terms in order
-        double *acc = a.val + off;
-        for (int c = ls; c < le; c += OSH_CHUNK)
-        {
-            const int total = osh_load_chunk(a, b, c, le, ev, incl_c, es, elen, scr, true);
-            const int nent = min(OSH_CHUNK, le - c);
-            for (int base = 0; base < total; base += blockDim.x * OSH_TPT)
-            {
-                int pos[OSH_TPT];
-                double prod[OSH_TPT];
-                unsigned pend = 0;
-#pragma unroll
-                for (int k = 0; k < OSH_TPT; ++k)
-                {
-                    const int ub = base + k * blockDim.x + (threadIdx.x & ~31);
-                    const int u = ub + lane_id();
-                    pos[k] = 0;
-                    prod[k] = 0.0;
-                    if (ub >= total) continue; // uniform over the warp
-                    const int e = warp_chunk_entry(incl_c, nent, ub, u);
-                    if (u < total)
-                    {
-                        const int jj = es[e] + u - (incl_c[e] - elen[e]);
-                        pos[k] = osh_rank(bm, pre, a.Ai[jj]);
-                        prod[k] = __dmul_rn(ev[e], a.Ax[jj]);
-                        if ((unsigned)pos[k] < (unsigned)nn)
-                            pend |= 1u << k;
-                        else
-                            atomicOr(err, 1);
-                    }
-                }
-                while (true)
-                {
-#pragma unroll
-                    for (int k = 0; k < OSH_TPT; ++k)
-                        if (pend & (1u << k))
-                            atomicMin(&claim[pos[k] & (OSH_CLAIM - 1)], base + k * (int)blockDim.x + (int)threadIdx.x);
-                    __syncthreads();
-                    unsigned won = 0;
-#pragma unroll
-                    for (int k = 0; k < OSH_TPT; ++k)
-                        if ((pend & (1u << k)) &&
-                            claim[pos[k] & (OSH_CLAIM - 1)] == base + k * (int)blockDim.x + (int)threadIdx.x)
-                        {
-                            won |= 1u << k;
-                            acc[pos[k]] = __dadd_rn(acc[pos[k]], prod[k]);
-                        }
-                    __syncthreads();
-#pragma unroll
-                    for (int k = 0; k < OSH_TPT; ++k)
-                        if (won & (1u << k)) claim[pos[k] & (OSH_CLAIM - 1)] = INT_MAX;
-                    pend &= ~won;
-                    if (!__syncthreads_or(pend != 0)) break;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
 __global__ void k_mark_class(const unsigned char *__restrict__ cls, int m_out, int which,
                              unsigned char *__restrict__ out)
 {
@@ -1667,9 +1437,10 @@ __global__ void k_num_cta(const int *__restrict__ rows, int count, NumArgs a,
     }
 }
 
-constexpr int GMEM_CLAIM = 16384; // claim slots (a power of two)
-constexpr int GMEM_TPT = 8;        // terms per thread in one claim round
-constexpr int GMEM_EPT = 8;        // L entries per thread in one chunk
+constexpr int GMEM_CLAIM = 8192; // claim slots (a power of two)
+constexpr int GMEM_TPT = 4;       // terms per thread in one claim round
+constexpr int GMEM_EPT = 2;       // L entries per thread in one chunk
+constexpr int GMEM_CTAS_PER_SM = 2;
 constexpr int GMEM_THREADS = 512;
 constexpr int GMEM_CHUNK = GMEM_THREADS * GMEM_EPT;
 
@@ -1688,7 +1459,7 @@ __host__ __device__ constexpr size_t gmem_smem_bytes()
 // with its term index, the smallest index of a slot adds its product, and the round
 // repeats until no term is pending -- so the terms of one output are added in
 // ascending term order (upstream's visiting order), whichever threads hold them.
-__global__ void __launch_bounds__(GMEM_THREADS) k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
+__global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
                                                           int *__restrict__ posmap_all, int n,
                                                           const ProdPtrs *__restrict__ vals)
 {
@@ -2272,7 +2043,7 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     {
         long long per_slot = std::max(1, P.n);
         long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
-        P.gmem_slots = (int)std::min<long long>({(long long)rt.num_sms, max_slots,
+        P.gmem_slots = (int)std::min<long long>({(long long)rt.num_sms * GMEM_CTAS_PER_SM, max_slots,
                                                  (long long)P.num_count[NUM_GMEM]});
         P.gmem_scratch.reset((size_t)P.gmem_slots * per_slot);
     }
@@ -2571,23 +2342,10 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
     OneShotArgs oa{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, cap_off.get(), cap.get(),
                    tcol.get(), tval.get(), row_nnz.get(), overflow.get()};
     oneshot_launch(oa, lists.get(), cnt, off, cfg, s);
-    // larger rows: structure and values in one kernel when the row's column bitmap
-    // fits shared memory; else their columns by the bitmap pass and the values once
-    // C is laid out
-    const int osh_words = (int)((((long long)d.A_n + 31) / 32 + 3) / 4 * 4);
-    const bool heavy_fused = osh_smem_bytes(osh_words) <= (size_t)rt.smem_optin;
-    auto heavy = [&](const OneShotArgs &ha, const int *hrows, int hcount) {
-        if (!hcount) return;
-        const size_t sm = osh_smem_bytes(osh_words);
-        set_smem(k_oneshot_heavy, sm);
-        SDL_LAUNCH(k_oneshot_heavy, std::min(hcount, rt.num_sms), OSH_THREADS, sm, s, hrows, hcount, ha, osh_words,
-                   rt.d_error);
-    };
+    // larger rows: their columns by the bitmap pass (values once C is laid out)
     int bcnt[SYM_NBINS] = {0};
     bcnt[SYM_BITMAP] = cnt[SYM_BITMAP];
-    if (bcnt[SYM_BITMAP] && heavy_fused)
-        heavy(oa, lists.get() + off[SYM_BITMAP], cnt[SYM_BITMAP]);
-    else if (bcnt[SYM_BITMAP])
+    if (bcnt[SYM_BITMAP])
     {
         SymArgs sa{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, cap_off.get(), tcol.get(), row_nnz.get(),
                    cap.get(), overflow.get()};
@@ -2616,9 +2374,7 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
         oneshot_launch(fa, flists.get(), fcnt, foff, cfg, s);
         int fb_bits[SYM_NBINS] = {0};
         fb_bits[SYM_BITMAP] = fcnt[SYM_BITMAP];
-        if (fb_bits[SYM_BITMAP] && heavy_fused)
-            heavy(fa, flists.get() + foff[SYM_BITMAP], fcnt[SYM_BITMAP]);
-        else if (fb_bits[SYM_BITMAP])
+        if (fb_bits[SYM_BITMAP])
         {
             SymArgs sb{d.Lp, d.Li, d.L_m, P.n_L, d.A_n, d.Ap, d.Ai, fb_off.get(), fcol.get(), row_nnz.get(),
                        nullptr, nullptr};
@@ -2628,25 +2384,21 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
     Cx.reset(std::max(1, P.nnz));
-    // rows whose values come after the compaction (the unfused large rows)
+    // rows whose values come after the compaction (the large rows)
     DevBuf<unsigned char> late(m_out);
-    if (heavy_fused)
-        SDL_CUDA(cudaMemsetAsync(late.get(), 0, late.bytes(), s));
-    else
-        SDL_LAUNCH(k_mark_class, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, cls.get(), m_out, (int)SYM_BITMAP,
-                   late.get());
+    SDL_LAUNCH(k_mark_class, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, cls.get(), m_out, (int)SYM_BITMAP,
+               late.get());
     if (P.nnz > 0)
         SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, cap_off.get(), fb_off.get(),
                    overflow.get(), late.get(), tcol.get(), fcol.get(), tval.get(), fval.get(), P.Ci.get(), Cx.get());
     // values of the larger rows: accumulated in C.x through a per-CTA column ->
     // position map, same-position terms applied in visiting order
-    if (heavy_fused && cnt[SYM_BITMAP] && take_device_error(s))
-        fail(SDL_ERR_INTERNAL, "one-shot product: a term column is missing from its row");
-    if (!heavy_fused && cnt[SYM_BITMAP] && P.nnz > 0)
+    if (cnt[SYM_BITMAP] && P.nnz > 0)
     {
         const long long per_slot = std::max(1, P.n);
         const long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
-        const int slots = (int)std::min<long long>({(long long)rt.num_sms, max_slots, (long long)cnt[SYM_BITMAP]});
+        const int slots = (int)std::min<long long>(
+            {(long long)rt.num_sms * GMEM_CTAS_PER_SM, max_slots, (long long)cnt[SYM_BITMAP]});
         DevBuf<int> posmap((size_t)slots * per_slot);
         NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(), Cx.get(),
                    rt.d_error};
