@@ -130,6 +130,15 @@ sdl_status sdl_product_replan(sdl_product *P, int tile_budget, int tile_max_term
 /* Threads of P's refill CTAs (256, or 128 for the small-tile refill) and the largest
    row (terms) its tiles take. Any pointer may be NULL. */
 sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, int *tile_max_terms);
+/* No upstream counterpart. Chooses between the two refills of P's tiles: the
+   pipelined one (on = 1, the default: each tile's term words and entry records are
+   copied into shared memory two tiles ahead and its A.x / V values one tile ahead,
+   so computing a tile reads shared memory only), used when every tile of the plan
+   holds at most 1024 terms, 512 entries and 1024 outputs (plans of at most 512-term
+   tiles, which sdl_product_replan and the autotuner make), or the direct one
+   (on = 0). Both give the same bits. *used (may be NULL) reports whether the
+   pipelined refill will run. */
+sdl_status sdl_product_set_refill_pipe(sdl_product *P, int on, int *used);
 
 /* No upstream counterpart (it generalises upstream's fixed plan-vs-accumulator
    threshold GUSTAVSON_PLAN_MAX_RATIO, src/internal/gustavson.h:52, used at

@@ -169,6 +169,15 @@ extern "C" sdl_status sdl_product_replan(sdl_product *P, int tile_budget, int ti
     });
 }
 
+extern "C" sdl_status sdl_product_set_refill_pipe(sdl_product *P, int on, int *used)
+{
+    return guard_status("sdl_product_set_refill_pipe", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        P->P.cfg.refill_pipe = on ? 1 : 0;
+        if (used) *used = pipe_refill(P->P) ? 1 : 0;
+    });
+}
+
 extern "C" sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, int *tile_max_terms)
 {
     return guard_status("sdl_product_refill_shape", [&]() {

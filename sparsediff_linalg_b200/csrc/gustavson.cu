@@ -1349,6 +1349,206 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
     }
 }
 
+// ------------------------------------------------------------ pipelined refill
+// The same refill as k_tile_refill for a single product whose tiles hold at most
+// PIPE_T terms, PIPE_E entries and PIPE_WIN outputs, with every load of a tile
+// moved off the critical path by asynchronous copies into shared memory: the
+// tile's term words and entry records are copied two tiles ahead (cp.async), its
+// A.x value of every term and V value of every entry one tile ahead (cp.async
+// gathers addressed by the staged records), so computing a tile reads shared
+// memory only. Three stages rotate; one wait and one barrier per tile open each
+// step. Products, order of the sums and roundings are those of k_tile_refill
+// (bit-identical): a single term stored as 0.0 + v * A.x, a pair added atomically,
+// outputs of three or more terms summed in visiting order by one thread each.
+constexpr int PIPE_NT = 256;
+constexpr int PIPE_T = 1024;
+constexpr int PIPE_E = 512;
+constexpr int PIPE_WIN = 1024;
+constexpr int PIPE_RU = PIPE_T / PIPE_NT;
+// descriptor ring: a descriptor is copied three tiles ahead, into a slot last used
+// five tiles earlier (barriers in between), never one a slower thread still reads
+constexpr int PIPE_RING = 8;
+
+struct PipeStage
+{
+    unsigned w[PIPE_T];
+    int2 es[PIPE_E];
+    double ax[PIPE_T];
+    double v[PIPE_E];
+};
+
+__host__ __device__ constexpr size_t pipe_smem_bytes()
+{
+    return 3 * sizeof(PipeStage) + 2 * PIPE_WIN * sizeof(double) + PIPE_RING * (sizeof(TileDesc) + sizeof(int));
+}
+
+__device__ __forceinline__ unsigned pipe_smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void pipe_cp4(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(pipe_smem_u32(dst)), "l"(src));
+}
+__device__ __forceinline__ void pipe_cp8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(pipe_smem_u32(dst)), "l"(src));
+}
+__device__ __forceinline__ void pipe_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void pipe_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// stage a: the tile's term words and entry records
+__device__ __forceinline__ void pipe_stage_a(PipeStage &st, const TileDesc &D, int nent, const ProdSched &S)
+{
+    for (int u = threadIdx.x; u < D.nterms; u += PIPE_NT) pipe_cp4(&st.w[u], S.W + D.word_begin + u);
+    for (int e = threadIdx.x; e < nent; e += PIPE_NT) pipe_cp8(&st.es[e], S.ES + D.vbase + e);
+}
+
+// stage b: A.x of every term and V of every entry, addressed by the staged records;
+// the thread's words are kept for the compute step
+__device__ __forceinline__ void pipe_stage_b(PipeStage &st, const TileDesc &D, int nent, const double *Ax,
+                                             const double *V, unsigned (&w)[PIPE_RU])
+{
+#pragma unroll
+    for (int j = 0; j < PIPE_RU; ++j)
+    {
+        const int u = threadIdx.x + j * PIPE_NT;
+        w[j] = u < D.nterms ? st.w[u] : (TERM_LIST << 12); // a list word is skipped by the term step
+        if (u < D.nterms) pipe_cp8(&st.ax[u], Ax + st.es[w[j] >> 14].x + u);
+    }
+    for (int e = threadIdx.x; e < nent; e += PIPE_NT)
+    {
+        if (V)
+            pipe_cp8(&st.v[e], V + st.es[e].y);
+        else
+            st.v[e] = 1.0;
+    }
+}
+
+__global__ void __launch_bounds__(PIPE_NT, 2) k_tile_refill_pipe(const TileDesc *__restrict__ tiles, int ntiles,
+                                                                 const int *__restrict__ nent_of, ProdPtrs P1,
+                                                                 ProdSched S1, int *__restrict__ err)
+{
+    extern __shared__ __align__(16) unsigned char psm[];
+    PipeStage *st = reinterpret_cast<PipeStage *>(psm);
+    double *wins = reinterpret_cast<double *>(psm + 3 * sizeof(PipeStage));
+    TileDesc *dsc = reinterpret_cast<TileDesc *>(wins + 2 * PIPE_WIN);
+    int *nent_r = reinterpret_cast<int *>(dsc + PIPE_RING);
+    const int tid = threadIdx.x, G = gridDim.x;
+    int t = blockIdx.x;
+    if (t >= ntiles) return;
+    const double *V = (P1.Lx || P1.d) ? S1.V : nullptr;
+    auto load_desc = [&](int slot, int tile) {
+        if (tid < (int)(sizeof(TileDesc) / 4))
+            reinterpret_cast<int *>(dsc + slot)[tid] = reinterpret_cast<const int *>(tiles + tile)[tid];
+        else if (tid == (int)(sizeof(TileDesc) / 4))
+            nent_r[slot] = nent_of[tile];
+    };
+    for (int i = tid; i < 2 * PIPE_WIN; i += PIPE_NT) wins[i] = 0.0;
+    load_desc(0, t);
+    if (t + G < ntiles) load_desc(1, t + G);
+    if (t + 2 * G < ntiles) load_desc(2, t + 2 * G);
+    __syncthreads();
+    pipe_stage_a(st[0], dsc[0], nent_r[0], S1);
+    pipe_commit();
+    if (t + G < ntiles) pipe_stage_a(st[1], dsc[1], nent_r[1], S1);
+    pipe_commit();
+    // launched as a programmatic dependent of the entry-value kernel: V is read only
+    // after that grid completed (a no-op for an ordinary launch)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    pipe_wait_all();
+    __syncthreads();
+    unsigned w[PIPE_RU];
+    pipe_stage_b(st[0], dsc[0], nent_r[0], P1.Ax, V, w);
+    pipe_commit();
+    for (int k = 0;; ++k)
+    {
+        const bool has1 = t + G < ntiles, has2 = t + 2 * G < ntiles;
+        if (t + 3 * G < ntiles) load_desc((k + 3) & (PIPE_RING - 1), t + 3 * G);
+        // stage b of this tile and stage a of the next have landed; the descriptor
+        // copied last step is visible
+        pipe_wait_all();
+        __syncthreads();
+        if (has2) pipe_stage_a(st[(k + 2) % 3], dsc[(k + 2) & (PIPE_RING - 1)], nent_r[(k + 2) & (PIPE_RING - 1)], S1);
+        pipe_commit();
+        unsigned wn[PIPE_RU];
+#pragma unroll
+        for (int j = 0; j < PIPE_RU; ++j) wn[j] = TERM_LIST << 12;
+        if (has1)
+            pipe_stage_b(st[(k + 1) % 3], dsc[(k + 1) & (PIPE_RING - 1)], nent_r[(k + 1) & (PIPE_RING - 1)], P1.Ax,
+                         V, wn);
+        pipe_commit();
+        const TileDesc &D = dsc[k & (PIPE_RING - 1)];
+        const PipeStage &cs = st[k % 3];
+        double *win = wins + (k & 1) * PIPE_WIN;
+#pragma unroll
+        for (int j = 0; j < PIPE_RU; ++j)
+        {
+            if (w[j] & (TERM_LIST << 12)) continue;
+            const int u = tid + j * PIPE_NT;
+            const int p = (int)(w[j] & 0xfffu);
+            const double prod = __dmul_rn(cs.v[w[j] >> 14], cs.ax[u]);
+            if (w[j] & (TERM_PAIR << 12))
+                atomicAdd(&win[p], prod);
+            else
+                win[p] = __dadd_rn(0.0, prod);
+        }
+        __syncthreads(); // the window is complete
+        if (D.nlist > 0)
+        {
+            const unsigned *hdr = S1.X + D.x_begin;
+            const unsigned *items = hdr + D.nlist + 1;
+            for (int l = tid; l < D.nlist; l += PIPE_NT)
+            {
+                const unsigned h = hdr[l];
+                const int p = (int)(h & 0xfffu);
+                double acc = 0.0;
+                for (int i = (int)(h >> 12); i < (int)(hdr[l + 1] >> 12); ++i)
+                {
+                    const int u = (int)items[i];
+                    if ((unsigned)u >= (unsigned)D.nterms)
+                    {
+                        atomicOr(err, 1);
+                        continue;
+                    }
+                    acc = __dadd_rn(acc, __dmul_rn(cs.v[cs.w[u] >> 14], cs.ax[u]));
+                }
+                if (p < D.nout)
+                    win[p] = acc;
+                else
+                    atomicOr(err, 1);
+            }
+            __syncthreads();
+        }
+        double *C = P1.Cx + D.out_begin;
+        const int nout = D.nout;
+        if ((reinterpret_cast<uintptr_t>(C) & 15) == 0)
+        {
+            double2 *C2 = reinterpret_cast<double2 *>(C);
+            double2 *w2 = reinterpret_cast<double2 *>(win);
+            for (int o = tid; o < (nout >> 1); o += PIPE_NT)
+            {
+                C2[o] = w2[o];
+                w2[o] = make_double2(0.0, 0.0);
+            }
+            if ((nout & 1) && tid == 0)
+            {
+                C[nout - 1] = win[nout - 1];
+                win[nout - 1] = 0.0;
+            }
+        }
+        else
+            for (int o = tid; o < nout; o += PIPE_NT)
+            {
+                C[o] = win[o];
+                win[o] = 0.0;
+            }
+        if (!has1) break;
+        t += G;
+#pragma unroll
+        for (int j = 0; j < PIPE_RU; ++j) w[j] = wn[j];
+    }
+    pipe_wait_all();
+}
+
 // Value pointers from a device binding table (batched refills replayed from a CUDA
 // graph read the pointers bound at replay time), when given.
 __device__ __forceinline__ void bind_values(NumArgs &a, const ProdPtrs *__restrict__ vals)
@@ -1957,6 +2157,31 @@ __global__ void k_tile_max_out(const TileDesc *__restrict__ tiles, int ntiles, i
     atomicMax(out, m);
 }
 
+// Entries of every tile (its largest entry index + 1, from its term words; entry
+// indices grow along a tile's words) and the largest term and entry counts of a tile.
+__global__ void k_tile_nent(const TileDesc *__restrict__ tiles, int ntiles, const unsigned *__restrict__ W,
+                            int *__restrict__ nent, int *__restrict__ mx)
+{
+    const int lane = lane_id(), wpb = blockDim.x >> 5;
+    int mt = 0, me = 0;
+    for (long long t = blockIdx.x * (long long)wpb + (threadIdx.x >> 5); t < ntiles; t += (long long)gridDim.x * wpb)
+    {
+        const TileDesc D = tiles[t];
+        int e = -1;
+        for (int u = lane; u < D.nterms; u += 32) e = max(e, (int)(W[D.word_begin + u] >> 14));
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) e = max(e, __shfl_xor_sync(FULL_MASK, e, o));
+        if (lane == 0) nent[t] = e + 1;
+        mt = max(mt, D.nterms);
+        me = max(me, e + 1);
+    }
+    if (lane == 0)
+    {
+        atomicMax(&mx[0], mt);
+        atomicMax(&mx[1], me);
+    }
+}
+
 // Everything the refill needs once C's structure is known: row classes, the
 // compiled tile schedule and the larger rows' scratch.
 void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
@@ -2036,7 +2261,16 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
         SDL_LAUNCH(k_tile_max_out, grid_for(P.ntiles, 256, rt.num_sms * 4), 256, 0, s, P.tiles.get(), P.ntiles,
                    mo.get());
         SDL_CUDA(cudaMemcpyAsync(&P.max_tile_out, mo.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        P.tile_nent.reset((size_t)P.ntiles);
+        DevBuf<int> mx(2);
+        SDL_CUDA(cudaMemsetAsync(mx.get(), 0, mx.bytes(), s));
+        SDL_LAUNCH(k_tile_nent, grid_for(P.ntiles, 8, rt.num_sms * 8), 256, 0, s, P.tiles.get(), P.ntiles, P.W.get(),
+                   P.tile_nent.get(), mx.get());
+        int hmx[2] = {0, 0};
+        SDL_CUDA(cudaMemcpyAsync(hmx, mx.get(), sizeof(hmx), cudaMemcpyDeviceToHost, s));
         SDL_CUDA(cudaStreamSynchronize(s));
+        P.max_tile_terms = hmx[0];
+        P.max_tile_ent = hmx[1];
     }
     build_big_lists(d, P, ub, na, s);
     if (P.num_count[NUM_GMEM] && !P.big_lists)
@@ -2544,6 +2778,39 @@ bool small_tile_refill(const Product &P)
     return P.cfg.refill_threads == REFILL_THREADS_SMALL && P.max_tile_out <= win_of<REFILL_THREADS_SMALL>();
 }
 
+bool pipe_refill(const Product &P)
+{
+    return P.cfg.refill_pipe && P.ntiles > 0 && P.max_tile_terms <= PIPE_T && P.max_tile_ent <= PIPE_E &&
+           P.max_tile_out <= PIPE_WIN;
+}
+
+void launch_refill_pipe(const Product &P, cudaStream_t s, const ProdPtrs &vals, const ProdSched &sched)
+{
+    static int per_sm = 0;
+    if (!per_sm)
+    {
+        set_smem(k_tile_refill_pipe, pipe_smem_bytes());
+        int n = 0;
+        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill_pipe, PIPE_NT, pipe_smem_bytes()));
+        per_sm = std::max(1, n);
+    }
+    const int use = P.cfg.refill_ctas_per_sm > 0 ? std::min(P.cfg.refill_ctas_per_sm, per_sm) : per_sm;
+    const int grid = std::min(P.ntiles, runtime().num_sms * use);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(PIPE_NT);
+    cfg.dynamicSmemBytes = pipe_smem_bytes();
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill_pipe, (const TileDesc *)P.tiles.get(), P.ntiles,
+                                (const int *)P.tile_nent.get(), vals, sched, runtime().d_error));
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
                  cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm, bool small)
 {
@@ -2652,8 +2919,11 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
     if (P.num_count[NUM_TILE])
     {
         if (!direct) entry_values(S, vals, s);
-        tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm,
-                    small_tile_refill(P));
+        if (pipe_refill(P))
+            launch_refill_pipe(P, s, vals, S);
+        else
+            tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm,
+                        small_tile_refill(P));
     }
     if (P.big_lists)
     {
@@ -2838,7 +3108,17 @@ TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
         build(c, Q);
         if (small_tile_refill(Q))
         {
-            const double us = refill_us(Q);
+            // the pipelined refill (when the tiles fit its stages) and the direct one
+            double us = refill_us(Q);
+            if (pipe_refill(Q))
+            {
+                Q.cfg.refill_pipe = 0;
+                const double us_direct = refill_us(Q);
+                if (us_direct < us)
+                    us = us_direct;
+                else
+                    Q.cfg.refill_pipe = 1;
+            }
             if (us < best_us)
             {
                 best_us = us;

@@ -274,6 +274,9 @@ struct TuneConfig
     // outputs (tile budget and tile_max_terms at most TILE_T / 2)
     int tile_max_terms = 0;
     int refill_threads = 256;
+    // the pipelined refill (tile data staged ahead by asynchronous copies) for plans
+    // whose tiles all fit its stages (1), or the direct one (0)
+    int refill_pipe = 1;
 };
 // Autotuner results: the chosen configuration and what it measured.
 struct TuneResult
@@ -308,6 +311,8 @@ struct Product
     // Compiled refill schedule of the tile rows.
     int ntiles = 0;
     int max_tile_out = 0; // largest tile window of the plan
+    int max_tile_terms = 0, max_tile_ent = 0; // largest term / entry count of a tile
+    DevBuf<int> tile_nent; // entries of every tile
     DevBuf<TileDesc> tiles;
     DevBuf<unsigned> W, X; // term words, list sections
     DevBuf<int2> ES;       // per entry: {A.p[k] - tile term offset, V slot} (L_nnz * blocks)
@@ -397,6 +402,9 @@ void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const 
                  int ctas_per_sm = 0, bool small = false);
 // Whether a single product's refill runs the 128-thread small-tile kernel.
 bool small_tile_refill(const Product &P);
+// Whether P's tiles are refilled by the pipelined kernel (its configuration asks for
+// it and every tile fits the kernel's stages).
+bool pipe_refill(const Product &P);
 // Whether a product's entry values are L.x itself (no d, one block, values in L's
 // value order or no L_map): the refill then reads L.x and skips the entry values.
 bool entry_values_are_lx(const Product &P, const double *Lx, const double *dvec);

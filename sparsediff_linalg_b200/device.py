@@ -102,6 +102,13 @@ class Product:
         check(lib().sdl_product_pattern_key(self.handle, buf, 512, _stream(stream)))
         return buf.value.decode()
 
+    def set_refill_pipe(self, on):
+        """Pipelined (True) or direct (False) tile refill; returns whether the
+        pipelined refill will run for this plan."""
+        used = C.c_int()
+        check(lib().sdl_product_set_refill_pipe(self.handle, 1 if on else 0, C.byref(used)))
+        return bool(used.value)
+
     def refill_shape(self):
         th, tm = C.c_int(), C.c_int()
         check(lib().sdl_product_refill_shape(self.handle, C.byref(th), C.byref(tm)))
