@@ -136,9 +136,11 @@ sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, i
    so computing a tile reads shared memory only), used when every tile of the plan
    holds at most 1024 terms, 512 entries and 1024 outputs (plans of at most 512-term
    tiles, which sdl_product_replan and the autotuner make), or the direct one
-   (on = 0). Both give the same bits. *used (may be NULL) reports whether the
-   pipelined refill will run. */
+   (on = 0, the default; the autotuner times both). Both give the same bits. *used
+   (may be NULL) reports whether the pipelined refill will run. */
 sdl_status sdl_product_set_refill_pipe(sdl_product *P, int on, int *used);
+/* Whether P's tiles are refilled by the pipelined refill (1) or the direct one (0). */
+sdl_status sdl_product_refill_pipe_used(const sdl_product *P, int *used);
 
 /* No upstream counterpart (it generalises upstream's fixed plan-vs-accumulator
    threshold GUSTAVSON_PLAN_MAX_RATIO, src/internal/gustavson.h:52, used at

@@ -178,6 +178,14 @@ extern "C" sdl_status sdl_product_set_refill_pipe(sdl_product *P, int on, int *u
     });
 }
 
+extern "C" sdl_status sdl_product_refill_pipe_used(const sdl_product *P, int *used)
+{
+    return guard_status("sdl_product_refill_pipe_used", [&]() {
+        if (!P || !used) fail(SDL_ERR_INVALID, "NULL argument");
+        *used = pipe_refill(P->P) ? 1 : 0;
+    });
+}
+
 extern "C" sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, int *tile_max_terms)
 {
     return guard_status("sdl_product_refill_shape", [&]() {

@@ -3108,17 +3108,19 @@ TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
         build(c, Q);
         if (small_tile_refill(Q))
         {
-            // the pipelined refill (when the tiles fit its stages) and the direct one
+            // the direct refill and, when the tiles fit its stages, the pipelined one
             double us = refill_us(Q);
+            Q.cfg.refill_pipe = 1;
             if (pipe_refill(Q))
             {
-                Q.cfg.refill_pipe = 0;
-                const double us_direct = refill_us(Q);
-                if (us_direct < us)
-                    us = us_direct;
+                const double us_pipe = refill_us(Q);
+                if (us_pipe < us)
+                    us = us_pipe;
                 else
-                    Q.cfg.refill_pipe = 1;
+                    Q.cfg.refill_pipe = 0;
             }
+            else
+                Q.cfg.refill_pipe = 0;
             if (us < best_us)
             {
                 best_us = us;

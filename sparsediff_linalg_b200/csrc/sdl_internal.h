@@ -275,8 +275,9 @@ struct TuneConfig
     int tile_max_terms = 0;
     int refill_threads = 256;
     // the pipelined refill (tile data staged ahead by asynchronous copies) for plans
-    // whose tiles all fit its stages (1), or the direct one (0)
-    int refill_pipe = 1;
+    // whose tiles all fit its stages (1), or the direct one (0, the default: on the
+    // patterns measured so far the direct refill is faster; the autotuner tries both)
+    int refill_pipe = 0;
 };
 // Autotuner results: the chosen configuration and what it measured.
 struct TuneResult

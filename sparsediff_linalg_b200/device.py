@@ -102,6 +102,11 @@ class Product:
         check(lib().sdl_product_pattern_key(self.handle, buf, 512, _stream(stream)))
         return buf.value.decode()
 
+    def refill_pipelined(self):
+        used = C.c_int()
+        check(lib().sdl_product_refill_pipe_used(self.handle, C.byref(used)))
+        return bool(used.value)
+
     def set_refill_pipe(self, on):
         """Pipelined (True) or direct (False) tile refill; returns whether the
         pipelined refill will run for this plan."""
@@ -123,7 +128,7 @@ class Product:
                                        C.byref(f[2])))
         th, tm = C.c_int(), C.c_int()
         check(lib().sdl_product_refill_shape(self.handle, C.byref(th), C.byref(tm)))
-        return {"warp_max_terms": i[0].value, "rows_per_cta_warp": i[1].value, "tile_budget": i[2].value,
+        return {"refill": "pipelined" if self.refill_pipelined() else "direct", "warp_max_terms": i[0].value, "rows_per_cta_warp": i[1].value, "tile_budget": i[2].value,
                 "refill_ctas_per_sm": i[3].value, "refill_threads": th.value, "tile_max_terms": tm.value,
                 "refill_us": round(f[0].value, 2),
                 "default_refill_us": round(f[1].value, 2), "candidates": i[4].value,
