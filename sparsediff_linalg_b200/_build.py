@@ -72,7 +72,7 @@ def build(verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
     rebuilt = [r for r in rebuilt if r]
     if rebuilt or not LIB_PATH.exists() or any(o.stat().st_mtime > LIB_PATH.stat().st_mtime for o in objs):
         cmd = [_nvcc(), *ARCH, "-shared", "-o", str(LIB_PATH), *map(str, objs),
-               "-Xlinker", "-Bsymbolic", "-lcudart"]
+               "-Xlinker", "-Bsymbolic", "-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

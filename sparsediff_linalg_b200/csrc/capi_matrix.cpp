@@ -146,9 +146,13 @@ void sparse_product_fill(sdl_sparse *Lsrc, const double *d, sdl_sparse *A, sdl_s
     if (op->A_m != A->csr->m || op->A_n != A->csr->n || op->A_nnz != A->csr->nnz ||
         op->L_src_m != Lsrc->csr->m || op->L_src_n != Lsrc->csr->n || op->L_src_nnz != Lsrc->csr->nnz)
         fail(SDL_ERR_INVALID, "operands do not match the ones C was allocated for");
-    const double *Ax = sparse_dev_values(A, s);
-    const double *Lx = sparse_dev_values(Lsrc, s);
-    if (d) h2d(op->dvec.get(), d, A->csr->m, s);
+    const double *Ax, *Lx;
+    {
+        NvtxRange r("sdl: operand values to the device");
+        Ax = sparse_dev_values(A, s);
+        Lx = sparse_dev_values(Lsrc, s);
+        if (d) h2d(op->dvec.get(), d, A->csr->m, s);
+    }
     product_numeric(op->P, Lx, d ? op->dvec.get() : nullptr, Ax, C->impl->vals.x.get(), s);
     publish_output(C, s);
 }
@@ -270,6 +274,7 @@ void wire_sparse(sdl_sparse *sm)
 // Copy the device values of an output into its host CSR and publish them.
 void publish_output(sdl_sparse *C, cudaStream_t s)
 {
+    NvtxRange r("sdl: C.x to the host");
     d2h(C->csr->x, C->impl->vals.x.get(), C->csr->nnz, s);
     check_device_errors(s, "fill");
     matrix_values_changed(&C->base);

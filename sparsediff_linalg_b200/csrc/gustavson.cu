@@ -2186,6 +2186,7 @@ __global__ void k_tile_nent(const TileDesc *__restrict__ tiles, int ntiles, cons
 // compiled tile schedule and the larger rows' scratch.
 void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaStream_t s)
 {
+    NvtxRange nvtx_range_("sdl: refill plan");
     Runtime &rt = runtime();
     const int m_out = P.m_out;
     DevBuf<long long> weight(m_out), wpref((size_t)m_out + 1);
@@ -2366,6 +2367,7 @@ __global__ void k_class_hits(const unsigned char *__restrict__ pcls, const int *
 void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, cudaStream_t s,
                       bool keep_row_terms)
 {
+    NvtxRange nvtx_range_("sdl: symbolic pass");
     Runtime &rt = runtime();
     validate_product(d, cfg, P, s);
     const int m_out = P.m_out;
@@ -2410,6 +2412,7 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
 void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const Mlp &net, float margin,
                               Product &P, LearnedStats &st, cudaStream_t s)
 {
+    NvtxRange nvtx_range_("sdl: learned symbolic pass");
     Runtime &rt = runtime();
     validate_product(d, cfg, P, s);
     const int m_out = P.m_out;
@@ -2537,6 +2540,7 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
                              const double *Lx, const double *dvec, const double *Ax, Product &P,
                              DevBuf<double> &Cx, LearnedStats &st, cudaStream_t s)
 {
+    NvtxRange nvtx_range_("sdl: learned one-shot pass");
     Runtime &rt = runtime();
     validate_product(d, cfg, P, s);
     const int m_out = P.m_out;
@@ -2908,6 +2912,7 @@ bool entry_values_are_lx(const Product &P, const double *Lx, const double *dvec)
 void product_numeric(const Product &P, const double *Lx, const double *dvec, const double *Ax,
                      double *Cx, cudaStream_t s)
 {
+    NvtxRange nvtx_range_("sdl: refill");
     if (!P.plan_ready)
         fail(SDL_ERR_INVALID, "product from the learned one-shot pass: build its refill plan first "
                               "(sdl_product_complete_plan)");

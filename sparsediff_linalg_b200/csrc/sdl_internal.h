@@ -16,9 +16,21 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "sparsediff_linalg_cuda.h"
 
 namespace sdl {
+
+// Named span of a host-side phase (symbolic pass, refill plan, refill, host
+// transfers) on an Nsight Systems timeline; free when no profiler is attached.
+struct NvtxRange
+{
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------------- errors
 struct Error : std::runtime_error
