@@ -270,47 +270,20 @@ void widen_i32(const int *d_src, long long *d_dst, long long n, cudaStream_t s)
 
 // ------------------------------------------------------------------ gather
 namespace {
-// Arrays of at most this many bytes are made L2-resident before they are gathered
-// through a permutation (the B200's L2 holds 126 MB; the streamed positions and
-// output pass through it as well, marked evict-first).
-constexpr size_t GATHER_L2_BYTES = 96u << 20;
-
-// Pulls x into L2 with evict-last priority, one prefetch per 128-byte line.
-__global__ void k_l2_keep(const double *__restrict__ x, long long nlines)
-{
-    for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nlines;
-         l += (long long)gridDim.x * blockDim.x)
-        asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(x + 16 * l));
-}
-
-template <bool KEEP>
-__device__ __forceinline__ double gather_ld(const double *p, unsigned long long pol)
-{
-    if (!KEEP) return *p;
-    double v;
-    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
-    return v;
-}
-
 // out[k] = x[src[k]], four consecutive positions per thread: one 16-byte load of
 // their sources, four independent gathers, two 16-byte stores. The positions and
 // the output are streamed (evict-first), so the gathered array keeps its place in
-// L2 while the permutation revisits it; with KEEP (x was pulled into L2 first) the
-// gathers also carry an evict-last policy. The last n % 4 positions go to the
-// first threads of the grid.
-template <bool KEEP>
+// L2 while the permutation revisits it. The last n % 4 positions go to the first
+// threads of the grid.
 __global__ void k_gather(const int4 *__restrict__ src4, const double *__restrict__ x, double2 *__restrict__ out2,
                          long long n4, const int *__restrict__ src_tail, double *__restrict__ out_tail, int ntail)
 {
-    unsigned long long pol = 0;
-    if (KEEP) asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
     const long long first = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long step = (long long)gridDim.x * blockDim.x;
     for (long long k = first; k < n4; k += step)
     {
         const int4 q = __ldcs(src4 + k);
-        const double a = gather_ld<KEEP>(x + q.x, pol), b = gather_ld<KEEP>(x + q.y, pol),
-                     c = gather_ld<KEEP>(x + q.z, pol), d = gather_ld<KEEP>(x + q.w, pol);
+        const double a = x[q.x], b = x[q.y], c = x[q.z], d = x[q.w];
         __stcs(out2 + 2 * k, make_double2(a, b));
         __stcs(out2 + 2 * k + 1, make_double2(c, d));
     }
@@ -340,19 +313,7 @@ void gather_values(const int *d_src, const double *d_x, double *d_out, int n, cu
     const long long n4 = n / 4;
     const int ntail = n - (int)(4 * n4);
     int grid = (int)std::max<long long>(1, std::min<long long>((n4 + 255) / 256, (long long)rt.num_sms * 8));
-    // a permutation reads every x once (src is a bijection onto x's positions for a
-    // transpose): x spans n doubles, which are made L2-resident first when they fit
-    const size_t xbytes = (size_t)n * sizeof(double);
-    if (xbytes >= (8u << 20) && xbytes <= GATHER_L2_BYTES && ((uintptr_t)d_x & 127) == 0)
-    {
-        const long long nlines = ((long long)n + 15) / 16;
-        SDL_LAUNCH(k_l2_keep, (int)std::min<long long>((nlines + 255) / 256, (long long)rt.num_sms * 8), 256, 0, s,
-                   d_x, nlines);
-        SDL_LAUNCH(k_gather<true>, grid, 256, 0, s, reinterpret_cast<const int4 *>(d_src), d_x,
-                   reinterpret_cast<double2 *>(d_out), n4, d_src + 4 * n4, d_out + 4 * n4, ntail);
-        return;
-    }
-    SDL_LAUNCH(k_gather<false>, grid, 256, 0, s, reinterpret_cast<const int4 *>(d_src), d_x,
+    SDL_LAUNCH(k_gather, grid, 256, 0, s, reinterpret_cast<const int4 *>(d_src), d_x,
                reinterpret_cast<double2 *>(d_out), n4, d_src + 4 * n4, d_out + 4 * n4, ntail);
 }
 

@@ -158,9 +158,7 @@ struct TransposePlan
 };
 void transpose_build(const int *d_p, const int *d_idx, int rows, int cols, int nnz,
                      TransposePlan &out, cudaStream_t s);
-// Tx[q] = x[src[q]] for q < n, where x holds (at least) n values and src is a
-// permutation of [0, n) (every caller gathers through a transpose's or grouping's
-// source map); x may be pulled into L2 whole before the gather.
+// Tx[q] = x[src[q]].
 void gather_values(const int *d_src, const double *d_x, double *d_out, int n,
                    cudaStream_t s);
 
