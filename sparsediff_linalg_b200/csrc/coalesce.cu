@@ -44,13 +44,13 @@ __global__ void k_coal_fill(const int *__restrict__ ostart, const int *__restric
             q0[j] = q1[j] = 0;
             if (o < nout)
             {
-                q0[j] = ostart[o];
-                q1[j] = ostart[o + 1];
+                q0[j] = __ldcs(ostart + o);
+                q1[j] = __ldcs(ostart + o + 1);
             }
         }
         int t[COAL_ILP];
 #pragma unroll
-        for (int j = 0; j < COAL_ILP; ++j) t[j] = q0[j] < q1[j] ? perm[q0[j]] : -1;
+        for (int j = 0; j < COAL_ILP; ++j) t[j] = q0[j] < q1[j] ? __ldcs(perm + q0[j]) : -1;
         double v[COAL_ILP];
 #pragma unroll
         for (int j = 0; j < COAL_ILP; ++j)
@@ -63,10 +63,10 @@ __global__ void k_coal_fill(const int *__restrict__ ostart, const int *__restric
             double acc = __dadd_rn(0.0, v[j]);
             for (int q = q0[j] + 1; q < q1[j]; ++q)
             {
-                const int tq = perm[q];
+                const int tq = __ldcs(perm + q);
                 acc = __dadd_rn(acc, f ? __dmul_rn(f[tq], x[tq]) : x[tq]);
             }
-            C[o] = acc;
+            __stcs(C + o, acc);
         }
     }
 }
@@ -280,25 +280,42 @@ __global__ void k_cb_perm2(const int *__restrict__ perm, const int *__restrict__
 __global__ void __launch_bounds__(CO_THREADS) k_cb_scatter(const double *__restrict__ x, const double *__restrict__ f,
                                                           int n, int nb, const unsigned short *__restrict__ lperm,
                                                           const int *__restrict__ cbound,
-                                                          const long long *__restrict__ dst, int nchunks,
+                                                          const long long *__restrict__ dstc,
                                                           double *__restrict__ buf)
 {
     __shared__ double xs[CO_CHUNK];
     __shared__ int bs[CO_MAX_BUCKETS + 1];
+    __shared__ long long ds[CO_MAX_BUCKETS];
+    __shared__ unsigned short lp[CO_CHUNK];
     const int c = blockIdx.x;
     const long long t0 = (long long)c * CO_CHUNK;
     const int cnt = (int)(n - t0 < CO_CHUNK ? n - t0 : CO_CHUNK);
     for (int i = threadIdx.x; i < cnt; i += CO_THREADS)
+    {
         xs[i] = f ? __dmul_rn(__ldcs(f + t0 + i), __ldcs(x + t0 + i)) : __ldcs(x + t0 + i);
+        lp[i] = __ldcs(lperm + t0 + i);
+    }
     for (int b = threadIdx.x; b <= nb; b += CO_THREADS) bs[b] = __ldcs(cbound + (long long)c * (nb + 1) + b);
+    for (int b = threadIdx.x; b < nb; b += CO_THREADS) ds[b] = __ldcs(dstc + (long long)c * nb + b);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int b = warp; b < nb; b += CO_THREADS / 32)
     {
         const int i0 = bs[b], i1 = bs[b + 1];
         if (i0 == i1) continue;
-        double *out = buf + dst[(long long)b * nchunks + c];
-        for (int i = i0 + lane; i < i1; i += 32) out[i - i0] = xs[__ldcs(lperm + t0 + i)];
+        double *out = buf + ds[b];
+        for (int i = i0 + lane; i < i1; i += 32) out[i - i0] = xs[lp[i]];
+    }
+}
+
+// Chunk-major copy of the bucket-major run offsets (what a chunk's CTA reads).
+__global__ void k_cb_transpose_dst(const long long *__restrict__ dst, int nb, int nchunks, long long *__restrict__ dstc)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < (long long)nb * nchunks;
+         k += (long long)gridDim.x * blockDim.x)
+    {
+        const long long b = k / nchunks, c = k - b * nchunks;
+        dstc[c * nb + b] = dst[k];
     }
 }
 } // namespace
@@ -329,6 +346,11 @@ void coalesce_bucket_build(const int *ostart, const int *perm, int n, int nout, 
     B.perm2.reset((size_t)n);
     SDL_LAUNCH(k_cb_perm2, grid_coal(n, 256), 256, 0, s, perm, owner.get(), rank.get(), B.dst.get(), n, span,
                nchunks, B.perm2.get());
+    // the scatter reads every chunk's run offsets in one piece
+    DevBuf<long long> dstc((size_t)nb * nchunks);
+    SDL_LAUNCH(k_cb_transpose_dst, grid_coal((long long)nb * nchunks, 256), 256, 0, s, B.dst.get(), nb, nchunks,
+               dstc.get());
+    B.dst = std::move(dstc);
     B.buf.reset((size_t)n);
     B.nb = nb;
     B.nchunks = nchunks;
@@ -341,8 +363,11 @@ void coalesce_bucket_fill(const CoalesceBuckets &B, const int *ostart, const dou
                           double *C, cudaStream_t s)
 {
     SDL_LAUNCH(k_cb_scatter, B.nchunks, CO_THREADS, 0, s, x, f, B.n, B.nb, B.lperm.get(), B.cbound.get(), B.dst.get(),
-               B.nchunks, B.buf.get());
-    SDL_LAUNCH(k_coal_fill, grid_coal(nout, 256), 256, 0, s, ostart, B.perm2.get(), B.buf.get(), nullptr, nout, C);
+               B.buf.get());
+    // few outputs in flight (148 x 8 CTAs x 256 threads x 4 outputs: about eight
+    // buckets), so the buckets being summed stay in L2
+    const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)nout + 255) / 256, 148LL * 8));
+    SDL_LAUNCH(k_coal_fill, grid, 256, 0, s, ostart, B.perm2.get(), B.buf.get(), nullptr, nout, C);
 }
 
 } // namespace sdl

@@ -1661,7 +1661,8 @@ __host__ __device__ constexpr size_t gmem_smem_bytes()
 // ascending term order (upstream's visiting order), whichever threads hold them.
 __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
                                                           int *__restrict__ posmap_all, int n,
-                                                          const ProdPtrs *__restrict__ vals)
+                                                          const ProdPtrs *__restrict__ vals,
+                                                          int *__restrict__ next_row)
 {
     bind_values(a, vals);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -1672,8 +1673,19 @@ __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(con
     int *claim = elen + GMEM_CHUNK;
     int *scr = claim + GMEM_CLAIM;
     int *posmap = posmap_all + (long long)blockIdx.x * n;
-    for (int it = blockIdx.x; it < count; it += gridDim.x)
+    __shared__ int it_sh;
+    // rows taken in list order: from a shared counter when given (the list is then
+    // ordered by work, largest first), else every gridDim-th
+    for (int it = blockIdx.x;;)
     {
+        if (next_row)
+        {
+            __syncthreads();
+            if (threadIdx.x == 0) it_sh = atomicAdd(next_row, 1);
+            __syncthreads();
+            it = it_sh;
+        }
+        if (it >= count) break;
         int row = rows[it];
         int b = row / a.L_m, r = row - b * a.L_m;
         int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
@@ -1774,6 +1786,7 @@ __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(con
             __syncthreads();
         }
         __syncthreads();
+        if (!next_row) it += gridDim.x;
     }
 }
 
@@ -2640,10 +2653,25 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
         DevBuf<int> posmap((size_t)slots * per_slot);
         NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(), Cx.get(),
                    rt.d_error};
+        // the large rows by term count, largest first, handed out by a counter: the
+        // largest rows start first and no CTA is left with several of them
+        const int nbr = cnt[SYM_BITMAP];
+        std::vector<int> hrows(nbr);
+        std::vector<long long> hub(m_out);
+        SDL_CUDA(cudaMemcpyAsync(hrows.data(), lists.get() + off[SYM_BITMAP], (size_t)nbr * sizeof(int),
+                                 cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaMemcpyAsync(hub.data(), P.row_terms.get() ? P.row_terms.get() : ub.get(),
+                                 (size_t)m_out * sizeof(long long), cudaMemcpyDeviceToHost, s));
+        SDL_CUDA(cudaStreamSynchronize(s));
+        std::stable_sort(hrows.begin(), hrows.end(), [&](int x, int y) { return hub[x] > hub[y]; });
+        DevBuf<int> order((size_t)nbr), counter(1);
+        SDL_CUDA(cudaMemcpyAsync(order.get(), hrows.data(), (size_t)nbr * sizeof(int), cudaMemcpyHostToDevice, s));
+        SDL_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(int), s));
         const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
-        SDL_LAUNCH(k_num_gmem, slots, GMEM_THREADS, sm, s, lists.get() + off[SYM_BITMAP], cnt[SYM_BITMAP], na, posmap.get(),
-                   P.n, nullptr);
+        SDL_LAUNCH(k_num_gmem, slots, GMEM_THREADS, sm, s, order.get(), nbr, na, posmap.get(), P.n, nullptr,
+                   counter.get());
+        SDL_CUDA(cudaStreamSynchronize(s)); // hrows / hub and the queue are freed on return
         if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "one-shot product: a term column is missing from its row");
     }
     {
@@ -2860,7 +2888,7 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
         const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
         SDL_LAUNCH(k_num_gmem, P.gmem_slots, th, sm, s, rows + off[NUM_GMEM], cnt[NUM_GMEM], na,
-                   P.gmem_scratch.get(), P.n, vals);
+                   P.gmem_scratch.get(), P.n, vals, nullptr);
     }
 }
 
@@ -2897,7 +2925,7 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
         const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
         SDL_LAUNCH(k_num_gmem, std::min(slots, cnt[NUM_GMEM]), th, sm, s, rows + off[NUM_GMEM],
-                   cnt[NUM_GMEM], na, posmap, P.n, nullptr);
+                   cnt[NUM_GMEM], na, posmap, P.n, nullptr, nullptr);
     }
 }
 

@@ -167,7 +167,7 @@ void gather_values(const int *d_src, const double *d_x, double *d_out, int n,
 // COALESCE_BUCKET_MIN triplets the refill first writes the values, chunk by chunk,
 // into output-range buckets (lperm: each chunk's triplets in bucket order; cbound:
 // each bucket's first position in a chunk's order, nb + 1 per chunk; dst: start of
-// every (bucket, chunk) run in buf, bucket-major), then sums every output from its
+// every (chunk, bucket) run in buf, chunk-major), then sums every output from its
 // bucket (perm2: the buf position of every output-order slot). buf is the plan's
 // refill scratch.
 constexpr int COALESCE_BUCKET_MIN = 1 << 22;
