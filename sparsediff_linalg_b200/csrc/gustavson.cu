@@ -1912,9 +1912,12 @@ __global__ void k_big_sizes(const int *__restrict__ rows, int nbig, const long l
 // = its output's index among all big-row outputs and its {A position, entry-value
 // slot}. Output positions come from a per-CTA global map column -> position; only
 // the row's own columns are ever read, so it needs no clearing.
-__global__ void k_big_terms(const int *__restrict__ rows, int nbig, const int *__restrict__ tterm_off,
-                            const int *__restrict__ bout_off, NumArgs a, int *__restrict__ posmap_all, int n,
-                            unsigned *__restrict__ keys, uint2 *__restrict__ data)
+__global__ void __launch_bounds__(512, 2) k_big_terms(const int *__restrict__ rows, int nbig,
+                                                      const int *__restrict__ tterm_off,
+                                                      const int *__restrict__ bout_off, NumArgs a,
+                                                      int *__restrict__ posmap_all, int n,
+                                                      unsigned *__restrict__ keys, uint2 *__restrict__ data,
+                                                      const int *__restrict__ order, int *__restrict__ next_row)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     CtaChunk ch;
@@ -1924,8 +1927,15 @@ __global__ void k_big_terms(const int *__restrict__ rows, int nbig, const int *_
     ch.len = ch.s + blockDim.x;
     ch.scr = ch.len + blockDim.x;
     int *posmap = posmap_all + (long long)blockIdx.x * n;
-    for (int it = blockIdx.x; it < nbig; it += gridDim.x)
+    __shared__ int q_sh;
+    // the rows in the order `order` gives (largest first), handed out by a counter
+    for (;;)
     {
+        __syncthreads();
+        if (threadIdx.x == 0) q_sh = atomicAdd(next_row, 1);
+        __syncthreads();
+        if (q_sh >= nbig) break;
+        const int it = order[q_sh];
         const int row = rows[it];
         const int b = row / a.L_m, r = row - b * a.L_m;
         const int cs = a.Cp[row], nr = a.Cp[row + 1] - cs;
@@ -2074,8 +2084,19 @@ void build_big_lists(const ProductDesc &d, Product &P, const long long *ub, cons
     SDL_CUDA(cudaMemcpyAsync(P.bout_off.get(), hoi.data(), hoi.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     // terms -> (output, pair), then a stable sort by output
     const long long per_slot = std::max(1, P.n);
-    const int slots = (int)std::min<long long>({(long long)rt.num_sms, std::max<long long>(1, (2LL << 30) / (per_slot * 4)),
-                                                (long long)nbig});
+    const int slots = (int)std::min<long long>(
+        {(long long)rt.num_sms * 2, std::max<long long>(1, (2LL << 30) / (per_slot * 4)), (long long)nbig});
+    // the rows by term count, largest first (a counter hands them out)
+    std::vector<int> ord(nbig);
+    {
+        std::vector<long long> tc(nbig);
+        for (int i = 0; i < nbig; ++i) tc[i] = ht[i + 1] - ht[i];
+        for (int i = 0; i < nbig; ++i) ord[i] = i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return tc[x] > tc[y]; });
+    }
+    DevBuf<int> order((size_t)nbig), counter(1);
+    SDL_CUDA(cudaMemcpyAsync(order.get(), ord.data(), (size_t)nbig * sizeof(int), cudaMemcpyHostToDevice, s));
+    SDL_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(int), s));
     {
         DevBuf<int> posmap((size_t)slots * per_slot);
         DevBuf<unsigned> keys(std::max<long long>(1, T)), keys2(std::max<long long>(1, T));
@@ -2084,7 +2105,7 @@ void build_big_lists(const ProductDesc &d, Product &P, const long long *ub, cons
         const int th = 512;
         const size_t sm = (3 * (size_t)th + 32) * 4;
         SDL_LAUNCH(k_big_terms, slots, th, sm, s, rows, nbig, toff32.get(), P.bout_off.get(), na, posmap.get(), P.n,
-                   keys.get(), P.bpairs.get());
+                   keys.get(), P.bpairs.get(), order.get(), counter.get());
         if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "product plan: a term column is missing from its row");
         int bits = 1;
         while (bits < 32 && (1LL << bits) < O) ++bits;
