@@ -568,19 +568,48 @@ def run_e2e(args, A, B, d, A2x, B2x, d2, B_alg, allmax, barrier, world, check=Fa
         Cm.BTDA_fill(Am, dd, Bm)
     torch.cuda.synchronize()
     barrier()
+    t_set, t_fill = [], []
     t0 = time.perf_counter()
     for k in range(args.steps):
         ax, bx, dd = vals[k % 2]
+        ta = time.perf_counter()
         Am.set_values(ax)       # host write + matrix_values_changed, as a caller does
         Bm.set_values(bx)
+        tb = time.perf_counter()
         Cm.BTDA_fill(Am, dd, Bm)  # returns with C.x current on the host
+        t_set.append(tb - ta)
+        t_fill.append(time.perf_counter() - tb)
     t = (time.perf_counter() - t0) / args.steps
     t = allmax(t)
     h2d = 8 * (len(A[1]) + len(B[1]) + A[3])
     d2h = 8 * Cm.nnz
+    # the host link on this box: page-locked copies of the step's byte counts
+    link = {}
+    hb = torch.empty(max(h2d, d2h) // 8, dtype=torch.float64).pin_memory()
+    db = torch.empty_like(hb, device="cuda")
+    for name, nbytes, fn in (("h2d", h2d, lambda n: db[:n].copy_(hb[:n], non_blocking=True)),
+                             ("d2h", d2h, lambda n: hb[:n].copy_(db[:n], non_blocking=True))):
+        n = nbytes // 8
+        fn(n)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            fn(n)
+        e1.record()
+        torch.cuda.synchronize()
+        link[name] = e0.elapsed_time(e1) / 5
+    del hb, db
     out = {"value": round(world * B_alg / t / 1e9, 3), "unit": "GB/s",
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "ms_per_step": round(t * 1e3, 4),
+           "phases_ms": {"caller_host_writes": round(statistics.median(t_set) * 1e3, 3),
+                         "library_fill": round(statistics.median(t_fill) * 1e3, 3),
+                         "link_floor": round(link["h2d"] + link["d2h"], 3),
+                         "link_gbs": {"h2d": round(h2d / link["h2d"] / 1e6, 1),
+                                      "d2h": round(d2h / link["d2h"] / 1e6, 1)}},
+           "phases_note": "library_fill = operand uploads + refill + C.x download inside one call; link_floor = "
+                          "the same bytes copied between page-locked host memory and the device on this box",
            "api": "BTDA_matrices_fill_values (host value arrays from the library's constructors, "
                   "page-locked in place on their first transfer; d a caller-owned host array)"}
     if check:
@@ -664,6 +693,15 @@ def run_batched(args, dev, world=1, rank=0, barrier=lambda: None, allmax=lambda 
         s.synchronize()
         return allmax(sum(a.elapsed_time(b) for a, b in evs) / refills)
 
+    tuned = None
+    if not args.no_autotune:
+        # the group size picked by timing the candidates before the graph exists
+        bind(0)
+        t0 = time.perf_counter()
+        gb, ms_t = Bt.autotune(reps=3, stream=s)
+        s.synchronize()
+        tuned = {"group_bytes": gb, "refill_ms": round(ms_t, 4), "candidates_mib": [16, 32, 64, 128, 256, "one group"],
+                 "tune_s": round(time.perf_counter() - t0, 2)}
     for w in range(3):
         bind(w % 2)
         with torch.cuda.stream(s):
@@ -686,6 +724,8 @@ def run_batched(args, dev, world=1, rank=0, barrier=lambda: None, allmax=lambda 
            "plain_gbs": round(B_all / (ms_plain * 1e-3) / 1e9, 2),
            "speedup_vs_plain": round(ms_plain / ms_batched, 3),
            "generate_s": round(gen_s, 2), "symbolic_s": round(sym_s, 2)}
+    if tuned is not None:
+        out["autotune"] = tuned
     if world > 1:
         out["ranks"] = world
         out["partition"] = "products by term count (LPT), no collective on the data path; time = max over ranks"

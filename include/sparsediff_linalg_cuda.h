@@ -201,6 +201,14 @@ sdl_status sdl_batch_bind(sdl_batch *B, int i, const double *Lx, const double *d
 sdl_status sdl_batch_set_group_bytes(sdl_batch *B, long long bytes);
 /* Number of product groups of the batch. */
 sdl_status sdl_batch_groups(const sdl_batch *B, int *groups);
+/* No upstream counterpart: the batch's autotuner. Before the batch's first refill
+   (its graph does not exist yet) and with every product bound, times `reps`
+   refills (eagerly, on `stream`, which must not be the legacy default stream) at
+   each candidate group size -- 16, 32, 64, 128, 256 MiB of entry values and
+   records per group, and one group -- and keeps the fastest. Reports the chosen
+   size (0: one group) and its milliseconds per refill (either pointer may be
+   NULL). The refills it runs write the bound outputs. */
+sdl_status sdl_batch_autotune(sdl_batch *B, int reps, void *stream, long long *group_bytes, double *ms);
 /* One refill of every product of the batch, asynchronous on the stream. */
 sdl_status sdl_batch_refill(sdl_batch *B, void *stream);
 /* The same refill as sdl_batch_refill done the plain way: one sdl_product_fill

@@ -200,41 +200,96 @@ extern "C" sdl_status sdl_batch_bind(sdl_batch *B, int i, const double *Lx, cons
     });
 }
 
+namespace {
+// One refill of the batch, enqueued on s: per group, the entry values of its products
+// on the side stream (after the refill of group g - 2, so they run at most one group
+// ahead), then the group's tiles on s; then the rows beyond the tile budget.
+void batch_enqueue(sdl_batch &Bq, cudaStream_t s)
+{
+    sdl_batch *B = &Bq;
+    SDL_CUDA(cudaEventRecord(B->fork, s));
+    SDL_CUDA(cudaStreamWaitEvent(B->side, B->fork, 0));
+    for (size_t g = 0; g < B->entry_done.size(); ++g)
+    {
+        const int c0 = B->group_chunks[g], t0 = B->group_tiles[g];
+        if (g >= 2) SDL_CUDA(cudaStreamWaitEvent(B->side, B->refill_done[g - 2], 0));
+        entry_values_batched(B->chunks.get() + c0, B->group_chunks[g + 1] - c0, B->ptrs.get(), B->scheds.get(),
+                             B->side);
+        SDL_CUDA(cudaEventRecord(B->entry_done[g], B->side));
+        SDL_CUDA(cudaStreamWaitEvent(s, B->entry_done[g], 0));
+        tile_refill(B->tiles.get() + t0, B->group_tiles[g + 1] - t0, B->ptrs.get(), B->scheds.get(), s);
+        SDL_CUDA(cudaEventRecord(B->refill_done[g], s));
+    }
+    SDL_CUDA(cudaEventRecord(B->join, B->side));
+    SDL_CUDA(cudaStreamWaitEvent(s, B->join, 0));
+    for (int i : B->with_big)
+    {
+        const ProdPtrs &pp = B->host_ptrs[i];
+        if (B->prods[i]->big_lists)
+            big_lists_refill(*B->prods[i], B->ptrs.get() + i, s);
+        else
+            big_rows_refill(*B->prods[i], pp.Lx, pp.d, pp.Ax, pp.Cx, s, B->ptrs.get() + i);
+    }
+}
+
+void check_bound(const sdl_batch &B)
+{
+    for (size_t i = 0; i < B.prods.size(); ++i)
+        if (B.prods[i]->nnz > 0 && !B.host_ptrs[i].Cx)
+            fail(SDL_ERR_INVALID, "product " + std::to_string(i) + " has no bound values");
+}
+} // namespace
+
+extern "C" sdl_status sdl_batch_autotune(sdl_batch *B, int reps, void *stream, long long *group_bytes, double *ms)
+{
+    return guard_status("sdl_batch_autotune", [&]() {
+        if (!B) fail(SDL_ERR_INVALID, "NULL batch");
+        if (B->exec) fail(SDL_ERR_INVALID, "the batch has been refilled: its groups are fixed");
+        check_bound(*B);
+        cudaStream_t s = pick_stream(stream);
+        if (s == cudaStreamLegacy) fail(SDL_ERR_INVALID, "batched refills need a non-default stream");
+        reps = std::max(1, std::min(reps, 20));
+        cudaEvent_t e0, e1;
+        SDL_CUDA(cudaEventCreate(&e0));
+        SDL_CUDA(cudaEventCreate(&e1));
+        const long long cands[] = {16LL << 20, 32LL << 20, 64LL << 20, 128LL << 20, 256LL << 20, 0};
+        long long best_bytes = B->group_bytes;
+        double best = 1e30;
+        for (long long c : cands)
+        {
+            B->group_bytes = c;
+            make_groups(*B);
+            batch_enqueue(*B, s); // warm
+            SDL_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; ++r) batch_enqueue(*B, s);
+            SDL_CUDA(cudaEventRecord(e1, s));
+            SDL_CUDA(cudaEventSynchronize(e1));
+            float t = 0;
+            SDL_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            if (t / reps < best)
+            {
+                best = t / reps;
+                best_bytes = c;
+            }
+        }
+        SDL_CUDA(cudaEventDestroy(e0));
+        SDL_CUDA(cudaEventDestroy(e1));
+        B->group_bytes = best_bytes;
+        make_groups(*B);
+        if (group_bytes) *group_bytes = best_bytes;
+        if (ms) *ms = best;
+    });
+}
+
 extern "C" sdl_status sdl_batch_refill(sdl_batch *B, void *stream)
 {
     return guard_status("sdl_batch_refill", [&]() {
         if (!B) fail(SDL_ERR_INVALID, "NULL batch");
-        for (size_t i = 0; i < B->prods.size(); ++i)
-            if (B->prods[i]->nnz > 0 && !B->host_ptrs[i].Cx)
-                fail(SDL_ERR_INVALID, "product " + std::to_string(i) + " has no bound values");
+        check_bound(*B);
         cudaStream_t s = pick_stream(stream);
         if (s == cudaStreamLegacy)
             fail(SDL_ERR_INVALID, "batched refills need a non-default stream (graph capture)");
-        auto enqueue = [&]() {
-            SDL_CUDA(cudaEventRecord(B->fork, s));
-            SDL_CUDA(cudaStreamWaitEvent(B->side, B->fork, 0));
-            for (size_t g = 0; g < B->entry_done.size(); ++g)
-            {
-                const int c0 = B->group_chunks[g], t0 = B->group_tiles[g];
-                if (g >= 2) SDL_CUDA(cudaStreamWaitEvent(B->side, B->refill_done[g - 2], 0));
-                entry_values_batched(B->chunks.get() + c0, B->group_chunks[g + 1] - c0, B->ptrs.get(),
-                                     B->scheds.get(), B->side);
-                SDL_CUDA(cudaEventRecord(B->entry_done[g], B->side));
-                SDL_CUDA(cudaStreamWaitEvent(s, B->entry_done[g], 0));
-                tile_refill(B->tiles.get() + t0, B->group_tiles[g + 1] - t0, B->ptrs.get(), B->scheds.get(), s);
-                SDL_CUDA(cudaEventRecord(B->refill_done[g], s));
-            }
-            SDL_CUDA(cudaEventRecord(B->join, B->side));
-            SDL_CUDA(cudaStreamWaitEvent(s, B->join, 0));
-            for (int i : B->with_big)
-            {
-                const ProdPtrs &pp = B->host_ptrs[i];
-                if (B->prods[i]->big_lists)
-                    big_lists_refill(*B->prods[i], B->ptrs.get() + i, s);
-                else
-                    big_rows_refill(*B->prods[i], pp.Lx, pp.d, pp.Ax, pp.Cx, s, B->ptrs.get() + i);
-            }
-        };
+        auto enqueue = [&]() { batch_enqueue(*B, s); };
         if (!B->exec)
         {
             // first refill runs eagerly (every lazily set kernel attribute is set

@@ -323,6 +323,13 @@ class Batch:
         self._bound[i] = (Lx, d, Ax, Cx)
         check(lib().sdl_batch_bind(self.handle, i, _ptr(Lx), _ptr(d), _ptr(Ax), _ptr(Cx)))
 
+    def autotune(self, reps=3, stream=None):
+        """Times the candidate group sizes before the first refill and keeps the
+        fastest (sdl_batch_autotune). Returns (group bytes, ms per refill)."""
+        gb, ms = C.c_longlong(), C.c_double()
+        check(lib().sdl_batch_autotune(self.handle, reps, _stream(stream), C.byref(gb), C.byref(ms)))
+        return gb.value, ms.value
+
     def refill(self, stream=None):
         check(lib().sdl_batch_refill(self.handle, _stream(stream)))
 

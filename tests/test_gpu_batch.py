@@ -121,3 +121,43 @@ def test_batch_with_heavy_rows_and_unit_products(sdl):
             got = outs[i][:P.nnz].cpu().numpy().view(np.int64)
             want = refs[i][:P.nnz].cpu().numpy().view(np.int64)
             assert np.array_equal(got, want), f"round {rnd}, product {i}"
+
+
+def test_batch_autotune_keeps_the_bits(sdl):
+    """The batch autotuner times its candidate group sizes before the graph exists;
+    the refill it settles on is bit-identical to each product's own fill."""
+    import torch
+    from sparsediff_linalg_b200.device import Batch, btda_product
+    inst = wl.batched_device(seed=13, count=16, lo=500, hi=8000)
+    prods, outs, refs = [], [], []
+    for k in inst:
+        P, T = btda_product(k["Ap"], k["Ai"], k["n"], k["Bp"], k["Bi"], k["n"])
+        prods.append((P, T))
+        outs.append(torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda"))
+        refs.append(torch.empty(max(1, P.nnz), dtype=torch.float64, device="cuda"))
+    B = Batch([p for p, _ in prods])
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    vals = []
+    for i, k in enumerate(inst):
+        v = (torch.randn(k["Ai"].numel(), generator=g, device="cuda", dtype=torch.float64),
+             torch.randn(k["Bi"].numel(), generator=g, device="cuda", dtype=torch.float64),
+             torch.rand(k["m"], generator=g, device="cuda", dtype=torch.float64) * 9.9 + 0.1)
+        vals.append(v)
+        B.bind(i, v[1], v[2], v[0], outs[i])
+    s = torch.cuda.Stream()
+    gb, ms = B.autotune(reps=2, stream=s)
+    assert gb in (16 << 20, 32 << 20, 64 << 20, 128 << 20, 256 << 20, 0) and ms > 0
+    with torch.cuda.stream(s):
+        B.refill(stream=s)   # eager, then captured
+        B.refill(stream=s)   # graph replay
+    s.synchronize()
+    for i, (P, _) in enumerate(prods):
+        ax, bx, d = vals[i]
+        P.fill(bx, d, ax, refs[i])
+    torch.cuda.synchronize()
+    for i, (P, _) in enumerate(prods):
+        assert np.array_equal(outs[i][:P.nnz].cpu().numpy().view(np.int64),
+                              refs[i][:P.nnz].cpu().numpy().view(np.int64)), i
+    with pytest.raises(Exception):
+        B.autotune(reps=1, stream=s)    # the graph exists: groups are fixed
