@@ -32,11 +32,19 @@ __device__ __forceinline__ void mma_f64(double &c0, double &c1, double a, double
                  : "d"(a), "d"(b));
 }
 
-// One warp per 16 x 16 tile (a0, b0) of partial P_k = X^T diag(d_perm) X: four
-// m8n8k4 accumulators, K = the block's rows in steps of 4.
+// One CTA (4 warps) per 64 x 64 tile (a0, b0) of partial P_k = X^T diag(d_perm) X.
+// The block's rows are taken ATA_KC at a time: columns a0.. and b0.. of those rows
+// are staged in shared memory (the b side as dwork = diag(d_perm) X, upstream's one
+// rounding per product), then each warp runs its 32 x 32 quarter as 4 x 4 m8n8k4
+// accumulators: per step of 4 rows, 4 A and 4 B fragments from shared memory feed 16
+// MMAs. The K order (rows ascending, 4 per MMA) is the same for every output.
 //   A fragment (8 x 4, row-major): lane holds A[lane / 4][lane % 4] = X[k + lane % 4][a + lane / 4]
 //   B fragment (4 x 8, col-major): lane holds B[lane % 4][lane / 4] = d * X[k + lane % 4][b + lane / 4]
 //   C (8 x 8): lane holds C[lane / 4][2 (lane % 4) + {0, 1}]
+constexpr int ATA_T = 64;   // output tile edge
+constexpr int ATA_KC = 32;  // rows staged at a time
+constexpr int ATA_LD = 68;  // shared row stride (doubles)
+
 __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ mtiles, int nmt,
                                                       const long long *__restrict__ x_off,
                                                       const long long *__restrict__ p_off,
@@ -46,44 +54,64 @@ __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ m
                                                       const double *__restrict__ X_vals,
                                                       const double *__restrict__ d, double *__restrict__ P)
 {
-    const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (w >= nmt) return;
-    const int lane = threadIdx.x & 31;
-    const int4 t = mtiles[w];
+    __shared__ double As[ATA_KC][ATA_LD];
+    __shared__ double Bs[ATA_KC][ATA_LD];
+    if (blockIdx.x >= nmt) return;
+    const int4 t = mtiles[blockIdx.x];
     const int k = t.x, a0 = t.y, b0 = t.z;
     const int m0 = m0d[k], n0 = n0d[k];
     const double *X = X_vals + x_off[k];
     const int *rp = rowperm_all + rowperm_off[k];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, q = lane & 3;
-    double c[2][2][2] = {};
-    for (int kk = 0; kk < m0; kk += 4)
+    const int wa = 32 * (w >> 1), wb = 32 * (w & 1);
+    double c[4][4][2] = {};
+    for (int k0 = 0; k0 < m0; k0 += ATA_KC)
     {
-        const int i = kk + q;
-        const bool ok = i < m0;
-        const double di = (ok && d) ? d[rp[i]] : 1.0;
-        double a[2], b[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int e = threadIdx.x; e < ATA_KC * ATA_T; e += blockDim.x)
         {
-            const int ca = a0 + 8 * h + g, cb = b0 + 8 * h + g;
-            a[h] = (ok && ca < n0) ? X[(long long)i * n0 + ca] : 0.0;
-            const double xb = (ok && cb < n0) ? X[(long long)i * n0 + cb] : 0.0;
-            b[h] = d ? __dmul_rn(xb, di) : xb; // dwork = diag(d_perm) X, as upstream
+            const int r = e / ATA_T, col = e % ATA_T;
+            const int i = k0 + r;
+            double xa = 0.0, xb = 0.0;
+            if (i < m0)
+            {
+                if (a0 + col < n0) xa = X[(long long)i * n0 + a0 + col];
+                if (b0 + col < n0)
+                {
+                    const double x = X[(long long)i * n0 + b0 + col];
+                    xb = d ? __dmul_rn(x, d[rp[i]]) : x; // dwork = diag(d_perm) X, as upstream
+                }
+            }
+            As[r][col] = xa;
+            Bs[r][col] = xb;
         }
+        __syncthreads();
+        const int kend = min(ATA_KC, m0 - k0);
+        for (int kk = 0; kk < kend; kk += 4)
+        {
+            double af[4], bf[4];
 #pragma unroll
-        for (int ha = 0; ha < 2; ++ha)
+            for (int h = 0; h < 4; ++h)
+            {
+                af[h] = As[kk + q][wa + 8 * h + g];
+                bf[h] = Bs[kk + q][wb + 8 * h + g];
+            }
 #pragma unroll
-            for (int hb = 0; hb < 2; ++hb) mma_f64(c[ha][hb][0], c[ha][hb][1], a[ha], b[hb]);
+            for (int ha = 0; ha < 4; ++ha)
+#pragma unroll
+                for (int hb = 0; hb < 4; ++hb) mma_f64(c[ha][hb][0], c[ha][hb][1], af[ha], bf[hb]);
+        }
+        __syncthreads();
     }
     double *Pk = P + p_off[k];
 #pragma unroll
-    for (int ha = 0; ha < 2; ++ha)
+    for (int ha = 0; ha < 4; ++ha)
 #pragma unroll
-        for (int hb = 0; hb < 2; ++hb)
+        for (int hb = 0; hb < 4; ++hb)
 #pragma unroll
             for (int e = 0; e < 2; ++e)
             {
-                const int r = a0 + 8 * ha + g, cc = b0 + 8 * hb + 2 * q + e;
+                const int r = a0 + wa + 8 * ha + g, cc = b0 + wb + 8 * hb + 2 * q + e;
                 if (r < n0 && cc < n0) Pk[(long long)r * n0 + cc] = c[ha][hb][e];
             }
 }
@@ -256,8 +284,8 @@ std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const 
         h_rp.insert(h_rp.end(), row_perm[k], row_perm[k] + m0[k]);
         P->x_total += (long long)m0[k] * n0[k];
         P->p_total += (long long)n0[k] * n0[k];
-        for (int a = 0; a < n0[k]; a += 16)
-            for (int b = 0; b < n0[k]; b += 16) mt.push_back(make_int4(k, a, b, 0));
+        for (int a = 0; a < n0[k]; a += ATA_T)
+            for (int b = 0; b < n0[k]; b += ATA_T) mt.push_back(make_int4(k, a, b, 0));
     }
     // upstream's coalescing of the partials (row_perm = col_perm = col_perm_k)
     std::vector<std::vector<int>> prow(n_src), pcol(n_src);
@@ -290,7 +318,7 @@ void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double 
 {
     if (P.c_total == 0) return;
     if (P.nmtiles > 0)
-        SDL_LAUNCH(k_ata_partials, (P.nmtiles + 3) / 4, 128, 0, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
+        SDL_LAUNCH(k_ata_partials, P.nmtiles, 128, 0, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
                    P.p_off.get(), P.m0d.get(), P.n0d.get(), P.rowperm_all.get(), P.rowperm_off.get(), X_vals, d,
                    P.P.get());
     long long maxcells = 0;

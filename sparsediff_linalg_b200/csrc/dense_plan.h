@@ -85,7 +85,7 @@ struct BlocksAtaPlan
     DevBuf<int> rowperm_all;              // per source block, concatenated
     DevBuf<long long> rowperm_off;
     DevBuf<double> P;                     // partials (refill scratch)
-    DevBuf<int4> mtiles;                  // 16 x 16 tiles of the partials: (block, a0, b0, -)
+    DevBuf<int4> mtiles;                  // 64 x 64 tiles of the partials: (block, a0, b0, -)
     int nmtiles = 0;
     // gather of the output cells: per output block, per source: row / column maps
     struct OutDesc
