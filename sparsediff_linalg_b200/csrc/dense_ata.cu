@@ -33,18 +33,94 @@ __device__ __forceinline__ void mma_f64(double &c0, double &c1, double a, double
 }
 
 // One CTA (4 warps) per 64 x 64 tile (a0, b0) of partial P_k = X^T diag(d_perm) X.
-// The block's rows are taken ATA_KC at a time: columns a0.. and b0.. of those rows
-// are staged in shared memory (the b side as dwork = diag(d_perm) X, upstream's one
-// rounding per product), then each warp runs its 32 x 32 quarter as 4 x 4 m8n8k4
-// accumulators: per step of 4 rows, 4 A and 4 B fragments from shared memory feed 16
-// MMAs. The K order (rows ascending, 4 per MMA) is the same for every output.
+// The block's rows are taken ATA_KC at a time through a two-stage cp.async
+// pipeline: columns a0.. and b0.. of the next ATA_KC rows (and their d values) are
+// copied into shared memory while the current ones feed the tensor cores. Each
+// warp runs its 32 x 32 quarter as 4 x 4 m8n8k4 accumulators: per step of 4 rows,
+// 4 A and 4 B fragments from shared memory feed 16 MMAs. The B fragments are
+// dwork = d * X, formed as they are read (upstream's one rounding per product). The
+// K order (rows ascending, 4 per MMA) is the same for every output.
 //   A fragment (8 x 4, row-major): lane holds A[lane / 4][lane % 4] = X[k + lane % 4][a + lane / 4]
 //   B fragment (4 x 8, col-major): lane holds B[lane % 4][lane / 4] = d * X[k + lane % 4][b + lane / 4]
 //   C (8 x 8): lane holds C[lane / 4][2 (lane % 4) + {0, 1}]
 constexpr int ATA_T = 64;   // output tile edge
 constexpr int ATA_KC = 32;  // rows staged at a time
 constexpr int ATA_LD = 68;  // shared row stride (doubles)
+constexpr int ATA_STAGE = 2 * ATA_KC * ATA_LD + ATA_KC; // A panel, B panel, d values
+constexpr int ATA_SMEM = 2 * ATA_STAGE * (int)sizeof(double);
 
+__device__ __forceinline__ unsigned ata_smem_u32(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void ata_cp8(double *dst, const double *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(ata_smem_u32(dst)), "l"(src));
+}
+
+// Copies rows k0 .. k0 + ATA_KC - 1 of the tile's two column panels (zeros past
+// the block's rows or columns) and the rows' d values into one stage.
+__device__ __forceinline__ void ata_stage(double *st, const double *X, const int *rp, const double *d, int m0,
+                                          int n0, int a0, int b0, int k0)
+{
+    double *As = st, *Bs = st + ATA_KC * ATA_LD, *ds = st + 2 * ATA_KC * ATA_LD;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < ATA_KC * ATA_T; e += 128)
+    {
+        const int r = e / ATA_T, col = e % ATA_T;
+        const int i = k0 + r;
+        const double *row = X + (long long)i * n0;
+        if (i < m0 && a0 + col < n0)
+            ata_cp8(&As[r * ATA_LD + col], row + a0 + col);
+        else
+            As[r * ATA_LD + col] = 0.0;
+        if (i < m0 && b0 + col < n0)
+            ata_cp8(&Bs[r * ATA_LD + col], row + b0 + col);
+        else
+            Bs[r * ATA_LD + col] = 0.0;
+    }
+    if (d && threadIdx.x < ATA_KC)
+    {
+        const int i = k0 + threadIdx.x;
+        if (i < m0)
+            ata_cp8(&ds[threadIdx.x], d + rp[i]);
+        else
+            ds[threadIdx.x] = 0.0;
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// A tile's block, origin and shape.
+struct AtaTile
+{
+    const double *X;
+    const int *rp;
+    double *Pk;
+    int a0, b0, m0, n0, nch;
+};
+
+__device__ __forceinline__ AtaTile ata_tile(int t, const int4 *__restrict__ mtiles, const long long *__restrict__ x_off,
+                                            const long long *__restrict__ p_off, const int *__restrict__ m0d,
+                                            const int *__restrict__ n0d, const int *__restrict__ rowperm_all,
+                                            const long long *__restrict__ rowperm_off, const double *X_vals,
+                                            double *P)
+{
+    const int4 mt = mtiles[t];
+    AtaTile T;
+    T.X = X_vals + x_off[mt.x];
+    T.rp = rowperm_all + rowperm_off[mt.x];
+    T.Pk = P + p_off[mt.x];
+    T.a0 = mt.y;
+    T.b0 = mt.z;
+    T.m0 = m0d[mt.x];
+    T.n0 = n0d[mt.x];
+    T.nch = max(1, (T.m0 + ATA_KC - 1) / ATA_KC); // a block without rows still stores its zero partial
+    return T;
+}
+
+// Persistent: CTA c takes tiles c, c + G, ... and runs the chunks of all of them as
+// one sequence through the two stages, so the copy of the next tile's first rows
+// overlaps the current tile's last MMAs and its store.
 __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ mtiles, int nmt,
                                                       const long long *__restrict__ x_off,
                                                       const long long *__restrict__ p_off,
@@ -54,66 +130,76 @@ __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ m
                                                       const double *__restrict__ X_vals,
                                                       const double *__restrict__ d, double *__restrict__ P)
 {
-    __shared__ double As[ATA_KC][ATA_LD];
-    __shared__ double Bs[ATA_KC][ATA_LD];
-    if (blockIdx.x >= nmt) return;
-    const int4 t = mtiles[blockIdx.x];
-    const int k = t.x, a0 = t.y, b0 = t.z;
-    const int m0 = m0d[k], n0 = n0d[k];
-    const double *X = X_vals + x_off[k];
-    const int *rp = rowperm_all + rowperm_off[k];
+    extern __shared__ double ata_sm[];
+    int t = blockIdx.x;
+    if (t >= nmt) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, q = lane & 3;
     const int wa = 32 * (w >> 1), wb = 32 * (w & 1);
+    AtaTile cur = ata_tile(t, mtiles, x_off, p_off, m0d, n0d, rowperm_all, rowperm_off, X_vals, P);
+    ata_stage(ata_sm, cur.X, cur.rp, d, cur.m0, cur.n0, cur.a0, cur.b0, 0);
     double c[4][4][2] = {};
-    for (int k0 = 0; k0 < m0; k0 += ATA_KC)
+    for (int ch = 0, sq = 0;; ++sq)
     {
-        for (int e = threadIdx.x; e < ATA_KC * ATA_T; e += blockDim.x)
+        // the chunk after this one: the tile's next, or the first of the CTA's next tile
+        int nt = t, nch = ch + 1;
+        if (nch >= cur.nch)
         {
-            const int r = e / ATA_T, col = e % ATA_T;
-            const int i = k0 + r;
-            double xa = 0.0, xb = 0.0;
-            if (i < m0)
-            {
-                if (a0 + col < n0) xa = X[(long long)i * n0 + a0 + col];
-                if (b0 + col < n0)
-                {
-                    const double x = X[(long long)i * n0 + b0 + col];
-                    xb = d ? __dmul_rn(x, d[rp[i]]) : x; // dwork = diag(d_perm) X, as upstream
-                }
-            }
-            As[r][col] = xa;
-            Bs[r][col] = xb;
+            nt = t + gridDim.x;
+            nch = 0;
         }
+        const bool more = nt < nmt;
+        AtaTile nx = cur;
+        if (more && nt != t)
+            nx = ata_tile(nt, mtiles, x_off, p_off, m0d, n0d, rowperm_all, rowperm_off, X_vals, P);
+        if (more)
+        {
+            ata_stage(ata_sm + ((sq + 1) & 1) * ATA_STAGE, nx.X, nx.rp, d, nx.m0, nx.n0, nx.a0, nx.b0,
+                      nch * ATA_KC);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        }
+        else
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncthreads();
-        const int kend = min(ATA_KC, m0 - k0);
+        const double *As = ata_sm + (sq & 1) * ATA_STAGE;
+        const double *Bs = As + ATA_KC * ATA_LD, *ds = As + 2 * ATA_KC * ATA_LD;
+        const int kend = min(ATA_KC, cur.m0 - ch * ATA_KC);
         for (int kk = 0; kk < kend; kk += 4)
         {
             double af[4], bf[4];
+            const double dq = d ? ds[kk + q] : 1.0;
 #pragma unroll
             for (int h = 0; h < 4; ++h)
             {
-                af[h] = As[kk + q][wa + 8 * h + g];
-                bf[h] = Bs[kk + q][wb + 8 * h + g];
+                af[h] = As[(kk + q) * ATA_LD + wa + 8 * h + g];
+                const double x = Bs[(kk + q) * ATA_LD + wb + 8 * h + g];
+                bf[h] = d ? __dmul_rn(x, dq) : x; // dwork = diag(d_perm) X, as upstream
             }
 #pragma unroll
             for (int ha = 0; ha < 4; ++ha)
 #pragma unroll
                 for (int hb = 0; hb < 4; ++hb) mma_f64(c[ha][hb][0], c[ha][hb][1], af[ha], bf[hb]);
         }
-        __syncthreads();
+        __syncthreads(); // this stage is free for the chunk after next
+        if (ch + 1 >= cur.nch)
+        {
+#pragma unroll
+            for (int ha = 0; ha < 4; ++ha)
+#pragma unroll
+                for (int hb = 0; hb < 4; ++hb)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+                    {
+                        const int r = cur.a0 + wa + 8 * ha + g, cc = cur.b0 + wb + 8 * hb + 2 * q + e;
+                        if (r < cur.n0 && cc < cur.n0) cur.Pk[(long long)r * cur.n0 + cc] = c[ha][hb][e];
+                        c[ha][hb][e] = 0.0;
+                    }
+        }
+        if (!more) break;
+        t = nt;
+        ch = nch;
+        cur = nx;
     }
-    double *Pk = P + p_off[k];
-#pragma unroll
-    for (int ha = 0; ha < 4; ++ha)
-#pragma unroll
-        for (int hb = 0; hb < 4; ++hb)
-#pragma unroll
-            for (int e = 0; e < 2; ++e)
-            {
-                const int r = a0 + wa + 8 * ha + g, cc = b0 + wb + 8 * hb + 2 * q + e;
-                if (r < n0 && cc < n0) Pk[(long long)r * n0 + cc] = c[ha][hb][e];
-            }
 }
 
 // One warp per (block k, active column c of B): row c of the partial,
@@ -162,27 +248,76 @@ __global__ void __launch_bounds__(256) k_btda_partials(const int2 *__restrict__ 
 }
 
 // Output cells: the partials that hold the cell, summed from +0.0 in block order.
-__global__ void k_ata_gather(const BlocksAtaPlan::OutDesc *__restrict__ outd, int o_base,
-                             const int *__restrict__ srcs, const int *__restrict__ maps,
-                             const long long *__restrict__ p_off, const int *__restrict__ n0d,
-                             const double *__restrict__ P, double *__restrict__ C)
+// A CTA takes GATHER_THREADS consecutive cells of one output block (one per
+// thread); the sources' partial offsets and strides are staged in shared memory
+// GATHER_CHUNK at a time, and each thread issues the loads of GATHER_BATCH sources
+// before it adds them, so the partials (just written, mostly in L2) stream with
+// that many loads in flight per thread instead of one. An absent cell reads as
+// -0.0, which leaves every round-to-nearest sum bit-for-bit unchanged (x + -0.0 = x,
+// +0.0 + -0.0 = +0.0), so the sum equals the one that skips it.
+constexpr int GATHER_THREADS = 256;
+constexpr int GATHER_CHUNK = 64;
+constexpr int GATHER_BATCH = 16;
+
+__global__ void __launch_bounds__(GATHER_THREADS) k_ata_gather(const BlocksAtaPlan::OutDesc *__restrict__ outd,
+                                                               int o_base, const int *__restrict__ srcs,
+                                                               const int *__restrict__ maps,
+                                                               const long long *__restrict__ p_off,
+                                                               const int *__restrict__ n0d,
+                                                               const double *__restrict__ P,
+                                                               double *__restrict__ C)
 {
+    __shared__ long long sbase[GATHER_CHUNK];
+    __shared__ int sn0[GATHER_CHUNK];
     const BlocksAtaPlan::OutDesc D = outd[o_base + blockIdx.y];
     const long long cells = (long long)D.m0 * D.n0;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cells;
-         e += (long long)gridDim.x * blockDim.x)
+    const int ms = D.m0 + D.n0;
+    for (long long eb = (long long)blockIdx.x * GATHER_THREADS; eb < cells;
+         eb += (long long)gridDim.x * GATHER_THREADS)
     {
-        const int i = (int)(e / D.n0), j = (int)(e - (long long)i * D.n0);
+        const long long e = eb + threadIdx.x;
+        const bool live = e < cells;
+        const int i = live ? (int)(e / D.n0) : 0;
+        const int j = live ? (int)(e - (long long)i * D.n0) : 0;
         double acc = 0.0;
-        const int *mp = maps + D.map_off;
-        for (int t = D.s_begin; t < D.s_end; ++t, mp += D.m0 + D.n0)
+        for (int t0 = D.s_begin; t0 < D.s_end; t0 += GATHER_CHUNK)
         {
-            const int si = mp[i], sj = mp[D.m0 + j];
-            if (si < 0 || sj < 0) continue;
-            const int k = srcs[t];
-            acc = __dadd_rn(acc, P[p_off[k] + (long long)si * n0d[k] + sj]);
+            const int nt = min(GATHER_CHUNK, D.s_end - t0);
+            __syncthreads();
+            if (threadIdx.x < nt)
+            {
+                const int k = srcs[t0 + threadIdx.x];
+                sbase[threadIdx.x] = p_off[k];
+                sn0[threadIdx.x] = n0d[k];
+            }
+            __syncthreads();
+            if (!live) continue;
+            const int *mp = maps + D.map_off + (long long)(t0 - D.s_begin) * ms;
+            for (int u0 = 0; u0 < nt; u0 += GATHER_BATCH)
+            {
+                double v[GATHER_BATCH];
+#pragma unroll
+                for (int u = 0; u < GATHER_BATCH; ++u)
+                {
+                    v[u] = -0.0;
+                    if (u0 + u < nt)
+                    {
+                        if (D.direct)
+                            v[u] = P[sbase[u0 + u] + e];
+                        else
+                        {
+                            const int *m = mp + (long long)(u0 + u) * ms;
+                            const int si = m[i], sj = m[D.m0 + j];
+                            if (si >= 0 && sj >= 0) v[u] = P[sbase[u0 + u] + (long long)si * sn0[u0 + u] + sj];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < GATHER_BATCH; ++u)
+                    if (u0 + u < nt) acc = __dadd_rn(acc, v[u]);
+            }
         }
-        C[D.c_off + e] = acc;
+        if (live) C[D.c_off + e] = acc;
     }
 }
 
@@ -240,13 +375,23 @@ void coalesce_partials(const std::vector<std::vector<int>> &prow, const std::vec
         if ((long long)D.m0 * D.n0 > INT_MAX) fail(SDL_ERR_OVERFLOW, "dense blocks: output block exceeds INT_MAX values");
         D.s_begin = (int)h_srcs.size();
         D.map_off = (long long)h_maps.size();
+        D.direct = 1;
         for (int k : P.out_srcs[o])
         {
             h_srcs.push_back(k);
             for (size_t q = 0; q < prow[k].size(); ++q) rpos[prow[k][q]] = (int)q;
             for (size_t q = 0; q < pcol[k].size(); ++q) cpos[pcol[k][q]] = (int)q;
-            for (int r : P.out_rows[o]) h_maps.push_back(rpos[r]);
-            for (int c : cols) h_maps.push_back(cpos[c]);
+            if (prow[k].size() != (size_t)D.m0 || pcol[k].size() != (size_t)D.n0) D.direct = 0;
+            for (size_t q = 0; q < P.out_rows[o].size(); ++q)
+            {
+                h_maps.push_back(rpos[P.out_rows[o][q]]);
+                if (rpos[P.out_rows[o][q]] != (int)q) D.direct = 0;
+            }
+            for (size_t q = 0; q < cols.size(); ++q)
+            {
+                h_maps.push_back(cpos[cols[q]]);
+                if (cpos[cols[q]] != (int)q) D.direct = 0;
+            }
             for (int r : prow[k]) rpos[r] = -1;
             for (int c : pcol[k]) cpos[c] = -1;
         }
@@ -306,6 +451,17 @@ std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const 
     P->P.reset((size_t)std::max<long long>(1, P->p_total));
     P->nmtiles = (int)mt.size();
     P->mtiles = upload(mt.data(), std::max<size_t>(1, mt.size()), s);
+    // the partials' two pipeline stages exceed the default 48 KB of dynamic shared
+    // memory (set on the device the plan, and so its fills, live on)
+    SDL_CUDA(cudaFuncSetAttribute(k_ata_partials, cudaFuncAttributeMaxDynamicSharedMemorySize, ATA_SMEM));
+    // persistent grid: every CTA resident at once, each with the same number of tiles
+    {
+        int per_sm = 0;
+        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ata_partials, 128, ATA_SMEM));
+        const int slots = std::max(1, per_sm) * runtime().num_sms;
+        const int per_cta = std::max(1, (P->nmtiles + slots - 1) / slots);
+        P->partials_grid = std::max(1, (P->nmtiles + per_cta - 1) / per_cta);
+    }
     P->outd = upload(od.data(), std::max<size_t>(1, od.size()), s);
     P->srcs = upload(h_srcs.data(), std::max<size_t>(1, h_srcs.size()), s);
     P->maps = upload(h_maps.data(), std::max<size_t>(1, h_maps.size()), s);
@@ -318,7 +474,7 @@ void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double 
 {
     if (P.c_total == 0) return;
     if (P.nmtiles > 0)
-        SDL_LAUNCH(k_ata_partials, P.nmtiles, 128, 0, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
+        SDL_LAUNCH(k_ata_partials, P.partials_grid, 128, ATA_SMEM, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
                    P.p_off.get(), P.m0d.get(), P.n0d.get(), P.rowperm_all.get(), P.rowperm_off.get(), X_vals, d,
                    P.P.get());
     long long maxcells = 0;
@@ -328,8 +484,8 @@ void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double 
         maxcells = std::max(maxcells, (long long)P.out_rows[o].size() * (long long)P.out_cols[o].size());
     for (int o = 0; o < P.n_out; o += 65535)
     {
-        const dim3 grid(grid_cap2(maxcells, 256, 4096), (unsigned)std::min(65535, P.n_out - o));
-        SDL_LAUNCH(k_ata_gather, grid, 256, 0, s, P.outd.get(), o, P.srcs.get(), P.maps.get(), P.p_off.get(),
+        const dim3 grid(grid_cap2(maxcells, GATHER_THREADS, 4096), (unsigned)std::min(65535, P.n_out - o));
+        SDL_LAUNCH(k_ata_gather, grid, GATHER_THREADS, 0, s, P.outd.get(), o, P.srcs.get(), P.maps.get(), P.p_off.get(),
                    P.n0d.get(), P.P.get(), C_vals);
     }
 }
@@ -460,8 +616,8 @@ void blocks_btda_fill(const BlocksAtaPlan &P, const double *X_vals, const double
         maxcells = std::max(maxcells, (long long)P.out_rows[o].size() * (long long)P.out_cols[o].size());
     for (int o = 0; o < P.n_out; o += 65535)
     {
-        const dim3 grid(grid_cap2(maxcells, 256, 4096), (unsigned)std::min(65535, P.n_out - o));
-        SDL_LAUNCH(k_ata_gather, grid, 256, 0, s, P.outd.get(), o, P.srcs.get(), P.maps.get(), P.p_off.get(),
+        const dim3 grid(grid_cap2(maxcells, GATHER_THREADS, 4096), (unsigned)std::min(65535, P.n_out - o));
+        SDL_LAUNCH(k_ata_gather, grid, GATHER_THREADS, 0, s, P.outd.get(), o, P.srcs.get(), P.maps.get(), P.p_off.get(),
                    P.n0d.get(), P.P.get(), C_vals);
     }
 }
