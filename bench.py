@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--small-tiles", action="store_true",
                     help="plan the headline product for the small-tile refill (128-thread CTAs, "
                          "512-term tiles) instead of autotuning it (reproducible profiles)")
-    ap.add_argument("--refill", choices=["auto", "pipelined", "direct"], default="auto",
-                    help="with --small-tiles: force the pipelined or the direct tile refill of the headline "
-                         "product (auto: the library's default / the autotuner's choice)")
+    ap.add_argument("--refill", choices=["auto", "pipelined", "staged", "direct"], default="auto",
+                    help="with --small-tiles: force the pipelined, the entry-staged direct or the plain direct "
+                         "tile refill of the headline product (auto: the library's default / the autotuner's "
+                         "choice)")
     ap.add_argument("--split-rows", action="store_true",
                     help="N > 1: one headline product split by output rows across the ranks "
                          "(strong scaling) instead of one product per rank (weak scaling)")
@@ -390,6 +391,7 @@ def run_b200(args, world, rank, local):
         P.replan(tile_budget=512, tile_max_terms=512, refill_threads=128, stream=stream)
         if args.refill != "auto":
             P.set_refill_pipe(args.refill == "pipelined")
+            P.set_refill_staged(args.refill == "staged")
         tune = P.tuning()
         torch.cuda.synchronize()
     elif not args.no_autotune:

@@ -110,6 +110,8 @@ EXTENSION_SIGNATURES = {
     "sdl_product_plan_ready": (C.c_int, [vp, c_int_p]),
     "sdl_product_set_refill_pipe": (C.c_int, [vp, C.c_int, c_int_p]),
     "sdl_product_refill_pipe_used": (C.c_int, [vp, c_int_p]),
+    "sdl_product_set_refill_staged": (C.c_int, [vp, C.c_int, c_int_p]),
+    "sdl_product_refill_staged_used": (C.c_int, [vp, c_int_p]),
     "sdl_batch_autotune": (C.c_int, [vp, C.c_int, vp, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
     "sdl_product_apply_tuned": (C.c_int, [vp, c_int_p, vp]),
     "sdl_product_pattern_key": (C.c_int, [vp, C.c_char_p, C.c_int, vp]),

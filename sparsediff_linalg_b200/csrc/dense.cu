@@ -125,15 +125,18 @@ __global__ void __launch_bounds__(BC_THREADS) k_blocks_csr(const BlkTile *__rest
 // it copies the source block into shared memory once, row-paired -- entry
 // (r, lane) holds {B[lane][r], B[lane + 32][r]}, so a lane reads both of its rows of
 // a term's column with one 16-byte load -- and its 16 warps then work through the
-// groups on their own, with no CTA barrier until the next block: per column, the
-// compact-CSC terms in order (uniform loads of row and value), each output summed
-// from +0.0 exactly as in k_blocks_csr; per group the 64 x 8 results go through a
-// warp-private tile and leave as 64-byte row segments.
+// groups on their own, with no CTA barrier until the next block. A warp copies a
+// group's compact-CSC terms (block row, value) into its own shared slots with one
+// coalesced load per lane, 32 at a time, so the terms are read as shared-memory
+// broadcasts; each output is summed from +0.0 in the terms' order exactly as in
+// k_blocks_csr, and the group's 64 x 8 results go through a warp-private tile and
+// leave as 64-byte row segments.
 constexpr int BCS_THREADS = 512;
 constexpr int BCS_WARPS = BCS_THREADS / 32;
 constexpr int BCS_COLS = 8;
 constexpr int BCS_LD = BCS_COLS + 1;
-constexpr int BCS_WBUF = 64 * BCS_LD; // doubles per warp
+constexpr int BCS_TERMS = 32;                             // terms staged per warp at a time
+constexpr int BCS_WBUF = 64 * BCS_LD + 3 * BCS_TERMS / 2; // doubles per warp: tile, values, rows
 
 __global__ void __launch_bounds__(BCS_THREADS, 1) k_blocks_csr_sm(const BlkDesc *__restrict__ descs, int n_out,
                                                                   const long long *__restrict__ gpref, long long ng,
@@ -146,6 +149,8 @@ __global__ void __launch_bounds__(BCS_THREADS, 1) k_blocks_csr_sm(const BlkDesc 
     extern __shared__ double2 bcs_pairs[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *wbuf = reinterpret_cast<double *>(bcs_pairs + 32 * max_n0B) + warp * BCS_WBUF;
+    double *tv = wbuf + 64 * BCS_LD;                   // staged term values
+    int *tr = reinterpret_cast<int *>(tv + BCS_TERMS); // staged term rows (pair index r * 32)
     const long long g0 = (long long)blockIdx.x * ng / gridDim.x;
     const long long g1 = (long long)(blockIdx.x + 1) * ng / gridDim.x;
     if (g0 >= g1) return;
@@ -184,15 +189,29 @@ __global__ void __launch_bounds__(BCS_THREADS, 1) k_blocks_csr_sm(const BlkDesc 
         {
             const int c0 = (int)(gq - gpref[blk]) * BCS_COLS;
             const int ncol = min(BCS_COLS, D.n0_C - c0);
+            const int cpl = lane <= ncol ? cp[c0 + lane] : 0; // the group's column offsets
+            const int dend = __shfl_sync(0xffffffffu, cpl, ncol);
+            int sb = __shfl_sync(0xffffffffu, cpl, 0), se = sb; // staged terms [sb, se)
             for (int j = 0; j < ncol; ++j)
             {
-                const int d1 = cp[c0 + j + 1];
+                const int d0 = __shfl_sync(0xffffffffu, cpl, j), d1 = __shfl_sync(0xffffffffu, cpl, j + 1);
                 double a0 = 0.0, a1 = 0.0;
-#pragma unroll 4
-                for (int dd = cp[c0 + j]; dd < d1; ++dd)
+                for (int dd = d0; dd < d1; ++dd)
                 {
-                    const double v = vals[dd];
-                    const double2 x = bcs_pairs[rows[dd] * 32 + lane];
+                    if (dd >= se) // warp-uniform: the next terms into the warp's slots
+                    {
+                        __syncwarp();
+                        sb = dd;
+                        se = min(dd + BCS_TERMS, dend);
+                        if (sb + lane < se)
+                        {
+                            tv[lane] = vals[sb + lane];
+                            tr[lane] = rows[sb + lane] * 32;
+                        }
+                        __syncwarp();
+                    }
+                    const double v = tv[dd - sb];
+                    const double2 x = bcs_pairs[tr[dd - sb] + lane];
                     a0 = __dadd_rn(a0, __dmul_rn(x.x, v));
                     a1 = __dadd_rn(a1, __dmul_rn(x.y, v));
                 }

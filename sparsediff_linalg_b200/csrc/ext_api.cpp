@@ -174,7 +174,26 @@ extern "C" sdl_status sdl_product_set_refill_pipe(sdl_product *P, int on, int *u
     return guard_status("sdl_product_set_refill_pipe", [&]() {
         if (!P) fail(SDL_ERR_INVALID, "NULL product");
         P->P.cfg.refill_pipe = on ? 1 : 0;
+        if (on) P->P.cfg.refill_es = 0;
         if (used) *used = pipe_refill(P->P) ? 1 : 0;
+    });
+}
+
+extern "C" sdl_status sdl_product_set_refill_staged(sdl_product *P, int on, int *used)
+{
+    return guard_status("sdl_product_set_refill_staged", [&]() {
+        if (!P) fail(SDL_ERR_INVALID, "NULL product");
+        P->P.cfg.refill_es = on ? 1 : 0;
+        if (on) P->P.cfg.refill_pipe = 0;
+        if (used) *used = es_refill(P->P) ? 1 : 0;
+    });
+}
+
+extern "C" sdl_status sdl_product_refill_staged_used(const sdl_product *P, int *used)
+{
+    return guard_status("sdl_product_refill_staged_used", [&]() {
+        if (!P || !used) fail(SDL_ERR_INVALID, "NULL argument");
+        *used = es_refill(P->P) ? 1 : 0;
     });
 }
 

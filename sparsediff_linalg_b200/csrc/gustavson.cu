@@ -1123,10 +1123,29 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
 
 // Shared memory of a refill CTA: two windows, a ring of four tile descriptors and,
 // for batched refills, the resolved base pointers of each descriptor's product.
+// Entry records of one tile staged in shared memory by the entry-staged refill:
+// tiles of the 128-thread plan hold at most TILE_T / 2 terms, most far fewer entries.
 template <int NT>
+__host__ __device__ constexpr int escap_of()
+{
+    return NT == REFILL_THREADS ? 512 : 256;
+}
+template <int NT, bool ESS = false>
 __host__ __device__ constexpr size_t refill_smem_bytes()
 {
-    return 2 * (size_t)win_of<NT>() * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase);
+    return 2 * (size_t)win_of<NT>() * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase) +
+           (ESS ? 2 * (size_t)escap_of<NT>() * sizeof(int2) : 0);
+}
+
+// The entry records of a tile into a ring slot (8-byte asynchronous copies, one
+// commit group per call).
+template <int NT>
+__device__ __forceinline__ void stage_tile_es(int2 *dst, const int2 *__restrict__ ES, int vbase, int nent)
+{
+    for (int e = threadIdx.x; e < nent; e += NT)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst + e)),
+                     "l"(ES + vbase + e));
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 template <int NT>
@@ -1221,16 +1240,23 @@ __device__ __forceinline__ ProdBase base_of(const ProdBase *bse, int slot, const
 // coalesced, and cleared; two windows alternate, so a tile needs one barrier. The
 // words of the next step -- or of the next tile, whose descriptor is read two
 // tiles ahead -- are loaded while a step's gathers are in flight.
-template <bool BATCHED, int NT>
+// ESS (entry-staged, single products): the tile's entry records come from shared
+// memory, copied there by cp.async while the tile before it runs (tile_nent: each
+// tile's entry count), so a step waits on one global load (V / A.x) instead of two
+// in a row (the record, then V / A.x). Same products, same sums: same bits.
+template <bool BATCHED, int NT, bool ESS = false>
 __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
     const TileDesc *__restrict__ tiles, int ntiles, const ProdPtrs *__restrict__ ptrs,
-    const ProdSched *__restrict__ scheds, ProdPtrs P1, ProdSched S1, int *__restrict__ err)
+    const ProdSched *__restrict__ scheds, ProdPtrs P1, ProdSched S1, int *__restrict__ err,
+    const int *__restrict__ tile_nent)
 {
     constexpr int WIN = win_of<NT>();
     constexpr int RSTEP = RUNROLL * NT;
+    constexpr int ESCAP = escap_of<NT>();
     extern __shared__ __align__(16) double rsm[];
     TileDesc *dsc = reinterpret_cast<TileDesc *>(rsm + 2 * WIN);
     ProdBase *bse = reinterpret_cast<ProdBase *>(dsc + 4);
+    int2 *esr = reinterpret_cast<int2 *>(bse + 4); // ESS: two slots of ESCAP records
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     int t = blockIdx.x;
@@ -1242,12 +1268,18 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
     unsigned w[RUNROLL];
     {
         const ProdBase pb = base_of<BATCHED>(bse, 0, P1, S1);
+        if (ESS) stage_tile_es<NT>(esr, pb.ES, dsc[0].vbase, tile_nent[t]);
         load_terms<NT>(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
     }
     // launched as a programmatic dependent of the entry-value kernel: everything
     // above overlaps its tail; V is read only after it has completed (a no-op for
     // an ordinary launch)
     asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (ESS)
+    {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+    }
     for (int k = 0;; ++k)
     {
         const TileDesc &D = dsc[k & 3];
@@ -1256,6 +1288,11 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
             copy_desc<BATCHED>(dsc + ((k + 2) & 3), bse + ((k + 2) & 3), tiles + t + 2 * G, ptrs, scheds, P1, S1);
         double *win = rsm + (k & 1) * WIN;
         const ProdBase pb = base_of<BATCHED>(bse, k & 3, P1, S1);
+        // the next tile's records into the other slot (last read by the tile before
+        // this one, whose term pass ended at a barrier)
+        if (ESS && has1)
+            stage_tile_es<NT>(esr + ((k + 1) & 1) * ESCAP, pb.ES, dsc[(k + 1) & 3].vbase, tile_nent[t + G]);
+        const int2 *es_t = esr + (k & 1) * ESCAP;
         const int nterms = D.nterms, nout = D.nout, vbase = D.vbase;
         for (int base = 0;; base += RSTEP)
         {
@@ -1268,7 +1305,10 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
             for (int j = 0; j < RUNROLL; ++j)
             {
                 term[j] = !(w[j] & (TERM_LIST << 12));
-                es[j] = term[j] ? pb.ES[vbase + (int)(w[j] >> 14)] : make_int2(0, 0);
+                if (ESS)
+                    es[j] = term[j] ? es_t[(int)(w[j] >> 14)] : make_int2(0, 0);
+                else
+                    es[j] = term[j] ? pb.ES[vbase + (int)(w[j] >> 14)] : make_int2(0, 0);
             }
             double v[RUNROLL], x[RUNROLL];
 #pragma unroll
@@ -1303,6 +1343,7 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
             for (int j = 0; j < RUNROLL; ++j) w[j] = wn[j];
             if (last) break;
         }
+        if (ESS) asm volatile("cp.async.wait_all;" ::: "memory"); // the next tile's records
         __syncthreads(); // the window is complete
         if (D.nlist > 0)
         {
@@ -2779,32 +2820,34 @@ void rebase_tiles(const TileDesc *src, int n, int prod, TileDesc *dst, cudaStrea
 namespace {
 // Resident refill CTAs per SM of one kernel instance (its attributes are set on the
 // first call, which is an eager one).
-template <bool BATCHED, int NT>
+template <bool BATCHED, int NT, bool ESS>
 int refill_per_sm()
 {
     static int per_sm = 0;
     if (!per_sm)
     {
-        set_smem(k_tile_refill<BATCHED, NT>, refill_smem_bytes<NT>());
+        set_smem(k_tile_refill<BATCHED, NT, ESS>, refill_smem_bytes<NT, ESS>());
         int n = 0;
-        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT>, NT,
-                                                               refill_smem_bytes<NT>()));
+        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT, ESS>, NT,
+                                                               refill_smem_bytes<NT, ESS>()));
         per_sm = std::max(1, n);
     }
     return per_sm;
 }
 
-template <bool BATCHED, int NT>
+template <bool BATCHED, int NT, bool ESS = false>
 void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
-                   cudaStream_t s, const ProdPtrs &vals, const ProdSched &sched, int ctas_per_sm)
+                   cudaStream_t s, const ProdPtrs &vals, const ProdSched &sched, int ctas_per_sm,
+                   const int *tile_nent = nullptr)
 {
-    const int per_sm = refill_per_sm<BATCHED, NT>();
+    const int per_sm = refill_per_sm<BATCHED, NT, ESS>();
     const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm) : per_sm;
     const int grid = std::min(ntiles, runtime().num_sms * use);
     if (BATCHED)
     {
-        SDL_LAUNCH((k_tile_refill<BATCHED, NT>), grid, NT, refill_smem_bytes<NT>(), s, tiles, ntiles, ptrs, scheds,
-                   vals, sched, runtime().d_error);
+        const size_t smem = refill_smem_bytes<NT, ESS>();
+        SDL_LAUNCH((k_tile_refill<BATCHED, NT, ESS>), grid, NT, smem, s, tiles, ntiles, ptrs, scheds, vals, sched,
+                   runtime().d_error, tile_nent);
         return;
     }
     // programmatic dependent launch: the CTAs start while the entry-value kernel
@@ -2812,15 +2855,15 @@ void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, cons
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(NT);
-    cfg.dynamicSmemBytes = refill_smem_bytes<NT>();
+    cfg.dynamicSmemBytes = refill_smem_bytes<NT, ESS>();
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill<BATCHED, NT>, tiles, ntiles, ptrs, scheds, vals, sched,
-                                runtime().d_error));
+    SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill<BATCHED, NT, ESS>, tiles, ntiles, ptrs, scheds, vals, sched,
+                                runtime().d_error, tile_nent));
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
@@ -2829,6 +2872,12 @@ void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, cons
 bool small_tile_refill(const Product &P)
 {
     return P.cfg.refill_threads == REFILL_THREADS_SMALL && P.max_tile_out <= win_of<REFILL_THREADS_SMALL>();
+}
+
+bool es_refill(const Product &P)
+{
+    if (!P.cfg.refill_es || P.ntiles <= 0 || !P.tile_nent.get() || pipe_refill(P)) return false;
+    return P.max_tile_ent <= (small_tile_refill(P) ? escap_of<REFILL_THREADS_SMALL>() : escap_of<REFILL_THREADS>());
 }
 
 bool pipe_refill(const Product &P)
@@ -2865,11 +2914,17 @@ void launch_refill_pipe(const Product &P, cudaStream_t s, const ProdPtrs &vals, 
 }
 
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
-                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm, bool small)
+                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm, bool small, const int *tile_nent)
 {
     if (ntiles <= 0) return;
     if (ptrs)
         launch_refill<true, REFILL_THREADS>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
+    else if (tile_nent && small)
+        launch_refill<false, REFILL_THREADS_SMALL, true>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm,
+                                                         tile_nent);
+    else if (tile_nent)
+        launch_refill<false, REFILL_THREADS, true>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm,
+                                                   tile_nent);
     else if (small)
         launch_refill<false, REFILL_THREADS_SMALL>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
     else
@@ -2977,7 +3032,7 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
             launch_refill_pipe(P, s, vals, S);
         else
             tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm,
-                        small_tile_refill(P));
+                        small_tile_refill(P), es_refill(P) ? P.tile_nent.get() : nullptr);
     }
     if (P.big_lists)
     {
@@ -3175,6 +3230,21 @@ TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
             }
             else
                 Q.cfg.refill_pipe = 0;
+            // and the entry-staged direct refill, when the tiles' records fit its slots
+            if (!Q.cfg.refill_pipe)
+            {
+                Q.cfg.refill_es = 1;
+                if (es_refill(Q))
+                {
+                    const double us_es = refill_us(Q);
+                    if (us_es < us)
+                        us = us_es;
+                    else
+                        Q.cfg.refill_es = 0;
+                }
+                else
+                    Q.cfg.refill_es = 0;
+            }
             if (us < best_us)
             {
                 best_us = us;

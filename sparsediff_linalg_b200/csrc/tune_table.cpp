@@ -8,13 +8,16 @@
 // File format (text, one entry per line, '#' starts a comment line):
 //   <key> <warp_max_terms> <rows_per_cta_warp> <cta_threads_2k> <cta_threads_8k>
 //         <gmem_threads> <tile_budget> <refill_ctas_per_sm> <tile_max_terms>
-//         <refill_threads> <refill_us>
+//         <refill_threads> <refill_kind> <refill_us>
+// refill_kind: 0 direct, 1 pipelined, 2 entry-staged direct. Lines without it (the
+// first version of the format) load as direct.
 #include <cstdio>
 #include <fstream>
 #include <map>
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <vector>
 
 #include "capi_common.h"
 
@@ -35,8 +38,10 @@ bool valid(const TuneConfig &c)
            pos(c.cta_threads_2k) && pos(c.cta_threads_8k) && pos(c.gmem_threads) && c.tile_budget >= 0 &&
            c.tile_budget <= TILE_T && c.tile_max_terms >= 0 && c.tile_max_terms <= TILE_T &&
            c.refill_ctas_per_sm >= 0 && c.refill_ctas_per_sm <= 64 &&
-           (c.refill_threads == 256 || c.refill_threads == 128);
+           (c.refill_threads == 256 || c.refill_threads == 128) && (c.refill_pipe == 0 || c.refill_es == 0);
 }
+
+int refill_kind(const TuneConfig &c) { return c.refill_pipe ? 1 : c.refill_es ? 2 : 0; }
 } // namespace
 
 void tune_table_record(const std::string &key, const TuneConfig &c, double refill_us)
@@ -64,8 +69,9 @@ extern "C" sdl_status sdl_tune_table_save(const char *path)
         std::lock_guard<std::mutex> g(g_mu);
         std::ofstream f(path, std::ios::trunc);
         if (!f) fail(SDL_ERR_INVALID, std::string("cannot write ") + path);
-        f << "# sparsediff_linalg_b200 tuning table v1: key warp_max_terms rows_per_cta_warp cta_threads_2k "
-             "cta_threads_8k gmem_threads tile_budget refill_ctas_per_sm tile_max_terms refill_threads refill_us\n";
+        f << "# sparsediff_linalg_b200 tuning table v2: key warp_max_terms rows_per_cta_warp cta_threads_2k "
+             "cta_threads_8k gmem_threads tile_budget refill_ctas_per_sm tile_max_terms refill_threads "
+             "refill_kind refill_us\n";
         char num[32];
         for (const auto &kv : g_table)
         {
@@ -73,7 +79,7 @@ extern "C" sdl_status sdl_tune_table_save(const char *path)
             std::snprintf(num, sizeof num, "%.3f", kv.second.refill_us);
             f << kv.first << ' ' << c.warp_max_terms << ' ' << c.rows_per_cta_warp << ' ' << c.cta_threads_2k << ' '
               << c.cta_threads_8k << ' ' << c.gmem_threads << ' ' << c.tile_budget << ' ' << c.refill_ctas_per_sm
-              << ' ' << c.tile_max_terms << ' ' << c.refill_threads << ' ' << num << '\n';
+              << ' ' << c.tile_max_terms << ' ' << c.refill_threads << ' ' << refill_kind(c) << ' ' << num << '\n';
         }
         if (!f) fail(SDL_ERR_INVALID, std::string("write failed: ") + path);
     });
@@ -93,15 +99,47 @@ extern "C" sdl_status sdl_tune_table_load(const char *path, int *entries)
             ++lineno;
             if (line.empty() || line[0] == '#') continue;
             std::istringstream in(line);
-            std::string key, extra;
+            std::vector<std::string> tok;
+            for (std::string t; in >> t;) tok.push_back(t);
             TuneEntry e;
             TuneConfig &c = e.cfg;
-            if (!(in >> key >> c.warp_max_terms >> c.rows_per_cta_warp >> c.cta_threads_2k >> c.cta_threads_8k >>
-                  c.gmem_threads >> c.tile_budget >> c.refill_ctas_per_sm >> c.tile_max_terms >> c.refill_threads >>
-                  e.refill_us) ||
-                (in >> extra) || !valid(c))
+            bool ok = tok.size() == 11 || tok.size() == 12;
+            if (ok)
+            {
+                int *fields[] = {&c.warp_max_terms, &c.rows_per_cta_warp, &c.cta_threads_2k, &c.cta_threads_8k,
+                                 &c.gmem_threads, &c.tile_budget, &c.refill_ctas_per_sm, &c.tile_max_terms,
+                                 &c.refill_threads};
+                int kind = 0;
+                size_t used = 0;
+                try
+                {
+                    for (int q = 0; q < 9 && ok; ++q)
+                    {
+                        *fields[q] = std::stoi(tok[1 + q], &used);
+                        ok = used == tok[1 + q].size();
+                    }
+                    if (ok && tok.size() == 12)
+                    {
+                        kind = std::stoi(tok[10], &used);
+                        ok = used == tok[10].size() && kind >= 0 && kind <= 2;
+                    }
+                    if (ok)
+                    {
+                        const std::string &u = tok.back();
+                        e.refill_us = std::stod(u, &used);
+                        ok = used == u.size();
+                    }
+                }
+                catch (const std::exception &)
+                {
+                    ok = false;
+                }
+                c.refill_pipe = kind == 1;
+                c.refill_es = kind == 2;
+            }
+            if (!ok || !valid(c))
                 fail(SDL_ERR_INVALID, std::string(path) + ": malformed tuning entry on line " + std::to_string(lineno));
-            loaded[key] = e;
+            loaded[tok[0]] = e;
         }
         std::lock_guard<std::mutex> g(g_mu);
         for (auto &kv : loaded) g_table[kv.first] = kv.second;

@@ -20,19 +20,24 @@ def test_table_round_trip_and_malformed(sdl, tmp_path):
     assert D.tune_table_size() == 0
     src = tmp_path / "t.txt"
     src.write_text("# comment\n"
-                   "m10.n9.t6.c4.h3:8, 512 8 256 512 512 768 4 0 256 41.5\n"
-                   "m4.n4.t2.c4.h1:8, 128 16 256 512 512 512 0 512 128 3.25\n")
+                   "m10.n9.t6.c4.h3:8, 512 8 256 512 512 768 4 0 256 41.5\n"       # first format
+                   "m4.n4.t2.c4.h1:8, 128 16 256 512 512 512 0 512 128 2 3.25\n")  # with refill kind
     assert D.tune_table_load(src) == 2
     assert D.tune_table_size() == 2
     out = tmp_path / "u.txt"
     D.tune_table_save(out)
     lines = [ln for ln in out.read_text().splitlines() if not ln.startswith("#")]
     assert sorted(ln.split()[0] for ln in lines) == ["m10.n9.t6.c4.h3:8,", "m4.n4.t2.c4.h1:8,"]
+    kinds = {ln.split()[0]: ln.split()[10] for ln in lines}
+    assert kinds == {"m10.n9.t6.c4.h3:8,": "0", "m4.n4.t2.c4.h1:8,": "2"}
     D.tune_table_clear()
     assert D.tune_table_load(out) == 2
     for bad in ("key 512 8\n",                                        # too few fields
                 "key 512 8 256 512 512 768 4 0 256 41.5 extra\n",     # too many
+                "key 512 8 256 512 512 768 4 0 256 1 41.5 7\n",       # too many
                 "key 333 8 256 512 512 768 4 0 256 41.5\n",           # invalid threshold
+                "key 512 8 256 512 512 768 4 0 256 3 41.5\n",         # invalid refill kind
+                "key 512 8 256 512 512 768 4 0 256 1.5 41.5\n",       # non-integer refill kind
                 "key 512 8 256 512 512 768 4 0 64 41.5\n"):           # invalid refill threads
         f = tmp_path / "bad.txt"
         f.write_text(bad)
