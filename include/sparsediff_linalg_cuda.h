@@ -355,10 +355,6 @@ sdl_status sdl_blocks_csr_block(const sdl_blocks_csr *P, int k, int *src_block, 
                                 int *n0_C, const int **col_perm);
 sdl_status sdl_blocks_csr_fill(const sdl_blocks_csr *P, const double *B_vals,
                                const double *S_x, double *C_vals, void *stream);
-/* 1 when the fill runs the persistent form (every block at most 64 rows and the
-   largest source block within one CTA's shared memory), 0 for the tiled form.
-   Both give the same bits. */
-int sdl_blocks_csr_persistent(const sdl_blocks_csr *P);
 void sdl_blocks_csr_destroy(sdl_blocks_csr *P);
 
 /* ------------------------------------------------------------------------

@@ -155,7 +155,6 @@ EXTENSION_SIGNATURES = {
     "sdl_blocks_csr_info": (C.c_int, [vp, c_int_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "sdl_blocks_csr_block": (C.c_int, [vp, C.c_int, c_int_p, c_int_p, c_int_p, C.POINTER(vp)]),
     "sdl_blocks_csr_fill": (C.c_int, [vp, vp, vp, vp, vp]),
-    "sdl_blocks_csr_persistent": (C.c_int, [vp]),
     "sdl_blocks_csr_destroy": (None, [vp]),
     "sdl_blocks_ata_create": (C.c_int, [C.c_int, vp, vp, C.POINTER(vp), C.POINTER(vp), C.c_int, C.c_int, vp,
                                         C.POINTER(vp)]),

@@ -595,8 +595,6 @@ extern "C" sdl_status sdl_blocks_csr_fill(const sdl_blocks_csr *P, const double 
     });
 }
 
-extern "C" int sdl_blocks_csr_persistent(const sdl_blocks_csr *P) { return P && P->P->sm_ok ? 1 : 0; }
-
 extern "C" void sdl_blocks_csr_destroy(sdl_blocks_csr *P) { delete P; }
 
 struct sdl_blocks_ata

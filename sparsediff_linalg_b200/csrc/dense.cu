@@ -119,118 +119,6 @@ __global__ void __launch_bounds__(BC_THREADS) k_blocks_csr(const BlkTile *__rest
     }
 }
 
-// Persistent form for blocks of at most 64 rows whose source block fits in shared
-// memory: one 512-thread CTA per SM takes an even share of the plan's 8-column
-// groups (groups never span two output blocks). For each output block of its share
-// it copies the source block into shared memory once, row-paired -- entry
-// (r, lane) holds {B[lane][r], B[lane + 32][r]}, so a lane reads both of its rows of
-// a term's column with one 16-byte load -- and its 16 warps then work through the
-// groups on their own, with no CTA barrier until the next block. A warp copies a
-// group's compact-CSC terms (block row, value) into its own shared slots with one
-// coalesced load per lane, 32 at a time, so the terms are read as shared-memory
-// broadcasts; each output is summed from +0.0 in the terms' order exactly as in
-// k_blocks_csr, and the group's 64 x 8 results go through a warp-private tile and
-// leave as 64-byte row segments.
-constexpr int BCS_THREADS = 512;
-constexpr int BCS_WARPS = BCS_THREADS / 32;
-constexpr int BCS_COLS = 8;
-constexpr int BCS_LD = BCS_COLS + 1;
-constexpr int BCS_TERMS = 32;                             // terms staged per warp at a time
-constexpr int BCS_WBUF = 64 * BCS_LD + 3 * BCS_TERMS / 2; // doubles per warp: tile, values, rows
-
-__global__ void __launch_bounds__(BCS_THREADS, 1) k_blocks_csr_sm(const BlkDesc *__restrict__ descs, int n_out,
-                                                                  const long long *__restrict__ gpref, long long ng,
-                                                                  int max_n0B, const int *__restrict__ cp_all,
-                                                                  const int *__restrict__ rows_all,
-                                                                  const double *__restrict__ vals_all,
-                                                                  const double *__restrict__ B_vals,
-                                                                  double *__restrict__ C_vals)
-{
-    extern __shared__ double2 bcs_pairs[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double *wbuf = reinterpret_cast<double *>(bcs_pairs + 32 * max_n0B) + warp * BCS_WBUF;
-    double *tv = wbuf + 64 * BCS_LD;                   // staged term values
-    int *tr = reinterpret_cast<int *>(tv + BCS_TERMS); // staged term rows (pair index r * 32)
-    const long long g0 = (long long)blockIdx.x * ng / gridDim.x;
-    const long long g1 = (long long)(blockIdx.x + 1) * ng / gridDim.x;
-    if (g0 >= g1) return;
-    int blk = 0; // the output block of group g0: the last with gpref[blk] <= g0
-    {
-        int lo = 0, hi = n_out - 1;
-        while (lo < hi)
-        {
-            const int mid = (lo + hi + 1) >> 1;
-            if (gpref[mid] <= g0)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        blk = lo;
-    }
-    for (long long gs = g0; gs < g1;)
-    {
-        while (gpref[blk + 1] <= gs) ++blk; // blocks without groups
-        const long long ge = min(g1, gpref[blk + 1]);
-        const BlkDesc D = descs[blk];
-        const double *B = B_vals + D.b_off;
-        __syncthreads(); // the previous block's pairs are no longer read
-        for (int e = threadIdx.x; e < 32 * D.n0_B; e += BCS_THREADS)
-        {
-            const int r = e >> 5, i = e & 31;
-            const double x0 = i < D.m0 ? B[(long long)i * D.n0_B + r] : 0.0;
-            const double x1 = i + 32 < D.m0 ? B[(long long)(i + 32) * D.n0_B + r] : 0.0;
-            bcs_pairs[e] = make_double2(x0, x1);
-        }
-        __syncthreads();
-        const int *cp = cp_all + D.cp_off;
-        const int *rows = rows_all + D.d_off;
-        const double *vals = vals_all + D.d_off;
-        for (long long gq = gs + warp; gq < ge; gq += BCS_WARPS)
-        {
-            const int c0 = (int)(gq - gpref[blk]) * BCS_COLS;
-            const int ncol = min(BCS_COLS, D.n0_C - c0);
-            const int cpl = lane <= ncol ? cp[c0 + lane] : 0; // the group's column offsets
-            const int dend = __shfl_sync(0xffffffffu, cpl, ncol);
-            int sb = __shfl_sync(0xffffffffu, cpl, 0), se = sb; // staged terms [sb, se)
-            for (int j = 0; j < ncol; ++j)
-            {
-                const int d0 = __shfl_sync(0xffffffffu, cpl, j), d1 = __shfl_sync(0xffffffffu, cpl, j + 1);
-                double a0 = 0.0, a1 = 0.0;
-                for (int dd = d0; dd < d1; ++dd)
-                {
-                    if (dd >= se) // warp-uniform: the next terms into the warp's slots
-                    {
-                        __syncwarp();
-                        sb = dd;
-                        se = min(dd + BCS_TERMS, dend);
-                        if (sb + lane < se)
-                        {
-                            tv[lane] = vals[sb + lane];
-                            tr[lane] = rows[sb + lane] * 32;
-                        }
-                        __syncwarp();
-                    }
-                    const double v = tv[dd - sb];
-                    const double2 x = bcs_pairs[tr[dd - sb] + lane];
-                    a0 = __dadd_rn(a0, __dmul_rn(x.x, v));
-                    a1 = __dadd_rn(a1, __dmul_rn(x.y, v));
-                }
-                wbuf[lane * BCS_LD + j] = a0;
-                wbuf[(lane + 32) * BCS_LD + j] = a1;
-            }
-            __syncwarp();
-            double *C = C_vals + D.c_off + c0;
-            for (int e = lane; e < 64 * BCS_COLS; e += 32)
-            {
-                const int i = e / BCS_COLS, j = e % BCS_COLS;
-                if (i < D.m0 && j < ncol) C[(long long)i * D.n0_C + j] = wbuf[i * BCS_LD + j];
-            }
-            __syncwarp();
-        }
-        gs = ge;
-    }
-}
-
 } // namespace
 
 std::unique_ptr<BlocksCsrPlan> blocks_csr_build(int n_src, const int *m0, const int *n0,
@@ -366,39 +254,6 @@ std::unique_ptr<BlocksCsrPlan> blocks_csr_build(int n_src, const int *m0, const 
     }
     P->desc = upload(descs.data(), std::max<size_t>(1, descs.size()), s);
     P->tiles = upload(tiles.data(), std::max<size_t>(1, tiles.size()), s);
-    // the persistent shared-memory form: every output block of at most 64 rows and
-    // the largest source block's row pairs plus the warp tiles within the opt-in
-    // shared memory of one CTA
-    {
-        int max_m0 = 0, max_n0B = 0;
-        for (const BlkDesc &D : descs)
-        {
-            max_m0 = std::max(max_m0, D.m0);
-            max_n0B = std::max(max_n0B, D.n0_B);
-        }
-        int optin = 0, dev = 0;
-        SDL_CUDA(cudaGetDevice(&dev));
-        SDL_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        const size_t bytes = (size_t)32 * std::max(1, max_n0B) * sizeof(double2) +
-                             (size_t)BCS_WARPS * BCS_WBUF * sizeof(double);
-        if (!descs.empty() && max_m0 <= 64 && bytes <= (size_t)optin)
-        {
-            std::vector<long long> gp(descs.size() + 1, 0);
-            for (size_t q = 0; q < descs.size(); ++q)
-                gp[q + 1] = gp[q] + (descs[q].m0 > 0 ? (descs[q].n0_C + BCS_COLS - 1) / BCS_COLS : 0);
-            P->sm_groups = gp.back();
-            if (P->sm_groups > 0)
-            {
-                P->sm_ok = true;
-                P->sm_bytes = bytes;
-                P->sm_max_n0B = std::max(1, max_n0B);
-                P->sm_grid = (int)std::min<long long>(runtime().num_sms, P->sm_groups);
-                P->gpref = upload(gp.data(), gp.size(), s);
-                SDL_CUDA(cudaFuncSetAttribute(k_blocks_csr_sm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)bytes));
-            }
-        }
-    }
     SDL_CUDA(cudaStreamSynchronize(s));
     return P;
 }
@@ -411,13 +266,6 @@ void blocks_csr_fill(const BlocksCsrPlan &P, const double *B_vals, const double 
     if (P.d_total > 0)
         SDL_LAUNCH(k_gather_vals, grid_cap(P.d_total, 256, rt.num_sms * 8), 256, 0, s, P.pos.get(), S_x,
                    P.d_total, P.vals.get());
-    if (P.sm_ok)
-    {
-        SDL_LAUNCH(k_blocks_csr_sm, P.sm_grid, BCS_THREADS, P.sm_bytes, s, P.desc.get(), (int)P.src.size(),
-                   P.gpref.get(), P.sm_groups, P.sm_max_n0B, P.cp.get(), P.rows.get(), P.vals.get(), B_vals,
-                   C_vals);
-        return;
-    }
     // the output blocks' sources, transposed (a source feeding two outputs is
     // transposed twice: outputs and sources are one to one here)
     const dim3 tg(std::max(1, P.tr_x), std::max(1, P.tr_y), (unsigned)P.src.size());

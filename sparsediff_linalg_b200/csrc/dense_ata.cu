@@ -44,7 +44,7 @@ __device__ __forceinline__ void mma_f64(double &c0, double &c1, double a, double
 //   B fragment (4 x 8, col-major): lane holds B[lane % 4][lane / 4] = d * X[k + lane % 4][b + lane / 4]
 //   C (8 x 8): lane holds C[lane / 4][2 (lane % 4) + {0, 1}]
 constexpr int ATA_T = 64;   // output tile edge
-constexpr int ATA_KC = 32;  // rows staged at a time
+constexpr int ATA_KC = 16;  // rows staged at a time
 constexpr int ATA_LD = 68;  // shared row stride (doubles)
 constexpr int ATA_STAGE = 2 * ATA_KC * ATA_LD + ATA_KC; // A panel, B panel, d values
 constexpr int ATA_SMEM = 2 * ATA_STAGE * (int)sizeof(double);
@@ -90,38 +90,6 @@ __device__ __forceinline__ void ata_stage(double *st, const double *X, const int
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-// A tile's block, origin and shape.
-struct AtaTile
-{
-    const double *X;
-    const int *rp;
-    double *Pk;
-    int a0, b0, m0, n0, nch;
-};
-
-__device__ __forceinline__ AtaTile ata_tile(int t, const int4 *__restrict__ mtiles, const long long *__restrict__ x_off,
-                                            const long long *__restrict__ p_off, const int *__restrict__ m0d,
-                                            const int *__restrict__ n0d, const int *__restrict__ rowperm_all,
-                                            const long long *__restrict__ rowperm_off, const double *X_vals,
-                                            double *P)
-{
-    const int4 mt = mtiles[t];
-    AtaTile T;
-    T.X = X_vals + x_off[mt.x];
-    T.rp = rowperm_all + rowperm_off[mt.x];
-    T.Pk = P + p_off[mt.x];
-    T.a0 = mt.y;
-    T.b0 = mt.z;
-    T.m0 = m0d[mt.x];
-    T.n0 = n0d[mt.x];
-    T.nch = max(1, (T.m0 + ATA_KC - 1) / ATA_KC); // a block without rows still stores its zero partial
-    return T;
-}
-
-// CTA c takes tiles c, c + G, ... and runs the chunks of all of them as one
-// sequence through the two stages, so that with fewer CTAs than tiles the copy of the
-// next tile's first rows overlaps the current tile's last MMAs and its store (the
-// plan launches one CTA per tile).
 __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ mtiles, int nmt,
                                                       const long long *__restrict__ x_off,
                                                       const long long *__restrict__ p_off,
@@ -132,39 +100,31 @@ __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ m
                                                       const double *__restrict__ d, double *__restrict__ P)
 {
     extern __shared__ double ata_sm[];
-    int t = blockIdx.x;
-    if (t >= nmt) return;
+    if (blockIdx.x >= nmt) return;
+    const int4 t = mtiles[blockIdx.x];
+    const int k = t.x, a0 = t.y, b0 = t.z;
+    const int m0 = m0d[k], n0 = n0d[k];
+    const double *X = X_vals + x_off[k];
+    const int *rp = rowperm_all + rowperm_off[k];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int g = lane >> 2, q = lane & 3;
     const int wa = 32 * (w >> 1), wb = 32 * (w & 1);
-    AtaTile cur = ata_tile(t, mtiles, x_off, p_off, m0d, n0d, rowperm_all, rowperm_off, X_vals, P);
-    ata_stage(ata_sm, cur.X, cur.rp, d, cur.m0, cur.n0, cur.a0, cur.b0, 0);
     double c[4][4][2] = {};
-    for (int ch = 0, sq = 0;; ++sq)
+    const int nch = (m0 + ATA_KC - 1) / ATA_KC;
+    if (nch > 0) ata_stage(ata_sm, X, rp, d, m0, n0, a0, b0, 0);
+    for (int ch = 0; ch < nch; ++ch)
     {
-        // the chunk after this one: the tile's next, or the first of the CTA's next tile
-        int nt = t, nch = ch + 1;
-        if (nch >= cur.nch)
+        if (ch + 1 < nch)
         {
-            nt = t + gridDim.x;
-            nch = 0;
-        }
-        const bool more = nt < nmt;
-        AtaTile nx = cur;
-        if (more && nt != t)
-            nx = ata_tile(nt, mtiles, x_off, p_off, m0d, n0d, rowperm_all, rowperm_off, X_vals, P);
-        if (more)
-        {
-            ata_stage(ata_sm + ((sq + 1) & 1) * ATA_STAGE, nx.X, nx.rp, d, nx.m0, nx.n0, nx.a0, nx.b0,
-                      nch * ATA_KC);
+            ata_stage(ata_sm + ((ch + 1) & 1) * ATA_STAGE, X, rp, d, m0, n0, a0, b0, (ch + 1) * ATA_KC);
             asm volatile("cp.async.wait_group 1;" ::: "memory");
         }
         else
             asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncthreads();
-        const double *As = ata_sm + (sq & 1) * ATA_STAGE;
+        const double *As = ata_sm + (ch & 1) * ATA_STAGE;
         const double *Bs = As + ATA_KC * ATA_LD, *ds = As + 2 * ATA_KC * ATA_LD;
-        const int kend = min(ATA_KC, cur.m0 - ch * ATA_KC);
+        const int kend = min(ATA_KC, m0 - ch * ATA_KC);
         for (int kk = 0; kk < kend; kk += 4)
         {
             double af[4], bf[4];
@@ -182,25 +142,18 @@ __global__ void __launch_bounds__(128) k_ata_partials(const int4 *__restrict__ m
                 for (int hb = 0; hb < 4; ++hb) mma_f64(c[ha][hb][0], c[ha][hb][1], af[ha], bf[hb]);
         }
         __syncthreads(); // this stage is free for the chunk after next
-        if (ch + 1 >= cur.nch)
-        {
-#pragma unroll
-            for (int ha = 0; ha < 4; ++ha)
-#pragma unroll
-                for (int hb = 0; hb < 4; ++hb)
-#pragma unroll
-                    for (int e = 0; e < 2; ++e)
-                    {
-                        const int r = cur.a0 + wa + 8 * ha + g, cc = cur.b0 + wb + 8 * hb + 2 * q + e;
-                        if (r < cur.n0 && cc < cur.n0) cur.Pk[(long long)r * cur.n0 + cc] = c[ha][hb][e];
-                        c[ha][hb][e] = 0.0;
-                    }
-        }
-        if (!more) break;
-        t = nt;
-        ch = nch;
-        cur = nx;
     }
+    double *Pk = P + p_off[k];
+#pragma unroll
+    for (int ha = 0; ha < 4; ++ha)
+#pragma unroll
+        for (int hb = 0; hb < 4; ++hb)
+#pragma unroll
+            for (int e = 0; e < 2; ++e)
+            {
+                const int r = a0 + wa + 8 * ha + g, cc = b0 + wb + 8 * hb + 2 * q + e;
+                if (r < n0 && cc < n0) Pk[(long long)r * n0 + cc] = c[ha][hb][e];
+            }
 }
 
 // One warp per (block k, active column c of B): row c of the partial,
@@ -455,11 +408,6 @@ std::unique_ptr<BlocksAtaPlan> blocks_ata_build(int n_src, const int *m0, const 
     // the partials' two pipeline stages exceed the default 48 KB of dynamic shared
     // memory (set on the device the plan, and so its fills, live on)
     SDL_CUDA(cudaFuncSetAttribute(k_ata_partials, cudaFuncAttributeMaxDynamicSharedMemorySize, ATA_SMEM));
-    // one CTA per tile: measured faster than a persistent grid of resident CTAs
-    // walking several tiles each (39 vs 43 us for 64 blocks of 64 x 256): the other
-    // resident CTAs hide a CTA's first copy and its store better than its own next
-    // tile does
-    P->partials_grid = std::max(1, P->nmtiles);
     P->outd = upload(od.data(), std::max<size_t>(1, od.size()), s);
     P->srcs = upload(h_srcs.data(), std::max<size_t>(1, h_srcs.size()), s);
     P->maps = upload(h_maps.data(), std::max<size_t>(1, h_maps.size()), s);
@@ -472,7 +420,7 @@ void blocks_ata_fill(const BlocksAtaPlan &P, const double *X_vals, const double 
 {
     if (P.c_total == 0) return;
     if (P.nmtiles > 0)
-        SDL_LAUNCH(k_ata_partials, P.partials_grid, 128, ATA_SMEM, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
+        SDL_LAUNCH(k_ata_partials, P.nmtiles, 128, ATA_SMEM, s, P.mtiles.get(), P.nmtiles, P.x_off.get(),
                    P.p_off.get(), P.m0d.get(), P.n0d.get(), P.rowperm_all.get(), P.rowperm_off.get(), X_vals, d,
                    P.P.get());
     long long maxcells = 0;

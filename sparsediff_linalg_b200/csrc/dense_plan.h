@@ -46,13 +46,6 @@ struct BlocksCsrPlan
     DevBuf<BlkDesc> desc;
     DevBuf<BlkTile> tiles;
     int ntiles = 0;
-    // persistent shared-memory form (blocks of at most 64 rows): 8-column groups,
-    // their prefix per output block, one CTA per SM
-    bool sm_ok = false;
-    long long sm_groups = 0;
-    size_t sm_bytes = 0;
-    int sm_max_n0B = 1, sm_grid = 0;
-    DevBuf<long long> gpref;
 };
 
 // Builds the plan of C_k = B_k S[col_perm_k, :] for n_src source blocks of shape
@@ -94,7 +87,6 @@ struct BlocksAtaPlan
     DevBuf<double> P;                     // partials (refill scratch)
     DevBuf<int4> mtiles;                  // 64 x 64 tiles of the partials: (block, a0, b0, -)
     int nmtiles = 0;
-    int partials_grid = 1;                // persistent CTAs of the partials kernel
     // gather of the output cells: per output block, per source: row / column maps
     struct OutDesc
     {

@@ -247,11 +247,6 @@ class BlocksCsr:
                 perm = np.zeros(0, np.int32)
             self.blocks.append((src.value, m.value, n0c.value, perm))
 
-    @property
-    def persistent(self) -> bool:
-        """True when the fill runs the persistent shared-memory form."""
-        return bool(lib().sdl_blocks_csr_persistent(self.handle))
-
     def fill(self, B_vals, S_x, C_vals, stream=None):
         check(lib().sdl_blocks_csr_fill(self.handle, _ptr(B_vals), _ptr(S_x), _ptr(C_vals),
                                         _stream(stream)))

@@ -60,7 +60,6 @@ def test_blocks_csr_bit_exact(sdl, orc, keep_empty):
     blocks.append((rng.standard_normal((4, 10)), np.arange(10, dtype=np.int32)))  # only empty rows
     want = orc.blocks_csr(blocks, S[0], S[1], S[2], S_n)
     P, got = _run_device(blocks, S, keep_empty)
-    assert P.persistent  # every block has at most 64 rows
     kept = [k for k, (cols, C_k) in enumerate(want) if keep_empty or C_k.size]
     assert [g[0] for g in got] == kept
     for (src, perm, Cg) in got:
@@ -81,7 +80,7 @@ def test_blocks_csr_config_shape(sdl, orc):
     blocks = [(rng.standard_normal((64, 256)), np.arange(256, dtype=np.int32)) for _ in range(4)]
     want = orc.blocks_csr(blocks, Sp, Si, Sx, S_n)
     P, got = _run_device(blocks, S, False)
-    assert len(got) == 4 and P.persistent
+    assert len(got) == 4
     for (src, perm, Cg) in got:
         cols, Cw = want[src]
         assert np.array_equal(perm, cols)
@@ -89,11 +88,10 @@ def test_blocks_csr_config_shape(sdl, orc):
 
 
 @pytest.mark.parametrize("specs", [[(100, 20), (65, 7), (3, 9)], [(8, 400), (64, 30)]],
-                         ids=["blocks_over_64_rows", "source_block_over_shared_memory"])
-def test_blocks_csr_tiled_form_bit_exact(sdl, orc, specs):
-    """Plans the persistent form cannot hold (a block of more than 64 rows, or a
-    400-column source block whose row pairs exceed one CTA's shared memory) take the
-    tiled kernel: the same bits as the oracle."""
+                         ids=["blocks_over_64_rows", "wide_source_block"])
+def test_blocks_csr_tall_and_wide_blocks_bit_exact(sdl, orc, specs):
+    """Blocks of more than 64 rows (several row passes of a tile) and a 400-column
+    source block: the same bits as the oracle."""
     rng = np.random.default_rng(93)
     S_m, S_n = 500, 3000
     lens = rng.integers(0, 30, S_m)
@@ -102,7 +100,6 @@ def test_blocks_csr_tiled_form_bit_exact(sdl, orc, specs):
     blocks = _blocks(rng, S_m, specs)
     want = orc.blocks_csr(blocks, S[0], S[1], S[2], S_n)
     P, got = _run_device(blocks, S, False)
-    assert not P.persistent
     assert len(got) == len(specs)
     for (src, perm, Cg) in got:
         cols, Cw = want[src]
@@ -110,10 +107,9 @@ def test_blocks_csr_tiled_form_bit_exact(sdl, orc, specs):
         assert np.array_equal(bits(Cg), bits(Cw)), f"block {src}"
 
 
-def test_blocks_csr_persistent_many_blocks_bit_exact(sdl, orc):
-    """Forty blocks over few columns: the CTAs' shares of 8-column groups start and
-    end inside blocks and span several blocks each (restaged in turn), blocks of 1
-    to 64 rows, some with an output narrower than one group."""
+def test_blocks_csr_many_small_blocks_bit_exact(sdl, orc):
+    """Forty blocks of 1 to 64 rows over few columns, some with an output narrower
+    than one 32-column tile, empty ones kept."""
     rng = np.random.default_rng(94)
     S_m, S_n = 200, 900
     lens = rng.integers(0, 6, S_m)
@@ -122,7 +118,6 @@ def test_blocks_csr_persistent_many_blocks_bit_exact(sdl, orc):
     blocks = _blocks(rng, S_m, specs)
     want = orc.blocks_csr(blocks, S[0], S[1], S[2], S_n)
     P, got = _run_device(blocks, S, True)
-    assert P.persistent
     for (src, perm, Cg) in got:
         cols, Cw = want[src]
         assert np.array_equal(perm, cols)
