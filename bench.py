@@ -58,7 +58,7 @@ def parse():
                     help="plan the headline product for the small-tile refill (128-thread CTAs, "
                          "512-term tiles) instead of autotuning it (reproducible profiles)")
     ap.add_argument("--refill", choices=["auto", "pipelined", "staged", "direct"], default="auto",
-                    help="with --small-tiles: force the pipelined, the entry-staged direct or the plain direct "
+                    help="with --small-tiles: force the pipelined, the staged direct or the plain direct "
                          "tile refill of the headline product (auto: the library's default / the autotuner's "
                          "choice)")
     ap.add_argument("--split-rows", action="store_true",

@@ -141,12 +141,12 @@ sdl_status sdl_product_refill_shape(const sdl_product *P, int *refill_threads, i
 sdl_status sdl_product_set_refill_pipe(sdl_product *P, int on, int *used);
 /* Whether P's tiles are refilled by the pipelined refill (1) or the direct one (0). */
 sdl_status sdl_product_refill_pipe_used(const sdl_product *P, int *used);
-/* The entry-staged direct refill (on = 1: each tile's entry records are copied into
-   shared memory while the tile before it runs, so a term waits on one global load
-   instead of two in a row), used when every tile holds at most 256 entries (512 for
-   the 256-thread plan); on = 0 the plain direct refill. Turning it on turns the
-   pipelined refill off. Same bits either way. *used (may be NULL) reports whether it
-   will run. */
+/* The staged direct refill (on = 1: each tile's term words and entry records are
+   bulk-copied into shared memory by one thread while the tile before it runs, so a
+   term step issues only the V and A.x gathers to global memory), used when two
+   slots for the plan's largest tile fit a 64 KB CTA; on = 0 the plain direct
+   refill. Turning it on turns the pipelined refill off. Same bits either way.
+   *used (may be NULL) reports whether it will run. */
 sdl_status sdl_product_set_refill_staged(sdl_product *P, int on, int *used);
 sdl_status sdl_product_refill_staged_used(const sdl_product *P, int *used);
 

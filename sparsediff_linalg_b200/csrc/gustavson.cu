@@ -21,6 +21,7 @@
 //             accumulator (<= 8192 output entries), CTA + accumulator in C.x itself
 //             with a global column->position map (larger rows).
 #include <algorithm>
+#include <mutex>
 #include <chrono>
 #include <cstddef>
 #include <climits>
@@ -1123,29 +1124,80 @@ __device__ __forceinline__ ProdBase prod_base(int prod, const ProdPtrs *__restri
 
 // Shared memory of a refill CTA: two windows, a ring of four tile descriptors and,
 // for batched refills, the resolved base pointers of each descriptor's product.
-// Entry records of one tile staged in shared memory by the entry-staged refill:
-// tiles of the 128-thread plan hold at most TILE_T / 2 terms, most far fewer entries.
 template <int NT>
-__host__ __device__ constexpr int escap_of()
-{
-    return NT == REFILL_THREADS ? 512 : 256;
-}
-template <int NT, bool ESS = false>
 __host__ __device__ constexpr size_t refill_smem_bytes()
 {
-    return 2 * (size_t)win_of<NT>() * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase) +
-           (ESS ? 2 * (size_t)escap_of<NT>() * sizeof(int2) : 0);
+    return 2 * (size_t)win_of<NT>() * 8 + 4 * sizeof(TileDesc) + 4 * sizeof(ProdBase);
 }
 
-// The entry records of a tile into a ring slot (8-byte asynchronous copies, one
-// commit group per call).
-template <int NT>
-__device__ __forceinline__ void stage_tile_es(int2 *dst, const int2 *__restrict__ ES, int vbase, int nent)
+// Staged refill (single products): each tile's term words and entry records, two
+// contiguous runs of the schedule, are copied into one of two shared-memory slots by
+// two 1-D bulk copies (cp.async.bulk, this GPU's own memory, no multicast) issued by
+// one thread while the tile before it runs, completing on the slot's mbarrier. A
+// slot holds wcap words then ecap records; the copies start at the 16-byte boundary
+// at or below the run (the schedule's arrays carry 16 bytes of padding past their
+// ends for the rounded-up tails).
+constexpr int STAGE_HDR = 4 * (int)sizeof(int) + 2 * (int)sizeof(unsigned long long); // entry counts, mbarriers
+constexpr size_t STAGED_SMEM_MAX = 64 * 1024; // shared memory of a staged refill CTA at most
+inline size_t staged_smem_bytes(int nt, int wcap, int ecap)
 {
-    for (int e = threadIdx.x; e < nent; e += NT)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst + e)),
-                     "l"(ES + vbase + e));
-    asm volatile("cp.async.commit_group;" ::: "memory");
+    const size_t base = nt == 256 ? refill_smem_bytes<256>() : refill_smem_bytes<128>();
+    return base + STAGE_HDR + 2 * ((size_t)wcap * 4 + (size_t)ecap * 8);
+}
+
+__device__ __forceinline__ unsigned rf_smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void rf_mbar_init(unsigned long long *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rf_smem_u32(bar)) : "memory");
+}
+
+// One thread: the tile's words and records into `slot`, completing on `bar`. The
+// records end at nV at the latest (the validated term words never index past it;
+// list words, whose entries the copy does not need, may count beyond).
+__device__ __forceinline__ void rf_stage_tile(unsigned *slot, int wcap, const TileDesc &D, int nent,
+                                              const unsigned *W, const int2 *ES, unsigned nV,
+                                              unsigned long long *bar)
+{
+    const int wb = D.word_begin & ~3;
+    const int wn = ((D.word_begin + D.nterms + 3) & ~3) - wb; // words, a multiple of 4
+    const int eb = D.vbase & ~1;
+    const long long eend = min((long long)D.vbase + nent, (long long)nV);
+    const int en = eend > eb ? (int)(((eend + 1) & ~1LL) - eb) : 0; // records, a multiple of 2
+    const unsigned bytes = (unsigned)wn * 4u + (unsigned)en * 8u;
+    unsigned long long state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                 : "=l"(state)
+                 : "r"(rf_smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    (void)state;
+    if (wn > 0)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(rf_smem_u32(slot)), "l"(W + wb), "r"((unsigned)wn * 4u), "r"(rf_smem_u32(bar))
+                     : "memory");
+    if (en > 0)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(rf_smem_u32(slot + wcap)), "l"(ES + eb), "r"((unsigned)en * 8u), "r"(rf_smem_u32(bar))
+                     : "memory");
+}
+
+// Waits for phase `parity` of `bar` to complete, at most ~2^20 polls (with a short
+// sleep between them); false if it did not.
+__device__ __forceinline__ bool rf_mbar_wait(unsigned long long *bar, unsigned parity)
+{
+    const unsigned a = rf_smem_u32(bar);
+    for (int it = 0; it < (1 << 20); ++it)
+    {
+        unsigned ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if (it > 8) __nanosleep(64);
+    }
+    return false;
 }
 
 template <int NT>
@@ -1240,23 +1292,26 @@ __device__ __forceinline__ ProdBase base_of(const ProdBase *bse, int slot, const
 // coalesced, and cleared; two windows alternate, so a tile needs one barrier. The
 // words of the next step -- or of the next tile, whose descriptor is read two
 // tiles ahead -- are loaded while a step's gathers are in flight.
-// ESS (entry-staged, single products): the tile's entry records come from shared
-// memory, copied there by cp.async while the tile before it runs (tile_nent: each
-// tile's entry count), so a step waits on one global load (V / A.x) instead of two
-// in a row (the record, then V / A.x). Same products, same sums: same bits.
+// ESS (staged, single products): the tile's term words and entry records come from
+// shared memory, bulk-copied there while the tile before it runs (the entry counts
+// tile_nent travel with the descriptors, two tiles ahead), so a step issues only the
+// V and A.x gathers to global memory. Same products, same sums: same bits.
 template <bool BATCHED, int NT, bool ESS = false>
 __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
     const TileDesc *__restrict__ tiles, int ntiles, const ProdPtrs *__restrict__ ptrs,
     const ProdSched *__restrict__ scheds, ProdPtrs P1, ProdSched S1, int *__restrict__ err,
-    const int *__restrict__ tile_nent)
+    const int *__restrict__ tile_nent, int wcap, int ecap)
 {
     constexpr int WIN = win_of<NT>();
     constexpr int RSTEP = RUNROLL * NT;
-    constexpr int ESCAP = escap_of<NT>();
     extern __shared__ __align__(16) double rsm[];
     TileDesc *dsc = reinterpret_cast<TileDesc *>(rsm + 2 * WIN);
     ProdBase *bse = reinterpret_cast<ProdBase *>(dsc + 4);
-    int2 *esr = reinterpret_cast<int2 *>(bse + 4); // ESS: two slots of ESCAP records
+    // ESS: the ring's entry counts, the two slots' mbarriers, the two slots
+    int *nent_r = reinterpret_cast<int *>(bse + 4);
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(nent_r + 4);
+    unsigned *slots = reinterpret_cast<unsigned *>(bars + 2);
+    const int sstride = wcap + 2 * ecap; // 4-byte units per slot
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     int t = blockIdx.x;
@@ -1264,36 +1319,95 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
     for (int i = tid; i < 2 * WIN; i += NT) rsm[i] = 0.0;
     copy_desc<BATCHED>(dsc, bse, tiles + t, ptrs, scheds, P1, S1);
     if (t + G < ntiles) copy_desc<BATCHED>(dsc + 1, bse + 1, tiles + t + G, ptrs, scheds, P1, S1);
+    if (ESS && tid == NT - 1)
+    {
+        nent_r[0] = tile_nent[t];
+        if (t + G < ntiles) nent_r[1] = tile_nent[t + G];
+        rf_mbar_init(&bars[0]);
+        rf_mbar_init(&bars[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
     unsigned w[RUNROLL];
     {
         const ProdBase pb = base_of<BATCHED>(bse, 0, P1, S1);
-        if (ESS) stage_tile_es<NT>(esr, pb.ES, dsc[0].vbase, tile_nent[t]);
-        load_terms<NT>(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
+        if (ESS)
+        {
+            if (tid == 0) rf_stage_tile(slots, wcap, dsc[0], nent_r[0], pb.W, pb.ES, pb.nV, &bars[0]);
+        }
+        else
+            load_terms<NT>(pb.W + dsc[0].word_begin, dsc[0].nterms, 0, w);
     }
     // launched as a programmatic dependent of the entry-value kernel: everything
     // above overlaps its tail; V is read only after it has completed (a no-op for
     // an ordinary launch)
     asm volatile("griddepcontrol.wait;" ::: "memory");
-    if (ESS)
-    {
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncthreads();
-    }
+    bool bad = false; // ESS: a slot that never arrived (its terms are skipped, err set)
     for (int k = 0;; ++k)
     {
         const TileDesc &D = dsc[k & 3];
         const bool has1 = t + G < ntiles;
         if (t + 2 * G < ntiles)
+        {
             copy_desc<BATCHED>(dsc + ((k + 2) & 3), bse + ((k + 2) & 3), tiles + t + 2 * G, ptrs, scheds, P1, S1);
+            if (ESS && tid == NT - 1) nent_r[(k + 2) & 3] = tile_nent[t + 2 * G];
+        }
         double *win = rsm + (k & 1) * WIN;
         const ProdBase pb = base_of<BATCHED>(bse, k & 3, P1, S1);
-        // the next tile's records into the other slot (last read by the tile before
-        // this one, whose term pass ended at a barrier)
-        if (ESS && has1)
-            stage_tile_es<NT>(esr + ((k + 1) & 1) * ESCAP, pb.ES, dsc[(k + 1) & 3].vbase, tile_nent[t + G]);
-        const int2 *es_t = esr + (k & 1) * ESCAP;
+        const unsigned *ws = nullptr;
+        const int2 *esl = nullptr;
+        if (ESS)
+        {
+            // the next tile's runs into the other slot (last read by the tile before
+            // this one, whose term pass ended at a barrier)
+            if (has1 && tid == 0)
+                rf_stage_tile(slots + ((k + 1) & 1) * sstride, wcap, dsc[(k + 1) & 3], nent_r[(k + 1) & 3], pb.W,
+                              pb.ES, pb.nV, &bars[(k + 1) & 1]);
+            if (!bad && !rf_mbar_wait(&bars[k & 1], (unsigned)(k >> 1) & 1u))
+            {
+                atomicOr(err, 1);
+                bad = true;
+            }
+            ws = slots + (k & 1) * sstride + (D.word_begin & 3);
+            esl = reinterpret_cast<const int2 *>(slots + (k & 1) * sstride + wcap) + (D.vbase & 1);
+        }
         const int nterms = D.nterms, nout = D.nout, vbase = D.vbase;
+        if (ESS)
+        {
+            for (int base = 0; base < nterms; base += RSTEP)
+            {
+                unsigned ww[RUNROLL];
+                int2 es[RUNROLL];
+                bool term[RUNROLL];
+#pragma unroll
+                for (int j = 0; j < RUNROLL; ++j)
+                {
+                    const int u = base + tid + j * NT;
+                    ww[j] = (!bad && u < nterms) ? ws[u] : (TERM_LIST << 12);
+                    term[j] = !(ww[j] & (TERM_LIST << 12));
+                    es[j] = term[j] ? esl[(int)(ww[j] >> 14)] : make_int2(0, 0);
+                }
+                double v[RUNROLL], x[RUNROLL];
+#pragma unroll
+                for (int j = 0; j < RUNROLL; ++j)
+                {
+                    v[j] = term[j] ? (pb.V ? pb.V[es[j].y] : 1.0) : 0.0;
+                    x[j] = term[j] ? pb.Ax[es[j].x + base + tid + j * NT] : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < RUNROLL; ++j)
+                {
+                    if (!term[j]) continue;
+                    const int p = (int)(ww[j] & 0xfffu);
+                    const double prod = __dmul_rn(v[j], x[j]);
+                    if (ww[j] & (TERM_PAIR << 12))
+                        atomicAdd(&win[p], prod);
+                    else
+                        win[p] = __dadd_rn(0.0, prod);
+                }
+            }
+        }
+        else
         for (int base = 0;; base += RSTEP)
         {
             const bool last = base + RSTEP >= nterms;
@@ -1305,10 +1419,7 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
             for (int j = 0; j < RUNROLL; ++j)
             {
                 term[j] = !(w[j] & (TERM_LIST << 12));
-                if (ESS)
-                    es[j] = term[j] ? es_t[(int)(w[j] >> 14)] : make_int2(0, 0);
-                else
-                    es[j] = term[j] ? pb.ES[vbase + (int)(w[j] >> 14)] : make_int2(0, 0);
+                es[j] = term[j] ? pb.ES[vbase + (int)(w[j] >> 14)] : make_int2(0, 0);
             }
             double v[RUNROLL], x[RUNROLL];
 #pragma unroll
@@ -1343,7 +1454,6 @@ __global__ void __launch_bounds__(NT, refill_minb<NT>()) k_tile_refill(
             for (int j = 0; j < RUNROLL; ++j) w[j] = wn[j];
             if (last) break;
         }
-        if (ESS) asm volatile("cp.async.wait_all;" ::: "memory"); // the next tile's records
         __syncthreads(); // the window is complete
         if (D.nlist > 0)
         {
@@ -2318,10 +2428,12 @@ void build_schedule(const ProductDesc &d, Product &P, const long long *ub, cudaS
     if (word_total > INT_MAX || x_total > INT_MAX)
         fail(SDL_ERR_OVERFLOW, "product: the tile rows' terms exceed the schedule's 31-bit offsets");
     P.tiles.reset(nt);
-    P.W.reset(std::max<long long>(1, word_total));
+    // W and ES carry 16 bytes past their ends: the staged refill's bulk copies round
+    // a tile's runs out to 16-byte boundaries
+    P.W.reset(std::max<long long>(1, word_total) + 4);
     P.X.reset(std::max<long long>(1, x_total));
     P.V.reset(std::max<long long>(1, nV));
-    P.ES.reset(std::max<long long>(1, nV));
+    P.ES.reset(std::max<long long>(1, nV) + 2);
     SDL_LAUNCH(k_tile_schedule<true>, P.ntiles, TILE_THREADS, build_smem_bytes(), s, na, rcls.get(),
                tile_start.get(), nullptr, nullptr, word_begin.get(), x_begin.get(), P.tiles.get(),
                P.W.get(), P.X.get(), P.ES.get());
@@ -2821,16 +2933,24 @@ namespace {
 // Resident refill CTAs per SM of one kernel instance (its attributes are set on the
 // first call, which is an eager one).
 template <bool BATCHED, int NT, bool ESS>
-int refill_per_sm()
+int refill_per_sm(size_t smem)
 {
+    // plain kernels: one size, cached; staged ones: the last size asked for
+    static size_t last_smem = 0;
     static int per_sm = 0;
-    if (!per_sm)
+    static std::mutex mu;
+    std::lock_guard<std::mutex> g(mu);
+    if (!per_sm || smem != last_smem)
     {
-        set_smem(k_tile_refill<BATCHED, NT, ESS>, refill_smem_bytes<NT, ESS>());
+        if (ESS)
+            SDL_CUDA(cudaFuncSetAttribute(k_tile_refill<BATCHED, NT, ESS>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STAGED_SMEM_MAX));
+        else
+            set_smem(k_tile_refill<BATCHED, NT, ESS>, smem);
         int n = 0;
-        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT, ESS>, NT,
-                                                               refill_smem_bytes<NT, ESS>()));
+        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT, ESS>, NT, smem));
         per_sm = std::max(1, n);
+        last_smem = smem;
     }
     return per_sm;
 }
@@ -2838,16 +2958,16 @@ int refill_per_sm()
 template <bool BATCHED, int NT, bool ESS = false>
 void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
                    cudaStream_t s, const ProdPtrs &vals, const ProdSched &sched, int ctas_per_sm,
-                   const int *tile_nent = nullptr)
+                   const int *tile_nent = nullptr, int wcap = 0, int ecap = 0)
 {
-    const int per_sm = refill_per_sm<BATCHED, NT, ESS>();
+    const size_t smem = ESS ? staged_smem_bytes(NT, wcap, ecap) : refill_smem_bytes<NT>();
+    const int per_sm = refill_per_sm<BATCHED, NT, ESS>(smem);
     const int use = ctas_per_sm > 0 ? std::min(ctas_per_sm, per_sm) : per_sm;
     const int grid = std::min(ntiles, runtime().num_sms * use);
     if (BATCHED)
     {
-        const size_t smem = refill_smem_bytes<NT, ESS>();
         SDL_LAUNCH((k_tile_refill<BATCHED, NT, ESS>), grid, NT, smem, s, tiles, ntiles, ptrs, scheds, vals, sched,
-                   runtime().d_error, tile_nent);
+                   runtime().d_error, tile_nent, wcap, ecap);
         return;
     }
     // programmatic dependent launch: the CTAs start while the entry-value kernel
@@ -2855,7 +2975,7 @@ void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, cons
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(NT);
-    cfg.dynamicSmemBytes = refill_smem_bytes<NT, ESS>();
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -2863,7 +2983,7 @@ void launch_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, cons
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     SDL_CUDA(cudaLaunchKernelEx(&cfg, k_tile_refill<BATCHED, NT, ESS>, tiles, ntiles, ptrs, scheds, vals, sched,
-                                runtime().d_error, tile_nent));
+                                runtime().d_error, tile_nent, wcap, ecap));
     g_launches.fetch_add(1, std::memory_order_relaxed);
 }
 
@@ -2874,10 +2994,22 @@ bool small_tile_refill(const Product &P)
     return P.cfg.refill_threads == REFILL_THREADS_SMALL && P.max_tile_out <= win_of<REFILL_THREADS_SMALL>();
 }
 
+// Slot capacities of the staged refill for P's tiles: the largest tile's words and
+// records, each rounded up to a 16-byte multiple plus the 16 bytes a run's rounded
+// start can add.
+void staged_caps(const Product &P, int &wcap, int &ecap)
+{
+    wcap = ((P.max_tile_terms + 3) & ~3) + 4;
+    ecap = ((P.max_tile_ent + 1) & ~1) + 2;
+}
+
 bool es_refill(const Product &P)
 {
     if (!P.cfg.refill_es || P.ntiles <= 0 || !P.tile_nent.get() || pipe_refill(P)) return false;
-    return P.max_tile_ent <= (small_tile_refill(P) ? escap_of<REFILL_THREADS_SMALL>() : escap_of<REFILL_THREADS>());
+    int wcap = 0, ecap = 0;
+    staged_caps(P, wcap, ecap);
+    const int nt = small_tile_refill(P) ? REFILL_THREADS_SMALL : REFILL_THREADS;
+    return staged_smem_bytes(nt, wcap, ecap) <= STAGED_SMEM_MAX;
 }
 
 bool pipe_refill(const Product &P)
@@ -2914,17 +3046,18 @@ void launch_refill_pipe(const Product &P, cudaStream_t s, const ProdPtrs &vals, 
 }
 
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
-                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm, bool small, const int *tile_nent)
+                 cudaStream_t s, ProdPtrs vals, ProdSched sched, int ctas_per_sm, bool small, const int *tile_nent,
+                 int wcap, int ecap)
 {
     if (ntiles <= 0) return;
     if (ptrs)
         launch_refill<true, REFILL_THREADS>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
     else if (tile_nent && small)
         launch_refill<false, REFILL_THREADS_SMALL, true>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm,
-                                                         tile_nent);
+                                                         tile_nent, wcap, ecap);
     else if (tile_nent)
         launch_refill<false, REFILL_THREADS, true>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm,
-                                                   tile_nent);
+                                                   tile_nent, wcap, ecap);
     else if (small)
         launch_refill<false, REFILL_THREADS_SMALL>(tiles, ntiles, ptrs, scheds, s, vals, sched, ctas_per_sm);
     else
@@ -3031,8 +3164,12 @@ void product_numeric(const Product &P, const double *Lx, const double *dvec, con
         if (pipe_refill(P))
             launch_refill_pipe(P, s, vals, S);
         else
+        {
+            int wcap = 0, ecap = 0;
+            staged_caps(P, wcap, ecap);
             tile_refill(P.tiles.get(), P.ntiles, nullptr, nullptr, s, vals, S, P.cfg.refill_ctas_per_sm,
-                        small_tile_refill(P), es_refill(P) ? P.tile_nent.get() : nullptr);
+                        small_tile_refill(P), es_refill(P) ? P.tile_nent.get() : nullptr, wcap, ecap);
+        }
     }
     if (P.big_lists)
     {
@@ -3230,7 +3367,7 @@ TuneResult product_autotune(Product &P, int reps, cudaStream_t s)
             }
             else
                 Q.cfg.refill_pipe = 0;
-            // and the entry-staged direct refill, when the tiles' records fit its slots
+            // and the staged direct refill, when its slots fit the largest tile
             if (!Q.cfg.refill_pipe)
             {
                 Q.cfg.refill_es = 1;

@@ -288,8 +288,9 @@ struct TuneConfig
     // whose tiles all fit its stages (1), or the direct one (0, the default: on the
     // patterns measured so far the direct refill is faster; the autotuner tries both)
     int refill_pipe = 0;
-    // the entry-staged direct refill (1) for plans whose tiles have few enough
-    // entries, or the plain direct one (0); the autotuner tries both
+    // the staged direct refill (1: tile words and entry records bulk-copied into
+    // shared memory a tile ahead) where its slots fit, or the plain direct one (0);
+    // the autotuner tries both
     int refill_es = 0;
 };
 // Autotuner results: the chosen configuration and what it measured.
@@ -413,10 +414,13 @@ void append_entry_chunks(long long nV, int prod, int chunk, std::vector<EntChunk
 // with null tables, from `vals` / `sched`.
 void tile_refill(const TileDesc *tiles, int ntiles, const ProdPtrs *ptrs, const ProdSched *scheds,
                  cudaStream_t s, ProdPtrs vals = ProdPtrs{}, ProdSched sched = ProdSched{},
-                 int ctas_per_sm = 0, bool small = false, const int *tile_nent = nullptr);
-// Whether a single product's refill runs the entry-staged direct kernel (each
-// tile's entry records copied into shared memory while the tile before it runs).
+                 int ctas_per_sm = 0, bool small = false, const int *tile_nent = nullptr, int wcap = 0,
+                 int ecap = 0);
+// Whether a single product's refill runs the staged direct kernel (each tile's term
+// words and entry records bulk-copied into shared memory while the tile before it
+// runs), and that kernel's slot capacities (words, records) for P's tiles.
 bool es_refill(const Product &P);
+void staged_caps(const Product &P, int &wcap, int &ecap);
 // Whether a single product's refill runs the 128-thread small-tile kernel.
 bool small_tile_refill(const Product &P);
 // Whether P's tiles are refilled by the pipelined kernel (its configuration asks for

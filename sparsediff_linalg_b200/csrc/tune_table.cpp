@@ -9,7 +9,7 @@
 //   <key> <warp_max_terms> <rows_per_cta_warp> <cta_threads_2k> <cta_threads_8k>
 //         <gmem_threads> <tile_budget> <refill_ctas_per_sm> <tile_max_terms>
 //         <refill_threads> <refill_kind> <refill_us>
-// refill_kind: 0 direct, 1 pipelined, 2 entry-staged direct. Lines without it (the
+// refill_kind: 0 direct, 1 pipelined, 2 staged direct. Lines without it (the
 // first version of the format) load as direct.
 #include <cstdio>
 #include <fstream>

@@ -120,8 +120,9 @@ class Product:
         return bool(used.value)
 
     def set_refill_staged(self, on):
-        """Entry-staged (True) or plain (False) direct tile refill; returns whether
-        the entry-staged refill will run for this plan."""
+        """Staged (True: tile words and entry records bulk-copied into shared
+        memory a tile ahead) or plain (False) direct tile refill; returns whether the
+        staged refill will run for this plan."""
         used = C.c_int()
         check(lib().sdl_product_set_refill_staged(self.handle, 1 if on else 0, C.byref(used)))
         return bool(used.value)
@@ -140,7 +141,7 @@ class Product:
                                        C.byref(f[2])))
         th, tm = C.c_int(), C.c_int()
         check(lib().sdl_product_refill_shape(self.handle, C.byref(th), C.byref(tm)))
-        kind = "pipelined" if self.refill_pipelined() else "entry-staged" if self.refill_staged() else "direct"
+        kind = "pipelined" if self.refill_pipelined() else "staged" if self.refill_staged() else "direct"
         return {"refill": kind, "warp_max_terms": i[0].value, "rows_per_cta_warp": i[1].value, "tile_budget": i[2].value,
                 "refill_ctas_per_sm": i[3].value, "refill_threads": th.value, "tile_max_terms": tm.value,
                 "refill_us": round(f[0].value, 2),

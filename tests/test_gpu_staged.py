@@ -1,5 +1,6 @@
-"""The entry-staged direct refill (each tile's entry records copied into shared
-memory while the tile before it runs): on the 128-thread small-tile plan and on the
+"""The staged direct refill (each tile's term words and entry records bulk-copied
+into shared memory by one thread while the tile before it runs, completing on an
+mbarrier): on the 128-thread small-tile plan and on the
 default 256-thread plan it must give the bits of the plain direct refill and of the
 oracle -- outputs of one term, pairs (added atomically), lists of up to ~70 terms over
 16 decades of magnitude, unit products, products read straight from L.x, refills with
@@ -63,8 +64,8 @@ def test_staged_refill_matches_plain_and_oracle(sdl, orc, case, plan):
     if plan == "small_tiles":
         P.replan(tile_budget=512, tile_max_terms=512, refill_threads=128)
     if not P.set_refill_staged(True):
-        assert plan == "default", "tiles of at most 512 terms always fit the staged refill"
-        pytest.skip("this default plan's tiles hold more entries than the staged refill's slots")
+        assert plan == "default", "the small-tile plan's tiles always fit the staged refill"
+        pytest.skip("this default plan's largest tile does not fit the staged refill's slots")
     for rnd in range(2):
         if rnd:
             A = (A[0], A[1], rng.standard_normal(len(A[1])), A[3], A[4])
@@ -104,4 +105,4 @@ def test_staged_and_pipelined_switches_exclude_each_other(sdl):
     assert P.set_refill_staged(True) and P.refill_staged() and not P.refill_pipelined()
     assert P.set_refill_pipe(True) and P.refill_pipelined() and not P.refill_staged()
     assert P.set_refill_staged(True) and not P.refill_pipelined()
-    assert P.tuning()["refill"] == "entry-staged"
+    assert P.tuning()["refill"] == "staged"
