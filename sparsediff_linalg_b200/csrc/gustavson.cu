@@ -2723,6 +2723,15 @@ void oneshot_launch(const OneShotArgs &oa, const int *lists, const int *cnt, con
 }
 } // namespace
 
+namespace {
+// Term counts of the listed rows.
+__global__ void k_gather_row_terms(const int *__restrict__ rows, int n, const long long *__restrict__ terms,
+                                   long long *__restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = terms[rows[q]];
+}
+} // namespace
+
 void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const Mlp &net, float margin,
                              const double *Lx, const double *dvec, const double *Ax, Product &P,
                              DevBuf<double> &Cx, LearnedStats &st, cudaStream_t s)
@@ -2824,26 +2833,49 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
         const long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
         const int slots = (int)std::min<long long>(
             {(long long)rt.num_sms * GMEM_CTAS_PER_SM, max_slots, (long long)cnt[SYM_BITMAP]});
-        DevBuf<int> posmap((size_t)slots * per_slot);
+        // the column -> position maps need no clearing (a row reads only its own
+        // columns' entries): the one-shot rows' column scratch, dead once compacted
+        // into C, holds them when it is large enough
+        DevBuf<int> posmap_own;
+        int *posmap = tcol.get();
+        if (tcol.n < (size_t)slots * per_slot)
+        {
+            posmap_own.reset((size_t)slots * per_slot);
+            posmap = posmap_own.get();
+        }
         NumArgs na{d.Lp, d.Li, d.L_map, d.L_m, P.n_L, Lx, dvec, d.Ap, d.Ai, Ax, P.Cp.get(), P.Ci.get(), Cx.get(),
                    rt.d_error};
         // the large rows by term count, largest first, handed out by a counter: the
-        // largest rows start first and no CTA is left with several of them
+        // largest rows start first and no CTA is left with several of them (only the
+        // large rows' counts come to the host)
         const int nbr = cnt[SYM_BITMAP];
         std::vector<int> hrows(nbr);
-        std::vector<long long> hub(m_out);
-        SDL_CUDA(cudaMemcpyAsync(hrows.data(), lists.get() + off[SYM_BITMAP], (size_t)nbr * sizeof(int),
-                                 cudaMemcpyDeviceToHost, s));
-        SDL_CUDA(cudaMemcpyAsync(hub.data(), P.row_terms.get() ? P.row_terms.get() : ub.get(),
-                                 (size_t)m_out * sizeof(long long), cudaMemcpyDeviceToHost, s));
-        SDL_CUDA(cudaStreamSynchronize(s));
-        std::stable_sort(hrows.begin(), hrows.end(), [&](int x, int y) { return hub[x] > hub[y]; });
+        std::vector<long long> hub(nbr);
+        {
+            DevBuf<long long> big_terms((size_t)nbr);
+            SDL_LAUNCH(k_gather_row_terms, grid_for(nbr, 256, rt.num_sms * 4), 256, 0, s,
+                       lists.get() + off[SYM_BITMAP], nbr, P.row_terms.get() ? P.row_terms.get() : ub.get(),
+                       big_terms.get());
+            SDL_CUDA(cudaMemcpyAsync(hrows.data(), lists.get() + off[SYM_BITMAP], (size_t)nbr * sizeof(int),
+                                     cudaMemcpyDeviceToHost, s));
+            SDL_CUDA(cudaMemcpyAsync(hub.data(), big_terms.get(), (size_t)nbr * sizeof(long long),
+                                     cudaMemcpyDeviceToHost, s));
+            SDL_CUDA(cudaStreamSynchronize(s));
+        }
+        std::vector<int> idx(nbr);
+        for (int q = 0; q < nbr; ++q) idx[q] = q;
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return hub[x] > hub[y]; });
+        {
+            std::vector<int> sorted(nbr);
+            for (int q = 0; q < nbr; ++q) sorted[q] = hrows[idx[q]];
+            hrows.swap(sorted);
+        }
         DevBuf<int> order((size_t)nbr), counter(1);
         SDL_CUDA(cudaMemcpyAsync(order.get(), hrows.data(), (size_t)nbr * sizeof(int), cudaMemcpyHostToDevice, s));
         SDL_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(int), s));
         const size_t sm = gmem_smem_bytes();
         set_smem(k_num_gmem, sm);
-        SDL_LAUNCH(k_num_gmem, slots, GMEM_THREADS, sm, s, order.get(), nbr, na, posmap.get(), P.n, nullptr,
+        SDL_LAUNCH(k_num_gmem, slots, GMEM_THREADS, sm, s, order.get(), nbr, na, posmap, P.n, nullptr,
                    counter.get());
         SDL_CUDA(cudaStreamSynchronize(s)); // hrows / hub and the queue are freed on return
         if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "one-shot product: a term column is missing from its row");
