@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--learned-matrices", type=int, default=200)
     ap.add_argument("--learned-runs", type=int, default=5,
                     help="new-pattern builds per path in the skewed case (median and spread reported)")
+    ap.add_argument("--learned-size", type=int, nargs=2, default=[1_000_000, 20_000_000],
+                    metavar=("ROWS", "NNZ"),
+                    help="skewed case: rows (= columns) of A and B and their target nonzeros "
+                         "(the configuration is 1000000 20000000; smaller for profiling)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the CPU leg's comparison of every sub-result with the oracle")
     ap.add_argument("--stub", action="store_true",
@@ -1076,7 +1080,8 @@ def run_learned(args, dev, check=False):
     from sparsediff_linalg_b200.train_scheduler import train
     net, info = train(matrices=args.learned_matrices, epochs=8)
     t0 = time.perf_counter()
-    (Ap, Ai, Ax), (Bp, Bi, Bx), scales = wl.skewed_device(seed=0)
+    rows, target = args.learned_size
+    (Ap, Ai, Ax), (Bp, Bi, Bx), scales = wl.skewed_device(seed=0, m=rows, n=rows, target=target)
     gen_s = time.perf_counter() - t0
     m = Ap.numel() - 1
 
@@ -1125,8 +1130,9 @@ def run_learned(args, dev, check=False):
                 torch.equal(cx_plain[:Q.nnz].view(torch.int64), cx_learned.view(torch.int64)))
     st = Q.stats
     med = lambda v: round(statistics.median(v), 2)  # noqa: E731
-    res = {"workload": "C = A B, A and B 1M x 1M, Zipf(1.5) row lengths scaled to ~20M nnz, cap 50k; "
-                       "the pattern met for the first time (structure + first values)",
+    short = lambda v: f"{v // 10**6}M" if v % 10**6 == 0 else f"{v // 1000}k" if v % 1000 == 0 else str(v)  # noqa: E731
+    res = {"workload": f"C = A B, A and B {short(rows)} x {short(rows)}, Zipf(1.5) row lengths scaled to "
+                       f"~{short(target)} nnz, cap 50k; the pattern met for the first time (structure + first values)",
            "nnz_A": int(Ai.numel()), "nnz_B": int(Bi.numel()), "terms": int(Q.terms),
            "nnz_C": int(Q.nnz), "zipf_scale": [round(x, 6) for x in scales], "runs": runs,
            "plain": {"new_pattern_ms_median": med(plain_ms), "new_pattern_ms_range": [round(min(plain_ms), 2),
