@@ -1810,6 +1810,20 @@ __host__ __device__ constexpr size_t gmem_smem_bytes()
 // with its term index, the smallest index of a slot adds its product, and the round
 // repeats until no term is pending -- so the terms of one output are added in
 // ascending term order (upstream's visiting order), whichever threads hold them.
+// RANK: the map is a rank structure instead -- per 64 columns one 16-byte entry
+// {column bitmap of the row's columns in the word, position of the word's first
+// column}, position = prefix + popcount of the lower bits -- 1/16 of the plain map's
+// bytes, so the CTAs' maps (n / 4 bytes each) stay in L2; the row writes one entry
+// per word it touches and reads only those, so it needs no clearing either.
+__device__ __forceinline__ int rank_pos(const uint4 *__restrict__ rmap, int j)
+{
+    const uint4 e = rmap[j >> 6];
+    const unsigned long long bits = ((unsigned long long)e.y << 32) | e.x;
+    const unsigned long long below = bits & ((1ull << (j & 63)) - 1ull);
+    return (int)e.z + __popcll(below);
+}
+
+template <bool RANK>
 __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(const int *__restrict__ rows, int count, NumArgs a,
                                                           int *__restrict__ posmap_all, int n,
                                                           const ProdPtrs *__restrict__ vals,
@@ -1824,6 +1838,7 @@ __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(con
     int *claim = elen + GMEM_CHUNK;
     int *scr = claim + GMEM_CLAIM;
     int *posmap = posmap_all + (long long)blockIdx.x * n;
+    uint4 *rmap = reinterpret_cast<uint4 *>(posmap_all) + (long long)blockIdx.x * ((n + 63) / 64);
     __shared__ int it_sh;
     // rows taken in list order: from a shared counter when given (the list is then
     // ordered by work, largest first), else every gridDim-th
@@ -1843,7 +1858,25 @@ __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(con
         double *acc = a.Cx + cs;
         for (int q = threadIdx.x; q < nr; q += blockDim.x)
         {
-            posmap[a.Ci[cs + q]] = q;
+            const int j = a.Ci[cs + q];
+            if (RANK)
+            {
+                // the thread holding a word's first column writes the word's entry
+                const int w = j >> 6;
+                if (q == 0 || (a.Ci[cs + q - 1] >> 6) != w)
+                {
+                    unsigned long long bits = 0;
+                    for (int r = q; r < nr; ++r)
+                    {
+                        const int jr = a.Ci[cs + r];
+                        if ((jr >> 6) != w) break;
+                        bits |= 1ull << (jr & 63);
+                    }
+                    rmap[w] = make_uint4((unsigned)bits, (unsigned)(bits >> 32), (unsigned)q, 0u);
+                }
+            }
+            else
+                posmap[j] = q;
             acc[q] = 0.0;
         }
         for (int q = threadIdx.x; q < GMEM_CLAIM; q += blockDim.x) claim[q] = INT_MAX;
@@ -1903,7 +1936,7 @@ __global__ void __launch_bounds__(GMEM_THREADS, GMEM_CTAS_PER_SM) k_num_gmem(con
                         int jj = es[e] + u - (incl[e] - elen[e]);
                         int j = a.Ai[jj];
                         prod[k] = __dmul_rn(ev[e], a.Ax[jj]);
-                        pos[k] = posmap[j];
+                        pos[k] = RANK ? rank_pos(rmap, j) : posmap[j];
                         if (pos[k] < 0 || pos[k] >= nr)
                             atomicOr(a.err, 1);
                         else
@@ -2078,6 +2111,7 @@ __global__ void __launch_bounds__(512, 2) k_big_terms(const int *__restrict__ ro
     ch.len = ch.s + blockDim.x;
     ch.scr = ch.len + blockDim.x;
     int *posmap = posmap_all + (long long)blockIdx.x * n;
+    uint4 *rmap = reinterpret_cast<uint4 *>(posmap_all) + (long long)blockIdx.x * ((n + 63) / 64);
     __shared__ int q_sh;
     // the rows in the order `order` gives (largest first), handed out by a counter
     for (;;)
@@ -2829,13 +2863,14 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
     // position map, same-position terms applied in visiting order
     if (cnt[SYM_BITMAP] && P.nnz > 0)
     {
-        const long long per_slot = std::max(1, P.n);
+        // rank maps: per CTA one 16-byte entry (4 ints) per 64 columns
+        const long long per_slot = 4LL * ((std::max(1, P.n) + 63) / 64);
         const long long max_slots = std::max<long long>(1, (2LL << 30) / (per_slot * 4));
         const int slots = (int)std::min<long long>(
             {(long long)rt.num_sms * GMEM_CTAS_PER_SM, max_slots, (long long)cnt[SYM_BITMAP]});
-        // the column -> position maps need no clearing (a row reads only its own
-        // columns' entries): the one-shot rows' column scratch, dead once compacted
-        // into C, holds them when it is large enough
+        // the maps need no clearing (a row reads only the entries it wrote): the
+        // one-shot rows' column scratch, dead once compacted into C, holds them when
+        // it is large enough
         DevBuf<int> posmap_own;
         int *posmap = tcol.get();
         if (tcol.n < (size_t)slots * per_slot)
@@ -2874,8 +2909,8 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
         SDL_CUDA(cudaMemcpyAsync(order.get(), hrows.data(), (size_t)nbr * sizeof(int), cudaMemcpyHostToDevice, s));
         SDL_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(int), s));
         const size_t sm = gmem_smem_bytes();
-        set_smem(k_num_gmem, sm);
-        SDL_LAUNCH(k_num_gmem, slots, GMEM_THREADS, sm, s, order.get(), nbr, na, posmap, P.n, nullptr,
+        set_smem(k_num_gmem<true>, sm);
+        SDL_LAUNCH(k_num_gmem<true>, slots, GMEM_THREADS, sm, s, order.get(), nbr, na, posmap, P.n, nullptr,
                    counter.get());
         SDL_CUDA(cudaStreamSynchronize(s)); // hrows / hub and the queue are freed on return
         if (take_device_error(s)) fail(SDL_ERR_INTERNAL, "one-shot product: a term column is missing from its row");
@@ -3127,8 +3162,8 @@ void big_rows_refill(const Product &P, const double *Lx, const double *dvec, con
     {
         const int th = GMEM_THREADS;
         const size_t sm = gmem_smem_bytes();
-        set_smem(k_num_gmem, sm);
-        SDL_LAUNCH(k_num_gmem, P.gmem_slots, th, sm, s, rows + off[NUM_GMEM], cnt[NUM_GMEM], na,
+        set_smem(k_num_gmem<false>, sm);
+        SDL_LAUNCH(k_num_gmem<false>, P.gmem_slots, th, sm, s, rows + off[NUM_GMEM], cnt[NUM_GMEM], na,
                    P.gmem_scratch.get(), P.n, vals, nullptr);
     }
 }
@@ -3164,8 +3199,8 @@ void big_rows_refill_scratch(const Product &P, const double *Lx, const double *d
     {
         const int th = GMEM_THREADS;
         const size_t sm = gmem_smem_bytes();
-        set_smem(k_num_gmem, sm);
-        SDL_LAUNCH(k_num_gmem, std::min(slots, cnt[NUM_GMEM]), th, sm, s, rows + off[NUM_GMEM],
+        set_smem(k_num_gmem<false>, sm);
+        SDL_LAUNCH(k_num_gmem<false>, std::min(slots, cnt[NUM_GMEM]), th, sm, s, rows + off[NUM_GMEM],
                    cnt[NUM_GMEM], na, posmap, P.n, nullptr, nullptr);
     }
 }
