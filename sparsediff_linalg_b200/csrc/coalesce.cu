@@ -188,6 +188,13 @@ void coalesce_order_fill(const int *ostart, const int *perm, const double *x, co
 // The sums are the same sums in the same order (ascending triplet per output,
 // from +0.0), so the result is bit-identical to the one-pass refill.
 namespace {
+// Outputs per bucket (a power of two; more when the buckets would exceed
+// CO_MAX_BUCKETS): the buckets being summed in pass 2 stay in L2, and a chunk's
+// run per bucket is chunk / buckets values long.
+#ifndef SDL_COALESCE_SPAN_LOG2
+#define SDL_COALESCE_SPAN_LOG2 20
+#endif
+constexpr int COALESCE_SPAN_LOG2 = SDL_COALESCE_SPAN_LOG2;
 constexpr int CO_CHUNK = 4096;
 constexpr int CO_THREADS = 256;
 constexpr int CO_MAX_BUCKETS = 512;
@@ -325,7 +332,7 @@ void coalesce_bucket_build(const int *ostart, const int *perm, int n, int nout, 
     B = CoalesceBuckets{};
     if (n < COALESCE_BUCKET_MIN || nout <= 0) return;
     Runtime &rt = runtime();
-    int span = 1 << 17;
+    int span = 1 << COALESCE_SPAN_LOG2;
     while ((long long)(nout + span - 1) / span > CO_MAX_BUCKETS) span <<= 1;
     const int nb = (nout + span - 1) / span;
     const int nchunks = (int)(((long long)n + CO_CHUNK - 1) / CO_CHUNK);
