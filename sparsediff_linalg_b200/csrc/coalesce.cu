@@ -195,6 +195,11 @@ namespace {
 #define SDL_COALESCE_SPAN_LOG2 20
 #endif
 constexpr int COALESCE_SPAN_LOG2 = SDL_COALESCE_SPAN_LOG2;
+// CTAs per SM of the gather pass over the buckets
+#ifndef SDL_COALESCE_FILL_CTAS
+#define SDL_COALESCE_FILL_CTAS 8
+#endif
+constexpr int COALESCE_FILL_CTAS = SDL_COALESCE_FILL_CTAS;
 constexpr int CO_CHUNK = 4096;
 constexpr int CO_THREADS = 256;
 constexpr int CO_MAX_BUCKETS = 512;
@@ -371,9 +376,10 @@ void coalesce_bucket_fill(const CoalesceBuckets &B, const int *ostart, const dou
 {
     SDL_LAUNCH(k_cb_scatter, B.nchunks, CO_THREADS, 0, s, x, f, B.n, B.nb, B.lperm.get(), B.cbound.get(), B.dst.get(),
                B.buf.get());
-    // few outputs in flight (148 x 8 CTAs x 256 threads x 4 outputs: about eight
-    // buckets), so the buckets being summed stay in L2
-    const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)nout + 255) / 256, 148LL * 8));
+    // few outputs in flight (SMs x COALESCE_FILL_CTAS x 256 threads x 4 outputs: a
+    // bucket or two), so the buckets being summed stay in L2
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>(((long long)nout + 255) / 256, (long long)runtime().num_sms * COALESCE_FILL_CTAS));
     SDL_LAUNCH(k_coal_fill, grid, 256, 0, s, ostart, B.perm2.get(), B.buf.get(), nullptr, nout, C);
 }
 
