@@ -61,7 +61,10 @@ __global__ void k_transpose_blocks(const BlkDesc *__restrict__ descs, int nblk, 
     }
 }
 
-constexpr int BC_COLS = 32; // output columns of a CTA tile
+#ifndef SDL_BC_COLS
+#define SDL_BC_COLS 32
+#endif
+constexpr int BC_COLS = SDL_BC_COLS; // output columns of a CTA tile
 constexpr int BC_ROWS = 64; // block rows per pass (two per lane)
 
 // One CTA: output columns [c0, c0 + 32) of one block; each warp takes four columns
