@@ -624,12 +624,30 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
 // Compaction of per-row slot ranges into C: row r's Cp[r + 1] - Cp[r] outputs are
 // copied from its slots (off0[r] in src0, or off1[r] in src1 for rows flagged in
 // sel) to C.i (and C.x when value sources are given, except for rows flagged in
-// late). A CTA takes COMPACT_ROWS consecutive rows and its threads stride over all
-// of their outputs (each output finds its row by a search over the CTA's row
-// offsets in shared memory), so rows of one or two outputs -- most rows of a skewed
-// product -- do not leave a warp idle.
-constexpr int COMPACT_ROWS = 256;
+// late). The work is cut by outputs, not rows: CTA chunks of COMPACT_Q consecutive
+// outputs (a skewed product's longest rows are shared out instead of landing on
+// one CTA), each chunk's first row found beforehand (k_compact_chunks). A chunk's
+// rows are staged COMPACT_R at a time (row offsets, slot offsets, flags) and its
+// threads stride over the outputs, each finding its row by a search over the
+// staged offsets, so rows of one or two outputs do not leave a warp idle.
+constexpr int COMPACT_Q = 2048;
+constexpr int COMPACT_R = 1024;
+
+// first_row[c] = the row holding output c * COMPACT_Q: each non-empty row marks the
+// chunk starts inside its range.
+__global__ void k_compact_chunks(const int *__restrict__ Cp, int m_out, int *__restrict__ first_row)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < m_out;
+         r += (long long)gridDim.x * blockDim.x)
+    {
+        const int q0 = Cp[r], q1 = Cp[r + 1];
+        for (long long c = ((long long)q0 + COMPACT_Q - 1) / COMPACT_Q; c * COMPACT_Q < q1; ++c)
+            first_row[c] = (int)r;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_compact_rows(const int *__restrict__ Cp, int m_out,
+                                                      const int *__restrict__ first_row,
                                                       const long long *__restrict__ off0,
                                                       const long long *__restrict__ off1,
                                                       const unsigned char *__restrict__ sel,
@@ -639,64 +657,84 @@ __global__ void __launch_bounds__(256) k_compact_rows(const int *__restrict__ Cp
                                                       const double *__restrict__ src1v, int *__restrict__ Ci,
                                                       double *__restrict__ Cx)
 {
-    __shared__ int cp[COMPACT_ROWS + 1];
-    __shared__ long long so[COMPACT_ROWS];
-    __shared__ unsigned char fl[COMPACT_ROWS];
-    for (long long r0 = (long long)blockIdx.x * COMPACT_ROWS; r0 < m_out; r0 += (long long)gridDim.x * COMPACT_ROWS)
+    __shared__ int cp[COMPACT_R + 1];
+    __shared__ long long so[COMPACT_R];
+    __shared__ unsigned char fl[COMPACT_R];
+    const int total = Cp[m_out];
+    for (long long c = blockIdx.x; c * COMPACT_Q < total; c += gridDim.x)
     {
-        const int nr = (int)(m_out - r0 < COMPACT_ROWS ? m_out - r0 : COMPACT_ROWS);
-        for (int i = threadIdx.x; i <= nr; i += blockDim.x) cp[i] = Cp[r0 + i];
-        for (int i = threadIdx.x; i < nr; i += blockDim.x)
+        const int q0 = (int)(c * COMPACT_Q);
+        const int q1 = (int)min((long long)total, c * COMPACT_Q + COMPACT_Q);
+        for (int r0 = first_row[c];;)
         {
-            const bool alt = sel && sel[r0 + i];
-            so[i] = alt ? off1[r0 + i] : off0[r0 + i];
-            fl[i] = (unsigned char)((alt ? 1 : 0) | (late && late[r0 + i] ? 2 : 0));
-        }
-        __syncthreads();
-        const int q0 = cp[0], q1 = cp[nr];
-        constexpr int ILP = 4; // outputs per thread whose loads are in flight together
-        for (int qb = q0 + threadIdx.x; qb < q1; qb += ILP * blockDim.x)
-        {
-            int col[ILP], lo[ILP];
-            double val[ILP];
-#pragma unroll
-            for (int k = 0; k < ILP; ++k)
+            const int nr = min(COMPACT_R, m_out - r0);
+            __syncthreads(); // the previous rows' offsets are no longer read
+            for (int i = threadIdx.x; i <= nr; i += blockDim.x) cp[i] = Cp[r0 + i];
+            for (int i = threadIdx.x; i < nr; i += blockDim.x)
             {
-                const int q = qb + k * blockDim.x;
-                lo[k] = -1;
-                if (q >= q1) continue;
-                int l = 0, hi = nr; // last row i with cp[i] <= q
-                while (hi - l > 1)
+                const bool alt = sel && sel[r0 + i];
+                so[i] = alt ? off1[r0 + i] : off0[r0 + i];
+                fl[i] = (unsigned char)((alt ? 1 : 0) | (late && late[r0 + i] ? 2 : 0));
+            }
+            __syncthreads();
+            const int qa = max(q0, cp[0]), qb = min(q1, cp[nr]);
+            constexpr int ILP = 4; // outputs per thread whose loads are in flight together
+            for (int qq = qa + threadIdx.x; qq < qb; qq += ILP * blockDim.x)
+            {
+                int col[ILP], lo[ILP];
+                double val[ILP];
+#pragma unroll
+                for (int k = 0; k < ILP; ++k)
                 {
-                    const int mid = (l + hi) >> 1;
-                    if (cp[mid] <= q)
-                        l = mid;
-                    else
-                        hi = mid;
+                    const int q = qq + k * blockDim.x;
+                    lo[k] = -1;
+                    if (q >= qb) continue;
+                    int l = 0, hi = nr; // last row i with cp[i] <= q
+                    while (hi - l > 1)
+                    {
+                        const int mid = (l + hi) >> 1;
+                        if (cp[mid] <= q)
+                            l = mid;
+                        else
+                            hi = mid;
+                    }
+                    lo[k] = l;
+                    const long long at = so[l] + (q - cp[l]);
+                    const bool alt = fl[l] & 1;
+                    col[k] = alt ? src1c[at] : src0c[at];
+                    if (Cx && !(fl[l] & 2)) val[k] = alt ? src1v[at] : src0v[at];
                 }
-                lo[k] = l;
-                const long long at = so[l] + (q - cp[l]);
-                const bool alt = fl[l] & 1;
-                col[k] = alt ? src1c[at] : src0c[at];
-                if (Cx && !(fl[l] & 2)) val[k] = alt ? src1v[at] : src0v[at];
-            }
 #pragma unroll
-            for (int k = 0; k < ILP; ++k)
-            {
-                if (lo[k] < 0) continue;
-                const int q = qb + k * blockDim.x;
-                Ci[q] = col[k];
-                if (Cx && !(fl[lo[k]] & 2)) Cx[q] = val[k];
+                for (int k = 0; k < ILP; ++k)
+                {
+                    if (lo[k] < 0) continue;
+                    const int q = qq + k * blockDim.x;
+                    Ci[q] = col[k];
+                    if (Cx && !(fl[lo[k]] & 2)) Cx[q] = val[k];
+                }
             }
+            if (cp[nr] >= q1 || r0 + nr >= m_out) break; // the chunk's last output is done
+            r0 += nr;
         }
-        __syncthreads();
     }
 }
 
-int compact_grid(int m_out)
+// C.i (and C.x) of every row from its slot range (see k_compact_rows).
+void compact_rows(const int *Cp, int m_out, int nnz, const long long *off0, const long long *off1,
+                  const unsigned char *sel, const unsigned char *late, const int *src0c, const int *src1c,
+                  const double *src0v, const double *src1v, int *Ci, double *Cx, cudaStream_t s)
 {
-    return (int)std::max<long long>(1, std::min<long long>(((long long)m_out + COMPACT_ROWS - 1) / COMPACT_ROWS,
-                                                           (long long)runtime().num_sms * 16));
+    if (nnz <= 0 || m_out <= 0) return;
+    Runtime &rt = runtime();
+    const long long nchunks = ((long long)nnz + COMPACT_Q - 1) / COMPACT_Q;
+    DevBuf<int> first_row((size_t)nchunks);
+    const int cgrid = (int)std::max<long long>(1, std::min<long long>(((long long)m_out + 255) / 256,
+                                                                      (long long)rt.num_sms * 8));
+    SDL_LAUNCH(k_compact_chunks, cgrid, 256, 0, s, Cp, m_out, first_row.get());
+    const int grid = (int)std::max<long long>(1, std::min<long long>(nchunks, (long long)rt.num_sms * 8));
+    SDL_LAUNCH(k_compact_rows, grid, 256, 0, s, Cp, m_out, first_row.get(), off0, off1, sel, late, src0c, src1c,
+               src0v, src1v, Ci, Cx);
+    SDL_CUDA(cudaStreamSynchronize(s)); // first_row is released on return
 }
 
 // ------------------------------------------------------------ numeric kernels
@@ -2622,8 +2660,8 @@ void product_symbolic(const ProductDesc &d, const TuneConfig &cfg, Product &P, c
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
     if (P.nnz > 0)
-        SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, ub_off.get(), nullptr, nullptr,
-                   nullptr, tmp.get(), nullptr, nullptr, nullptr, P.Ci.get(), nullptr);
+        compact_rows(P.Cp.get(), m_out, P.nnz, ub_off.get(), nullptr, nullptr, nullptr, tmp.get(), nullptr, nullptr,
+                     nullptr, P.Ci.get(), nullptr, s);
     P.scratch_bytes = (long long)tmp.bytes();
     build_schedule(d, P, ub.get(), s);
     if (keep_row_terms) P.row_terms = std::move(ub);
@@ -2693,8 +2731,8 @@ void product_symbolic_learned(const ProductDesc &d, const TuneConfig &cfg, const
     P.nnz = exclusive_scan_i32_checked(row_nnz.get(), P.Cp.get(), m_out, s);
     P.Ci.reset(std::max(1, P.nnz));
     if (P.nnz > 0)
-        SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, cap_off.get(), fb_off.get(),
-                   overflow.get(), nullptr, tmp.get(), fb.get(), nullptr, nullptr, P.Ci.get(), nullptr);
+        compact_rows(P.Cp.get(), m_out, P.nnz, cap_off.get(), fb_off.get(), overflow.get(), nullptr, tmp.get(),
+                     fb.get(), nullptr, nullptr, P.Ci.get(), nullptr, s);
     {
         DevBuf<unsigned long long> hits(1);
         SDL_CUDA(cudaMemsetAsync(hits.get(), 0, 8, s));
@@ -2857,8 +2895,8 @@ void product_oneshot_learned(const ProductDesc &d, const TuneConfig &cfg, const 
     SDL_LAUNCH(k_mark_class, grid_for(m_out, 256, rt.num_sms * 8), 256, 0, s, cls.get(), m_out, (int)SYM_BITMAP,
                late.get());
     if (P.nnz > 0)
-        SDL_LAUNCH(k_compact_rows, compact_grid(m_out), 256, 0, s, P.Cp.get(), m_out, cap_off.get(), fb_off.get(),
-                   overflow.get(), late.get(), tcol.get(), fcol.get(), tval.get(), fval.get(), P.Ci.get(), Cx.get());
+        compact_rows(P.Cp.get(), m_out, P.nnz, cap_off.get(), fb_off.get(), overflow.get(), late.get(), tcol.get(),
+                     fcol.get(), tval.get(), fval.get(), P.Ci.get(), Cx.get(), s);
     // values of the larger rows: accumulated in C.x through a per-CTA column ->
     // position map, same-position terms applied in visiting order
     if (cnt[SYM_BITMAP] && P.nnz > 0)
