@@ -554,7 +554,9 @@ __global__ void k_mark_class(const unsigned char *__restrict__ cls, int m_out, i
 
 // Large rows: mark columns in a shared-memory bitmap, one column window at a time;
 // reading the bitmap word by word yields the columns in ascending order.
-__global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a, int words)
+// Rows taken in list order: from a shared counter when given (the list is then
+// ordered by work, largest first), else every gridDim-th.
+__global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a, int words, int *__restrict__ next_row)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     unsigned *bm = (unsigned *)smraw;
@@ -565,9 +567,18 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
     ch.scr = ch.len + blockDim.x;
     ch.v = nullptr;
     __shared__ int tot_sh;
+    __shared__ int it_sh;
     const int wbits = words * 32;
-    for (int it = blockIdx.x; it < count; it += gridDim.x)
+    for (int it = blockIdx.x;;)
     {
+        if (next_row)
+        {
+            __syncthreads();
+            if (threadIdx.x == 0) it_sh = atomicAdd(next_row, 1);
+            __syncthreads();
+            it = it_sh;
+        }
+        if (it >= count) break;
         int row = rows[it];
         int b = row / a.L_m, r = row - b * a.L_m;
         int ls = a.Lp[r], le = a.Lp[r + 1];
@@ -618,7 +629,16 @@ __global__ void k_sym_bitmap(const int *__restrict__ rows, int count, SymArgs a,
             if (running > cap) a.overflow[row] = 1;
         }
         __syncthreads();
+        if (!next_row) it += gridDim.x;
     }
+}
+
+// Scratch span (work) of each listed row: off[row + 1] - off[row].
+__global__ void k_row_spans(const int *__restrict__ rows, int n, const long long *__restrict__ off,
+                            long long *__restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        out[q] = off[rows[q] + 1] - off[rows[q]];
 }
 
 // Compaction of per-row slot ranges into C: row r's Cp[r + 1] - Cp[r] outputs are
@@ -2092,8 +2112,34 @@ void sym_launch(const SymArgs &sa, const int *lists, const int *cnt, const int *
         int words = (int)std::max<long long>(32, w);
         size_t sm = (size_t)words * 4 + fixed;
         set_smem(k_sym_bitmap, sm);
-        SDL_LAUNCH(k_sym_bitmap, grid_for(cnt[SYM_BITMAP], 1, rt.num_sms * 2), th, sm, s,
-                   lists + off[SYM_BITMAP], cnt[SYM_BITMAP], sa, words);
+        const int nbr = cnt[SYM_BITMAP];
+        const int grid = grid_for(nbr, 1, rt.num_sms * 2);
+        if (nbr <= grid)
+            SDL_LAUNCH(k_sym_bitmap, grid, th, sm, s, lists + off[SYM_BITMAP], nbr, sa, words, nullptr);
+        else
+        {
+            // more rows than CTAs: handed out largest first (by their scratch span) from
+            // a counter, so no CTA is left with several of the largest rows
+            DevBuf<long long> span((size_t)nbr);
+            SDL_LAUNCH(k_row_spans, grid_for(nbr, 256, rt.num_sms * 4), 256, 0, s, lists + off[SYM_BITMAP], nbr,
+                       sa.ub_off, span.get());
+            std::vector<int> hrows(nbr);
+            std::vector<long long> hspan(nbr);
+            SDL_CUDA(cudaMemcpyAsync(hrows.data(), lists + off[SYM_BITMAP], (size_t)nbr * sizeof(int),
+                                     cudaMemcpyDeviceToHost, s));
+            SDL_CUDA(cudaMemcpyAsync(hspan.data(), span.get(), (size_t)nbr * sizeof(long long),
+                                     cudaMemcpyDeviceToHost, s));
+            SDL_CUDA(cudaStreamSynchronize(s));
+            std::vector<int> idx(nbr);
+            for (int q = 0; q < nbr; ++q) idx[q] = q;
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return hspan[x] > hspan[y]; });
+            for (int q = 0; q < nbr; ++q) idx[q] = hrows[idx[q]];
+            DevBuf<int> order((size_t)nbr), counter(1);
+            SDL_CUDA(cudaMemcpyAsync(order.get(), idx.data(), (size_t)nbr * sizeof(int), cudaMemcpyHostToDevice, s));
+            SDL_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(int), s));
+            SDL_LAUNCH(k_sym_bitmap, grid, th, sm, s, order.get(), nbr, sa, words, counter.get());
+            SDL_CUDA(cudaStreamSynchronize(s)); // idx and the queue are released on return
+        }
     }
 }
 
