@@ -21,6 +21,7 @@
 //             accumulator (<= 8192 output entries), CTA + accumulator in C.x itself
 //             with a global column->position map (larger rows).
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <chrono>
 #include <cstddef>
@@ -3086,23 +3087,24 @@ namespace {
 template <bool BATCHED, int NT, bool ESS>
 int refill_per_sm(size_t smem)
 {
-    // plain kernels: one size, cached; staged ones: the last size asked for
-    static size_t last_smem = 0;
-    static int per_sm = 0;
+    // resident CTAs per SM for each (device, shared-memory size) met; the kernel's
+    // shared-memory attribute is set on each device the first time
+    static std::map<std::pair<int, size_t>, int> cache;
     static std::mutex mu;
+    int dev = 0;
+    SDL_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> g(mu);
-    if (!per_sm || smem != last_smem)
-    {
-        if (ESS)
-            SDL_CUDA(cudaFuncSetAttribute(k_tile_refill<BATCHED, NT, ESS>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STAGED_SMEM_MAX));
-        else
-            set_smem(k_tile_refill<BATCHED, NT, ESS>, smem);
-        int n = 0;
-        SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT, ESS>, NT, smem));
-        per_sm = std::max(1, n);
-        last_smem = smem;
-    }
+    auto it = cache.find({dev, smem});
+    if (it != cache.end()) return it->second;
+    if (ESS)
+        SDL_CUDA(cudaFuncSetAttribute(k_tile_refill<BATCHED, NT, ESS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)STAGED_SMEM_MAX));
+    else
+        set_smem(k_tile_refill<BATCHED, NT, ESS>, smem);
+    int n = 0;
+    SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT, ESS>, NT, smem));
+    const int per_sm = std::max(1, n);
+    cache[{dev, smem}] = per_sm;
     return per_sm;
 }
 
