@@ -3091,11 +3091,21 @@ int refill_per_sm(size_t smem)
     // shared-memory attribute is set on each device the first time
     static std::map<std::pair<int, size_t>, int> cache;
     static std::mutex mu;
+    // the last answer of this thread, without the lock (launches repeat the same key)
+    thread_local int last_dev = -1, last_val = 0;
+    thread_local size_t last_smem = 0;
     int dev = 0;
     SDL_CUDA(cudaGetDevice(&dev));
+    if (dev == last_dev && smem == last_smem) return last_val;
     std::lock_guard<std::mutex> g(mu);
     auto it = cache.find({dev, smem});
-    if (it != cache.end()) return it->second;
+    if (it != cache.end())
+    {
+        last_dev = dev;
+        last_smem = smem;
+        last_val = it->second;
+        return last_val;
+    }
     if (ESS)
         SDL_CUDA(cudaFuncSetAttribute(k_tile_refill<BATCHED, NT, ESS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)STAGED_SMEM_MAX));
@@ -3105,6 +3115,9 @@ int refill_per_sm(size_t smem)
     SDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_tile_refill<BATCHED, NT, ESS>, NT, smem));
     const int per_sm = std::max(1, n);
     cache[{dev, smem}] = per_sm;
+    last_dev = dev;
+    last_smem = smem;
+    last_val = per_sm;
     return per_sm;
 }
 
