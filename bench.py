@@ -784,9 +784,10 @@ def _event_ms(fn, stream, steps, flush=None):
     return sum(a.elapsed_time(b) for a, b in evs) / steps
 
 
-_BUILD_NOTE = ("structure_ms: median wall time of 3 builds (structure + first value fill, device "
-               "memory released between them); first_build_ms: the first of them, which also loads the "
-               "kernels (CUDA loads modules on first launch)")
+_BUILD_NOTE = ("structure_ms: median wall time of 3 builds (structure + first value fill, each build's "
+               "device memory freed before the next: returned to the library's block cache, which the "
+               "next build allocates from); first_build_ms: the first of them, which also loads the kernels "
+               "(CUDA loads modules on first launch) and allocates from the driver")
 
 
 def _builds(build, runs=3):
@@ -1070,7 +1071,9 @@ def run_learned(args, dev, check=False):
     pass (rows up to 8192 terms sorted with their values into the network's
     predicted capacity, overflowing rows redone exactly, larger rows by the bitmap
     pass and an accumulating kernel; no refill plan). Each is timed `learned_runs`
-    times (median and range reported), device memory released between runs. The
+    times (median and range reported), each build's device memory freed before the
+    next (into the library's block cache, which both paths then allocate from; an
+    untimed build of each path runs first). The
     network is trained first on the row statistics of 200 seeded smaller matrices
     of the same recipe. Outputs are compared bit for bit."""
     import torch

@@ -56,6 +56,11 @@ int sdl_device_available(void);
 /* Number of device allocations / kernel launches the library has made so far. */
 unsigned long long sdl_device_alloc_count(void);
 unsigned long long sdl_kernel_launch_count(void);
+/* The library keeps device memory it has freed (plans' scratch, destroyed
+   products) in a cache for its next allocations, up to a quarter of the device's
+   memory; this returns the current device's cached blocks to the driver (after a
+   device synchronisation), e.g. before a large allocation of the application's own. */
+void sdl_release_cached_memory(void);
 /* The library's stream (a cudaStream_t) and a full synchronisation of it. */
 void *sdl_stream(void);
 sdl_status sdl_synchronize(void);

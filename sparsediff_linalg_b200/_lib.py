@@ -91,6 +91,7 @@ EXTENSION_SIGNATURES = {
     "sdl_set_fatal_errors": (None, [C.c_int]),
     "sdl_device_available": (C.c_int, []),
     "sdl_device_alloc_count": (C.c_ulonglong, []),
+    "sdl_release_cached_memory": (None, []),
     "sdl_kernel_launch_count": (C.c_ulonglong, []),
     "sdl_stream": (vp, []),
     "sdl_synchronize": (C.c_int, []),

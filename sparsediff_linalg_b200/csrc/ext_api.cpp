@@ -55,6 +55,8 @@ extern "C" int sdl_device_available(void)
 }
 
 extern "C" unsigned long long sdl_device_alloc_count(void) { return g_dev_allocs.load(); }
+
+extern "C" void sdl_release_cached_memory(void) { release_cached_device_memory(); }
 extern "C" unsigned long long sdl_kernel_launch_count(void) { return g_launches.load(); }
 
 extern "C" void *sdl_stream(void)

@@ -3,6 +3,8 @@
 // uses.
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <unordered_map>
 #include <mutex>
 #include <string>
 
@@ -64,24 +66,125 @@ int take_device_error(cudaStream_t s)
     return h;
 }
 
+// Device memory: a cache of freed blocks per device in front of cudaMalloc, so that
+// plans built again and again (new patterns, re-plans) reuse their scratch instead of
+// paying cudaMalloc / cudaFree for several GB each time. A block is cached only after
+// a device synchronisation -- what cudaFree implies -- so no kernel still in flight
+// uses it when it is handed out again. Sizes above 1 MiB are rounded up to 2 MiB; a
+// request takes the smallest cached block of its device between its size and twice
+// it. The cache holds at most a quarter of the device's memory; an allocation that
+// fails empties it and tries once more; sdl_release_cached_memory empties it.
+namespace {
+struct DevCache
+{
+    std::mutex mu;
+    std::unordered_map<void *, std::pair<size_t, int>> live; // block -> (bytes, device)
+    std::multimap<std::pair<int, size_t>, void *> idle;        // (device, bytes) -> block
+    std::unordered_map<int, size_t> idle_bytes, cap;           // per device
+};
+DevCache &dev_cache()
+{
+    static DevCache c;
+    return c;
+}
+
+size_t round_block(size_t bytes)
+{
+    const size_t q = bytes > (1u << 20) ? (2u << 20) : 512u;
+    return (bytes + q - 1) / q * q;
+}
+
+// Frees every idle block of `dev` (the caller holds the lock).
+void release_idle(DevCache &c, int dev)
+{
+    for (auto it = c.idle.lower_bound({dev, 0}); it != c.idle.end() && it->first.first == dev;)
+    {
+        cudaFree(it->second);
+        it = c.idle.erase(it);
+    }
+    c.idle_bytes[dev] = 0;
+}
+} // namespace
+
 void *dev_alloc(size_t bytes)
 {
     runtime();
+    const size_t want = round_block(bytes);
+    int dev = 0;
+    SDL_CUDA(cudaGetDevice(&dev));
+    DevCache &c = dev_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    g_dev_allocs.fetch_add(1, std::memory_order_relaxed);
+    auto it = c.idle.lower_bound({dev, want});
+    if (it != c.idle.end() && it->first.first == dev && it->first.second <= 2 * want)
+    {
+        void *p = it->second;
+        const size_t have = it->first.second;
+        c.idle.erase(it);
+        c.idle_bytes[dev] -= have;
+        c.live[p] = {have, dev};
+        return p;
+    }
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        release_idle(c, dev);
+        e = cudaMalloc(&p, want);
+    }
     if (e != cudaSuccess)
     {
         cudaGetLastError();
         throw Error(SDL_ERR_OOM, "device allocation of " + std::to_string(bytes) +
                                      " bytes failed: " + cudaGetErrorString(e));
     }
-    g_dev_allocs.fetch_add(1, std::memory_order_relaxed);
+    c.live[p] = {want, dev};
+    if (!c.cap.count(dev))
+    {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        c.cap[dev] = tot / 4;
+    }
     return p;
 }
 
 void dev_free(void *p)
 {
-    if (p) cudaFree(p);
+    if (!p) return;
+    DevCache &c = dev_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.live.find(p);
+    if (it == c.live.end())
+    {
+        cudaFree(p);
+        return;
+    }
+    const size_t bytes = it->second.first;
+    const int dev = it->second.second;
+    c.live.erase(it);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev || c.idle_bytes[dev] + bytes > c.cap[dev] || cudaDeviceSynchronize() != cudaSuccess)
+    {
+        cudaGetLastError();
+        cudaFree(p);
+        return;
+    }
+    c.idle.insert({{dev, bytes}, p});
+    c.idle_bytes[dev] += bytes;
+}
+
+void release_cached_device_memory()
+{
+    DevCache &c = dev_cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+    {
+        cudaDeviceSynchronize();
+        release_idle(c, dev);
+    }
 }
 
 // ------------------------------------------------------------------ scan

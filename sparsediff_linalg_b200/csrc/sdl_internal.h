@@ -83,8 +83,9 @@ inline cudaStream_t pick_stream(void *s)
 int take_device_error(cudaStream_t s);
 
 // ---------------------------------------------------------------- memory
-void *dev_alloc(size_t bytes); // cudaMalloc, counted; throws on failure
-void dev_free(void *p);
+void *dev_alloc(size_t bytes); // from the block cache or cudaMalloc, counted; throws on failure
+void dev_free(void *p);         // into the block cache (after a device synchronisation) or cudaFree
+void release_cached_device_memory(); // frees the current device's cached blocks
 extern std::atomic<unsigned long long> g_dev_allocs;
 
 template <class T>
