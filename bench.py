@@ -443,7 +443,11 @@ def run_b200(args, world, rank, local):
     traffic = None
     tj = ROOT / "profiles" / "btda_refill_traffic.json"
     if tj.exists():
-        traffic = json.loads(tj.read_text()).get("dram_bytes_per_launch")
+        tr = json.loads(tj.read_text())
+        # the capture of the refill this run uses (the autotuner's choice when it ran)
+        kind = (tune or {}).get("refill", "direct")
+        entry = tr if kind == "direct" else tr.get(kind)
+        traffic = entry.get("dram_bytes_per_launch") if isinstance(entry, dict) else None
     headline_parity = None
     if check:
         from oracle import parallel
